@@ -1,0 +1,347 @@
+"""The oracle pinned by the reference's own particle tests.
+
+Each test restates one reference test (FlipTest, Flip3Test, ScatterTest, SortTest,
+FixedScatterTest, under vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/)
+with its seeded inputs regenerated by the java.util.Random restatement, and applies the
+reference's assertions to the oracle. A test here failing means the restatement is wrong,
+not the kernels.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from _oracle import (F, WALL, Flip2State, Flip3State, JavaRandom, Particles, cells2, flip3_params, flip_column,
+                     flip_params, fp, ip, key3, lib, slab3, stable_step)
+
+
+# ---------------------------------------------------------------------------------- FlipTest
+
+def test_flip2_lone_particle_falls_as_gravity_says():
+    """FlipTest.aLoneParticleFallsAsGravitySays (FlipTest.java:27-47)."""
+    dt, g, steps = 0.01, -10.0, 5
+    s = Flip2State(16, 16, np.array([7.3], F), np.array([12.6], F), np.array([0.25], F))
+    for _ in range(steps):
+        s.step(flip_params(dt, 0, g, 0, 1))
+    assert abs(s.a["v"][0] - steps * g * dt) <= 1e-5
+    assert abs(s.a["y"][0] - (12.6 + g * dt * dt * steps * (steps + 1) / 2)) <= 1e-4
+    assert abs(s.a["x"][0] - 7.3) <= 1e-5
+    assert abs(s.a["u"][0]) <= 1e-6
+    assert abs(s.a["j"][0] - 1) <= 1e-6
+
+
+def flip2_dam_break(state_step, n=32, height=16, width=8, g=200.0, rho0=1.0, seed=71):
+    """FlipTest.aDamBreakStaysWaterInItsBox (FlipTest.java:72-127): returns the measured quantities."""
+    fall = math.sqrt(2 * g * height)
+    sound = 5 * fall
+    bulk = sound * sound * rho0
+    dt = stable_step(bulk, rho0, fall, 0.3)
+    early = math.ceil(0.1 / dt)
+    steps = math.ceil(0.6 / dt)
+    x, y, m = flip_column(seed, width, height)
+    return state_step(n, x, y, m, flip_params(dt, 0, -g, bulk, rho0), early, steps), (early, steps, dt, g, height)
+
+
+def check_flip2_dam_break(x, y, j, moved, early, dt, g, height, n=32):
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(y)) and np.all(np.isfinite(j))
+    assert np.all((x >= WALL) & (x <= n - 1 - WALL) & (y >= WALL) & (y <= n - 1 - WALL)), "a particle left the box"
+    ritter = 2 * math.sqrt(g * height) * early * dt
+    sj = np.sort(j)
+    sy = np.sort(y)
+    j_low = sj[int(0.01 * len(j))]
+    j_high = sj[int(0.99 * len(j))]
+    h95 = sy[int(0.95 * len(y))] - WALL
+    assert moved > 1, f"the front moved {moved} cells; the water did not fall"
+    assert moved < ritter * 1.05, f"the front moved {moved} cells, past Ritter's {ritter}"
+    assert j_low > 0.9 and j_high < 1.1, f"J spans {j_low} .. {j_high}; not weakly compressible"
+    assert h95 < height, f"95% of the water reaches {h95} cells"
+
+
+def test_flip2_dam_break_stays_water_in_its_box():
+    def run(n, x, y, m, params, early, steps):
+        s = Flip2State(n, n, x, y, m)
+        moved = 0.0
+        for k in range(steps):
+            if k % 10 == 0:
+                s.sort()
+            s.step(params)
+            if k == early - 1:
+                moved = float(s.a["x"].max()) - (1 + 8)
+        return s.a["x"], s.a["y"], s.a["j"], moved
+
+    (x, y, j, moved), (early, steps, dt, g, height) = flip2_dam_break(run)
+    check_flip2_dam_break(x, y, j, moved, early, dt, g, height)
+
+
+# ---------------------------------------------------------------------------------- Flip3Test
+
+def test_flip3_lone_particle_falls_as_gravity_says():
+    """Flip3Test.aLoneParticleFallsAsGravitySays (Flip3Test.java:25-50)."""
+    dt, g, steps = 0.01, -10.0, 5
+    s = Flip3State(12, 12, 12, np.array([5.3], F), np.array([8.6], F), np.array([6.2], F), np.array([0.125], F))
+    for _ in range(steps):
+        s.step(flip3_params(dt, 0, g, 0, 0, 1))
+    a = s.a
+    assert abs(a["v"][0] - steps * g * dt) <= 1e-5
+    assert abs(a["y"][0] - (8.6 + g * dt * dt * steps * (steps + 1) / 2)) <= 1e-4
+    assert abs(a["x"][0] - 5.3) <= 1e-5 and abs(a["z"][0] - 6.2) <= 1e-5
+    assert abs(a["u"][0]) <= 1e-6 and abs(a["w"][0]) <= 1e-6
+    assert abs(a["j"][0] - 1) <= 1e-6
+
+
+def conservation_particles3(n=14, count=150, seed=3):
+    """The inputs of Flip3Test.theScatterConservesMassAndMomentum (Flip3Test.java:57-90)."""
+    r = JavaRandom(seed)
+    x, y, z, m, j = (np.empty(count, F) for _ in range(5))
+    vel = np.empty((3, count), F)
+    c = np.empty((9, count), F)
+    for p in range(count):
+        x[p] = F(1) + r.next_float() * F(n - 3)
+        y[p] = F(1) + r.next_float() * F(n - 3)
+        z[p] = F(1) + r.next_float() * F(n - 3)
+        m[p] = F(0.1) + r.next_float() * F(0.3)
+        j[p] = F(0.8) + r.next_float() * F(0.4)
+        for a in range(3):
+            vel[a, p] = r.next_float() * F(4) - F(2)
+        for a in range(9):
+            c[a, p] = r.next_float() * F(2) - F(1)
+    return x, y, z, m, j, vel, c
+
+
+def test_flip3_scatter_conserves_mass_and_momentum():
+    """Flip3Test.theScatterConservesMassAndMomentum (Flip3Test.java:57-118)."""
+    n = 14
+    x, y, z, m, j, vel, c = conservation_particles3(n)
+    fields = {"u": vel[0], "v": vel[1], "w": vel[2], "j": j}
+    fields.update({f"c{a // 3}{a % 3}": c[a] for a in range(9)})
+    s = Flip3State(n, n, n, x, y, z, m, **fields)
+    s.clear_scatter(flip3_params(0.01, 0, -10, 0, 1e4, 1))
+    mass = float(np.sum(m.astype(np.float64)))
+    assert abs(mass - np.sum(s.g["gm"].astype(np.float64))) <= 1e-4 * mass
+    for a, g in enumerate(("gmu", "gmv", "gmw")):
+        mom = float(np.sum(m.astype(np.float64) * vel[a].astype(np.float64)))
+        tot = float(np.sum(s.g[g].astype(np.float64)))
+        assert abs(mom - tot) <= 1e-3 * max(1, abs(mom)) + 1e-3
+
+
+def test_flip3_dam_break_slab_stays_water_and_does_not_move_along_z():
+    """Flip3Test.aDamBreakInASlabStaysWaterInItsBoxAndDoesNotMoveAlongZ (Flip3Test.java:134-221)."""
+    n, height, g, rho0 = 24, 12, 200.0, 1.0
+    fall = math.sqrt(2 * g * height)
+    bulk = (5 * fall) ** 2 * rho0
+    dt = stable_step(bulk, rho0, fall, 0.3)
+    early = math.ceil(0.12 / dt)
+    steps = math.ceil(0.4 / dt)
+    x, y, z, m = slab3(71, n)
+    s = Flip3State(n, n, n, x, y, z, m)
+    params = flip3_params(dt, 0, -g, 0, bulk, rho0)
+    moved = 0.0
+    for k in range(steps):
+        s.step(params)
+        if k == early - 1:
+            moved = float(s.a["x"].max()) - (1 + 6)
+    a = s.a
+    for f in ("x", "y", "z", "j"):
+        assert np.all(np.isfinite(a[f]))
+    for f in ("x", "y", "z"):
+        assert np.all((a[f] >= WALL) & (a[f] <= n - 1 - WALL))
+    ritter = 2 * math.sqrt(g * height) * early * dt
+    sj, sy = np.sort(a["j"]), np.sort(a["y"])
+    cnt = len(x)
+    j_low, j_high = sj[int(0.01 * cnt)], sj[int(0.99 * cnt)]
+    h95 = sy[int(0.95 * cnt)] - WALL
+    along_z = math.sqrt(np.mean(a["w"].astype(np.float64) ** 2)) / math.sqrt(np.mean(a["u"].astype(np.float64) ** 2))
+    assert 1 < moved < ritter * 1.05
+    assert j_low > 0.9 and j_high < 1.1
+    assert h95 < height
+    assert along_z < 0.2
+
+
+# ---------------------------------------------------------------------------------- ScatterTest
+
+def scatter_reference(n, p: Particles):
+    gm, gmu, gmv = (np.zeros(n * n, np.float64) for _ in range(3))
+    from _oracle import dp
+    lib().or_scatter2_bilinear_f64(n, n, fp(p.x), fp(p.y), fp(p.u), fp(p.v), fp(p.m), p.count(), dp(gm), dp(gmu),
+                                   dp(gmv))
+    return gm, gmu, gmv
+
+
+def scatter_oracle(n, p: Particles):
+    gm, gmu, gmv = (np.zeros(n * n, F) for _ in range(3))
+    lib().or_scatter2_bilinear(n, n, fp(p.x), fp(p.y), fp(p.u), fp(p.v), fp(p.m), p.count(), fp(gm), fp(gmu),
+                               fp(gmv))
+    return gm, gmu, gmv
+
+
+def holds_what_the_particles_did(n, p: Particles, grid, label=""):
+    """ScatterTest.holdsWhatTheParticlesDid (ScatterTest.java:125-144)."""
+    expected = scatter_reference(n, p)
+    m = p.m.astype(np.float64)
+    mass = m.sum()
+    mx = (m * p.u.astype(np.float64)).sum()
+    my = (m * p.v.astype(np.float64)).sum()
+    g = [np.asarray(a, np.float64) for a in grid]
+    assert abs(mass - g[0].sum()) <= mass * 1e-6, label + ": the grid gained or lost mass"
+    assert abs(mx - g[1].sum()) <= abs(mx) * 1e-5 + 1e-3, label + ": x-momentum"
+    assert abs(my - g[2].sum()) <= abs(my) * 1e-5 + 1e-3, label + ": y-momentum"
+    for f in range(3):
+        err = np.abs(expected[f] - g[f])
+        tol = 1e-5 * np.maximum(1, np.abs(expected[f]))
+        assert np.all(err <= tol), f"{label}: field {f} at node {int(np.argmax(err - tol))}"
+
+
+@pytest.fixture(scope="module")
+def jittered64():
+    return Particles.jittered(63, 4, JavaRandom(7))
+
+
+def test_scatter_oracle_holds_what_the_particles_did(jittered64):
+    """ScatterTest.theGridHoldsWhatTheParticlesDid (ScatterTest.java:51-64), the particle-order sum."""
+    n = 64
+    for particles in (jittered64, jittered64.shuffled(JavaRandom(8))):
+        holds_what_the_particles_did(n, particles, scatter_oracle(n, particles))
+
+
+def broken_runs():
+    """The inputs of ScatterTest.theSegmentedSumKeepsBrokenRunsApart (ScatterTest.java:88-108)."""
+    cells = [(1, 1), (2, 1), (1, 2)]
+    pattern = [0, 0, 1, 0, 2, 2, 2, 0, 1, 1, 0]
+    count = 301
+    r = JavaRandom(51)
+    p = Particles(*(np.empty(count, F) for _ in range(5)))
+    for k in range(count):
+        c = cells[pattern[k % len(pattern)]]
+        p.x[k] = F(c[0]) + r.next_float() * F(0.999)
+        p.y[k] = F(c[1]) + r.next_float() * F(0.999)
+        p.u[k] = F(r.next_gaussian())
+        p.v[k] = F(r.next_gaussian())
+        p.m[k] = F(0.5) + r.next_float()
+    return p
+
+
+def test_scatter_oracle_broken_runs():
+    holds_what_the_particles_did(8, broken_runs(), scatter_oracle(8, broken_runs()))
+
+
+def test_a_particle_on_a_node_weighs_only_on_it():
+    """ScatterTest.aParticleOnANodeWeighsOnlyOnIt (ScatterTest.java:150-164)."""
+    n = 8
+    p = Particles(np.array([3, 7, -2], F), np.array([5, 7, 1e9], F), np.array([1, 1, 1], F), np.zeros(3, F),
+                  np.array([2, 3, 5], F))
+    gm = scatter_oracle(n, p)[0]
+    expected = np.zeros(n * n, F)
+    expected[5 * n + 3] = 2
+    expected[7 * n + 7] = 3
+    expected[7 * n] = 5
+    assert np.array_equal(gm, expected)
+
+
+def test_a_uniform_flow_reads_back_as_itself():
+    """ScatterTest.aUniformFlowReadsBackAsItself (ScatterTest.java:171-195)."""
+    n = 32
+    allp = Particles.jittered(n - 1, 4, JavaRandom(11))
+    west = allp.where(allp.x < n / 2 - 2)
+    west.u[:] = 1.25
+    west.v[:] = -0.5
+    gm, gmu, gmv = scatter_oracle(n, west)
+    node = np.arange(n * n)
+    east = node % n >= n // 2
+    assert np.all(gm[east] == 0) and np.all(gmu[east] == 0) and np.all(gmv[east] == 0)
+    wet = (~east) & (gm > 0)
+    assert np.all(np.abs(gmu[wet] / gm[wet] - 1.25) <= 1e-5)
+    assert np.all(np.abs(gmv[wet] / gm[wet] + 0.5) <= 1e-5)
+    assert wet.sum() > n * n / 3
+
+
+def test_cell_starts_refuses_particles_out_of_order():
+    """ScatterTest.cellStartsRefusesParticlesOutOfOrder (ScatterTest.java:111-123)."""
+    import ctypes
+    p = Particles.jittered(7, 2, JavaRandom(3)).shuffled(JavaRandom(4))
+    starts = np.zeros(50, np.int32)
+    bad = ctypes.c_int64(-1)
+    assert lib().or_cell_starts2(fp(p.x), fp(p.y), p.count(), 8, 8, ip(starts), ctypes.byref(bad)) == -1
+    q = p.sorted_by_cell(8)
+    assert lib().or_cell_starts2(fp(q.x), fp(q.y), q.count(), 8, 8, ip(starts), ctypes.byref(bad)) == 0
+    assert starts[49] == p.count()
+    assert np.all(np.diff(starts) == 2)
+
+
+# ---------------------------------------------------------------------------------- SortTest
+
+def counting_sort(keys, cells):
+    starts = np.zeros(cells + 1, np.int32)
+    perm = np.zeros(len(keys), np.int32)
+    lib().or_counting_sort(ip(keys), len(keys), cells, ip(starts), ip(perm))
+    return starts, perm
+
+
+def test_sort_by_cell_equals_the_hosts_stable_sort():
+    """SortTest.theDeviceSortsByCell (SortTest.java:51-61): starts exactly the host's cellStarts,
+    and the particles in cell order. The oracle's order within a cell is the input order, which
+    is also what the host's stable sortedByCell gives, so here the whole permutation matches."""
+    import ctypes
+    n = 260
+    p = Particles.jittered(n - 1, 1, JavaRandom(21)).shuffled(JavaRandom(22))
+    keys = cells2(p.x, p.y, n, n)
+    starts, perm = counting_sort(keys, (n - 1) * (n - 1))
+    expected = p.sorted_by_cell(n)
+    host_starts = np.zeros((n - 1) ** 2 + 1, np.int32)
+    bad = ctypes.c_int64(0)
+    assert lib().or_cell_starts2(fp(expected.x), fp(expected.y), expected.count(), n, n, ip(host_starts),
+                                 ctypes.byref(bad)) == 0
+    assert np.array_equal(starts, host_starts)
+    got = p.select(perm)
+    for f in ("x", "y", "u", "v", "m"):
+        assert np.array_equal(getattr(got, f).view(np.int32), getattr(expected, f).view(np.int32))
+
+
+def test_a_second_sort_starts_from_zero_counts():
+    """SortTest.aSecondSortStartsFromZeroCounts (SortTest.java:68-81), for the oracle's sort."""
+    n = 40
+    first = Particles.jittered(n - 1, 3, JavaRandom(31)).shuffled(JavaRandom(32))
+    second = Particles.jittered(n - 1, 3, JavaRandom(33)).shuffled(JavaRandom(34))
+    for p in (first, second):
+        keys = cells2(p.x, p.y, n, n)
+        starts, perm = counting_sort(keys, (n - 1) ** 2)
+        assert np.array_equal(perm, np.argsort(keys, kind="stable"))
+        assert starts[-1] == p.count()
+
+
+def test_key3_is_the_stencil_base_cell_brick_major():
+    """The 3D key: Stencil3's base cell (Flip3.java:671-673) in 8x8x8 bricks."""
+    nx, ny, nz = 40, 24, 20
+    r = np.random.default_rng(5)
+    x = (r.random(2000) * (nx + 4) - 2).astype(F)
+    y = (r.random(2000) * (ny + 4) - 2).astype(F)
+    z = (r.random(2000) * (nz + 4) - 2).astype(F)
+    keys = key3(x, y, z, nx, ny, nz)
+    nb = [(nx - 2 + 7) // 8, (ny - 2 + 7) // 8, (nz - 2 + 7) // 8]
+    for k, a, b, c in zip(keys, x, y, z):
+        cell = []
+        for v, size in ((a, nx), (b, ny), (c, nz)):
+            v = min(max(v, F(0.5)), F(size - 1.5))
+            cell.append(int(min(v - F(0.5), F(size - 3))))
+        brick = ((cell[2] // 8) * nb[1] + cell[1] // 8) * nb[0] + cell[0] // 8
+        local = ((cell[2] % 8) * 8 + cell[1] % 8) * 8 + cell[0] % 8
+        assert k == brick * 512 + local
+    assert lib().or_key3_count(nx, ny, nz) == nb[0] * nb[1] * nb[2] * 512
+
+
+# ---------------------------------------------------------------------------------- FixedScatterTest
+
+def test_fixed_scatter_conserves_mass_exactly_in_any_order(jittered64):
+    """FixedScatter (FixedScatter.java:24-60): integer accumulation gives the same grid in any order,
+    and the grid's mass quanta sum to the particles' exactly."""
+    n = 64
+    p = jittered64
+    outs = []
+    for q in (p, p.shuffled(JavaRandom(8))):
+        g = [np.zeros(n * n, np.int32) for _ in range(3)]
+        lib().or_fixed_scatter2(n, n, fp(q.x), fp(q.y), fp(q.u), fp(q.v), fp(q.m), q.count(), 14, 10,
+                                ip(g[0]), ip(g[1]), ip(g[2]))
+        outs.append(g)
+        quanta = (q.m * F(2 ** 14)).astype(np.int64)
+        assert int(g[0].astype(np.int64).sum()) == int(quanta.sum())
+    for f in range(3):
+        assert np.array_equal(outs[0][f], outs[1][f])
