@@ -1,0 +1,223 @@
+/*
+ * vexfluid.h -- C-ABI of libvexfluid, the B200 (sm_100a) implementation of the
+ * data-parallel fluid step of sibarum/vexelray-sim-fluid.
+ *
+ * It replaces, beneath the reference's three Java runner classes, SupirVast's
+ * PassRunner/Accelerator and the IR kernels they run:
+ *   ParticleSimulation   (vexelray-sim-fluid-gui/.../gui/ParticleSimulation.java)   -> vf_mpm2_*
+ *   ParticleSimulation3  (vexelray-sim-fluid-gui/.../gui/ParticleSimulation3.java)  -> vf_mpm3_*
+ *   PatchSimulation      (vexelray-sim-fluid-gui/.../gui/PatchSimulation.java)      -> vf_swe_*
+ * The Java classes keep their public methods and call these through Panama FFM
+ * (see INTEGRATION.md for the downcall stubs).
+ *
+ * Conventions
+ *  - Every function returns int32_t status: VF_OK (0) or a negative VF_E* code. The
+ *    message of the calling thread's last error is vf_last_error(). Nothing aborts.
+ *  - Handles are opaque. The library owns all device memory; host arrays are the
+ *    caller's and are copied in and out synchronously.
+ *  - Params are the reference's int[] of float bits (Flip.params, Flip3.params,
+ *    ShallowWater.params), so Java call sites pass the same arrays.
+ *  - Positions in node units; grid index (k*ny + j)*nx + i; SoA f32 particles.
+ *  - A handle belongs to the thread that made it (one CUDA stream per handle).
+ */
+#ifndef VEXFLUID_H
+#define VEXFLUID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum {
+    VF_OK = 0,
+    VF_EINVAL = -1,    /* an argument the reference refuses with IllegalArgumentException */
+    VF_ESTATE = -2,    /* a call the object's state or features do not allow (IllegalStateException) */
+    VF_ENOMEM = -3,    /* device or host allocation failed */
+    VF_ECUDA = -4,     /* a CUDA runtime error; vf_last_error has the text */
+    VF_ETIMEOUT = -5,  /* a bounded device-side wait gave up */
+    VF_ENODEV = -6,    /* no CUDA device, or not an sm_100 device */
+    VF_EDEVICE = -7    /* a kernel set an error bit in the handle's device status word */
+};
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated to cap). Returns its length. */
+int32_t vf_last_error(char* buf, size_t cap);
+/* Library version, and whether a usable CUDA device is present (1) or not (0). */
+int32_t vf_version(void);
+int32_t vf_device_ok(void);
+
+/* ------------------------------------------------------------------ physics flags */
+/* Flags for vf_mpm2_create / vf_mpm3_prepare. The reference's physics is the default (0):
+ * p = B(1/J - 1) (Flip.java:71-78) and the one-node wall ring (Flip.java:122-131). */
+enum {
+    VF_EOS_TAIT = 1u << 0,          /* p = k((1/J)^7 - 1), k = the params' bulk word */
+    VF_WALL_STICKY_SHIFT = 8,       /* bits 8..15: nodes within this many of an edge are stopped */
+    VF_WALL_STICKY_MASK = 0xffu << 8,
+    VF_P2G_SHIFT = 16,              /* bits 16..19: the 3D scatter schedule, VF_P2G_* */
+    VF_P2G_MASK = 0xfu << 16,
+    VF_NO_SORT = 1u << 20           /* 3D: keep the particles in load order (Flip3Step's behaviour) */
+};
+#define VF_WALL_STICKY(t) ((uint32_t)(t) << VF_WALL_STICKY_SHIFT)
+
+/* 3D P2G schedules: the three the 3D config compares. */
+enum {
+    VF_P2G_TILE = 0,    /* sorted particles, one CTA per 8^3-cell brick, shared-memory window, vector red to HBM */
+    VF_P2G_ATOMIC = 1,  /* one thread per particle, 27 vector atomics (Flip3.java:225-243's direct scatter) */
+    VF_P2G_WARP = 2     /* one thread per particle, runs of one cell summed across the warp first
+                           (Scatter.segmentedDeposit, Scatter.java:385-439, over 27 nodes x 4 fields) */
+};
+
+/* ------------------------------------------------------------------ 2D particles (ParticleSimulation) */
+typedef struct vf_mpm2 vf_mpm2;
+
+enum {   /* fields for vf_mpm2_read / vf_mpm2_write (FlipStep.java:95-110 buffer names) */
+    VF2_X = 0, VF2_Y, VF2_U, VF2_V, VF2_M, VF2_J, VF2_C00, VF2_C01, VF2_C10, VF2_C11,
+    VF2_GM = 16, VF2_GMU, VF2_GMV, VF2_GU, VF2_GV
+};
+
+/* new ParticleSimulation(nx, ny, particles) (ParticleSimulation.java:39-81): nx, ny >= 3
+ * (Scatter.java:516-520 needs >= 2; the quadratic stencil needs 3), particles >= 1 (FlipStep.java:86-88).
+ * flags: VF_EOS_TAIT, VF_WALL_STICKY(t). The sort's counts start at zero. */
+int32_t vf_mpm2_create(int32_t nx, int32_t ny, int32_t particles, uint32_t flags, vf_mpm2** out);
+/* ParticleSimulation.load (ParticleSimulation.java:129-143): positions, velocities and masses; J = 1, C = 0;
+ * params = Flip.params words (>= 5); resets the step count. */
+int32_t vf_mpm2_load(vf_mpm2* h, const float* x, const float* y, const float* u, const float* v, const float* m,
+                     const int32_t* params, int32_t nparams);
+/* ParticleSimulation.params(int[]) (ParticleSimulation.java:170-172) */
+int32_t vf_mpm2_params(vf_mpm2* h, const int32_t* params, int32_t nparams);
+/* ParticleSimulation.advance(count, sortEvery) (ParticleSimulation.java:175-183): sorts first on every step
+ * whose number (counted across calls) is a multiple of sort_every (>= 1). */
+int32_t vf_mpm2_advance(vf_mpm2* h, int32_t count, int32_t sort_every);
+/* One FlipStep.step() (clear, scatter, grid, advect), and one FlipStep.sort(), without counting a step:
+ * what the reference's test Rig runs (Rig.java:30-34). */
+int32_t vf_mpm2_step(vf_mpm2* h);
+int32_t vf_mpm2_sort(vf_mpm2* h);
+/* Readbacks (grid(), positions(), velocities(), masses(), compression(); ParticleSimulation.java:190-220)
+ * and writes (compression(float[]) at 213-215; any particle field for tests). n must equal the field's length. */
+int32_t vf_mpm2_read(vf_mpm2* h, int32_t field, float* out, int64_t n);
+int32_t vf_mpm2_write(vf_mpm2* h, int32_t field, const float* in, int64_t n);
+/* The last sort's cell starts, (nx-1)(ny-1)+1 words (Scatter.cellStarts' layout, Scatter.java:484-502). */
+int32_t vf_mpm2_read_starts(vf_mpm2* h, int32_t* out, int64_t n);
+int64_t vf_mpm2_steps(const vf_mpm2* h);
+int32_t vf_mpm2_on_gpu(const vf_mpm2* h);
+void vf_mpm2_destroy(vf_mpm2* h);
+
+/* ------------------------------------------------------------------ 2D bilinear P2G (Scatter) */
+/* Scatter.Mode (Scatter.java:122-144): the four schedules of the bilinear transfer. */
+enum { VF_SCATTER_GRID = 0, VF_SCATTER_PRE_REDUCED = 1, VF_SCATTER_GATHER = 2, VF_SCATTER_SEGMENTED = 3 };
+/* One bilinear P2G of host particles onto an nx x ny grid (Scatter.kernel/preReduced/gather/segmented,
+ * Scatter.java:154-350); GATHER needs the particles in cell order (Scatter.cellStarts refuses others:
+ * VF_EINVAL). Outputs gm, gmu, gmv of nx*ny floats. */
+int32_t vf_scatter2(int32_t mode, int32_t nx, int32_t ny, const float* x, const float* y, const float* u,
+                    const float* v, const float* m, int64_t np, float* gm, float* gmu, float* gmv);
+/* The fixed-point bilinear P2G (FixedScatter.kernel, FixedScatter.java:153-229): i32 registers, the same bits
+ * in any order. */
+int32_t vf_fixed_scatter2(int32_t nx, int32_t ny, const float* x, const float* y, const float* u, const float* v,
+                          const float* m, int64_t np, int32_t mass_bits, int32_t velocity_bits,
+                          int32_t* gm, int32_t* gmu, int32_t* gmv);
+/* The device sort by cell of host particles (SortTest.Sorter: Scatter.sortCount + CountingSort,
+ * SortTest.java:255-313), stable: writes the permutation (perm[d] = source index) and the starts. */
+int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm,
+                 int32_t* starts);
+
+/* ------------------------------------------------------------------ 3D particles (ParticleSimulation3) */
+typedef struct vf_mpm3 vf_mpm3;
+typedef struct vf_mpm3_prepared vf_mpm3_prepared;
+
+enum {   /* fields (Flip3.PARTICLE, Flip3.java:112-115; grid names Flip3Step.java:65-67) */
+    VF3_X = 0, VF3_Y, VF3_Z, VF3_U, VF3_V, VF3_W, VF3_M, VF3_J,
+    VF3_C00, VF3_C01, VF3_C02, VF3_C10, VF3_C11, VF3_C12, VF3_C20, VF3_C21, VF3_C22,
+    VF3_GM = 32, VF3_GMU, VF3_GMV, VF3_GMW, VF3_GU, VF3_GV, VF3_GW
+};
+
+/* ParticleSimulation3.prepare (ParticleSimulation3.java:110-139): every buffer allocated and every kernel
+ * loaded, nothing submitted; may run on any thread. nx, ny, nz >= 3; particles >= 1 (Flip3Step.java:54-56).
+ * flags: VF_EOS_TAIT, VF_WALL_STICKY(t), P2G schedule << VF_P2G_SHIFT, VF_NO_SORT. */
+int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
+                        vf_mpm3_prepared** out);
+/* Prepared.close (ParticleSimulation3.java:94-102): frees a preparation never finished. Idempotent. */
+void vf_mpm3_prepared_close(vf_mpm3_prepared* p);
+/* new ParticleSimulation3(Prepared) (ParticleSimulation3.java:181-190), on the owning thread: clears the
+ * buffers. The preparation is consumed (VF_ESTATE if already taken). */
+int32_t vf_mpm3_create(vf_mpm3_prepared* p, vf_mpm3** out);
+/* ParticleSimulation3.load (ParticleSimulation3.java:227-275): J = 1, C = 0; params = Flip3.params words (>= 6). */
+int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z, const float* u, const float* v,
+                     const float* w, const float* m, const int32_t* params, int32_t nparams);
+int32_t vf_mpm3_params(vf_mpm3* h, const int32_t* params, int32_t nparams);
+/* ParticleSimulation3.advance (ParticleSimulation3.java:291-296); with the default flags each step sorts the
+ * particles by stencil cell first. */
+int32_t vf_mpm3_advance(vf_mpm3* h, int32_t count);
+/* Passes of one step, for tests (Flip3Test runs clear+scatter alone, Flip3Test.java:90):
+ * bit 0 sort, bit 1 clear, bit 2 scatter, bit 3 grid, bit 4 advect. Does not count a step. */
+enum { VF3_PASS_SORT = 1, VF3_PASS_CLEAR = 2, VF3_PASS_SCATTER = 4, VF3_PASS_GRID = 8, VF3_PASS_ADVECT = 16 };
+int32_t vf_mpm3_run(vf_mpm3* h, uint32_t passes);
+/* Readbacks: grid() (ParticleSimulation3.java:302-304; the last scatter's m, mu, mv, mw), velocities(), and
+ * any particle field; writes of any particle field. Blocking. */
+int32_t vf_mpm3_read(vf_mpm3* h, int32_t field, float* out, int64_t n);
+int32_t vf_mpm3_write(vf_mpm3* h, int32_t field, const float* in, int64_t n);
+/* The last sort's cell starts over the brick-major stencil-cell keys, vf_mpm3_key_count()+1 words. */
+int64_t vf_mpm3_key_count(const vf_mpm3* h);
+int32_t vf_mpm3_read_starts(vf_mpm3* h, int32_t* out, int64_t n);
+/* ParticleSimulation3.finish (ParticleSimulation3.java:399-402): waits for every step submitted. */
+int32_t vf_mpm3_finish(vf_mpm3* h);
+/* ParticleSimulation3.vkBuffer(name) (ParticleSimulation3.java:377-383), as a device pointer: "gm", "gmu",
+ * "gmv", "gmw" (the last scatter's grid) or "x", "y", "z". *stride is the element stride in floats (4 for the
+ * grid, whose nodes are stored as float4 {m, mu, mv, mw}; 1 for particles). Valid until the next step;
+ * call vf_mpm3_finish before reading. VF_EINVAL for another name. */
+int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* stride);
+/* The CUDA stream (cudaStream_t) the handle's work is submitted on, for event timing by a caller. */
+void* vf_mpm3_stream(vf_mpm3* h);
+/* Change the scatter schedule (VF_P2G_*) between steps. */
+int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
+/* Nodes with mass after the last scatter (N_t in the roofline's byte count). Blocking. */
+int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out);
+int64_t vf_mpm3_steps(const vf_mpm3* h);
+int32_t vf_mpm3_on_gpu(const vf_mpm3* h);
+void vf_mpm3_destroy(vf_mpm3* h);
+
+/* ------------------------------------------------------------------ shallow water (PatchSimulation) */
+typedef struct vf_swe vf_swe;
+enum { VF_EDGE_WALL = 0, VF_EDGE_OPEN = 1 };   /* Edge.java:11-25 */
+
+/* new PatchSimulation(nx, ny, edges) (PatchSimulation.java:58-76); edges = {west, east, south, north}
+ * (Edges.java:29). nx, ny >= 1 (ShallowWater.java:167-169). */
+int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** out);
+/* PatchSimulation.load (PatchSimulation.java:92-109): the state, params = ShallowWater.params words (5);
+ * the first step's speed is measured on the host (ShallowWater.fastestWave); the clock restarts at zero. */
+int32_t vf_swe_load(vf_swe* h, const float* hcell, const float* hu, const float* hv, const int32_t* params,
+                    int32_t nparams);
+int32_t vf_swe_params(vf_swe* h, const int32_t* params, int32_t nparams);
+/* PatchSimulation.advance(ticks, maxSteps) (PatchSimulation.java:120-145) and its Advance record (33-39). */
+int32_t vf_swe_advance(vf_swe* h, int64_t ticks, int32_t max_steps, int32_t* steps, int64_t* spent_ticks,
+                       int64_t* behind_ticks);
+/* PatchSimulation.read (148-152), fastestWave (158-160), clamped (176-178), now (181-183), steps (186-188). */
+int32_t vf_swe_read(vf_swe* h, float* hcell, float* hu, float* hv);
+int32_t vf_swe_fastest_wave(vf_swe* h, double* out);
+int32_t vf_swe_clamped(vf_swe* h, int32_t* out);
+int64_t vf_swe_now(const vf_swe* h);
+int64_t vf_swe_steps(const vf_swe* h);
+/* The raw rotation, for the reference's test harness (Stepper.java:72-77, 128-130): dispatch n steps
+ * k = dispatched, dispatched+1, ... with state k%2 -> (k+1)%2, speed k%3 read / (k+1)%3 max / (k+2)%3 clear,
+ * budget k%2 -> (k+1)%2; and the budget words. */
+int32_t vf_swe_dispatch(vf_swe* h, int32_t n);
+int64_t vf_swe_dispatched(const vf_swe* h);
+int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks);
+int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks);
+/* Diagnostics.of over the current state (Diagnostics.java:43-81), reduced on the device.
+ * out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
+int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]);
+void* vf_swe_stream(vf_swe* h);
+int32_t vf_swe_on_gpu(const vf_swe* h);
+void vf_swe_destroy(vf_swe* h);
+
+/* ------------------------------------------------------------------ particle diagnostics */
+/* ParticleDiagnostics.of over a device-resident J (ParticleDiagnostics.java:126-148): out = {minDensity,
+ * maxDensity, lowDensity, highDensity, mach, courant, nonFinite}. */
+int32_t vf_mpm3_particle_diagnostics(vf_mpm3* h, double speed, double sound, double dt, double out[7]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VEXFLUID_H */

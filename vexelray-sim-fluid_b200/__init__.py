@@ -1,0 +1,645 @@
+"""vexfluid: the B200 (sm_100a) fluid step of sibarum/vexelray-sim-fluid behind its runner API.
+
+The classes mirror the reference's Java runners, method for method, over the C-ABI library
+``libvexfluid.so`` (declared in include/vexfluid.h):
+
+* ``ParticleSimulation``  -- vexelray-sim-fluid-gui/.../gui/ParticleSimulation.java (2D MLS-MPM)
+* ``ParticleSimulation3`` -- vexelray-sim-fluid-gui/.../gui/ParticleSimulation3.java (3D MLS-MPM)
+* ``PatchSimulation``     -- vexelray-sim-fluid-gui/.../gui/PatchSimulation.java (shallow water)
+
+plus the core's param builders (``Flip.params``, ``Flip3.params``, ``ShallowWater.params``) and the
+scatter schedules of ``Scatter``. Errors the reference raises as IllegalArgumentException /
+IllegalStateException are raised as ``IllegalArgumentException`` (a ValueError) and
+``IllegalStateException`` (a RuntimeError). There is no CPU fallback: without the library or a
+CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import pathlib
+import subprocess
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIBRARY = HERE / "libvexfluid.so"
+
+VF_OK, VF_EINVAL, VF_ESTATE, VF_ENOMEM, VF_ECUDA, VF_ETIMEOUT, VF_ENODEV, VF_EDEVICE = 0, -1, -2, -3, -4, -5, -6, -7
+VF_EOS_TAIT = 1
+VF_WALL_STICKY_SHIFT = 8
+VF_P2G_SHIFT = 16
+VF_NO_SORT = 1 << 20
+VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP = 0, 1, 2
+VF_SCATTER_GRID, VF_SCATTER_PRE_REDUCED, VF_SCATTER_GATHER, VF_SCATTER_SEGMENTED = 0, 1, 2, 3
+VF3_PASS_SORT, VF3_PASS_CLEAR, VF3_PASS_SCATTER, VF3_PASS_GRID, VF3_PASS_ADVECT = 1, 2, 4, 8, 16
+EDGE_WALL, EDGE_OPEN = 0, 1
+
+FIELDS2 = {"x": 0, "y": 1, "u": 2, "v": 3, "m": 4, "j": 5, "c00": 6, "c01": 7, "c10": 8, "c11": 9,
+           "gm": 16, "gmu": 17, "gmv": 18, "gu": 19, "gv": 20}
+FIELDS3 = {n: k for k, n in enumerate(("x", "y", "z", "u", "v", "w", "m", "j", "c00", "c01", "c02", "c10", "c11",
+                                       "c12", "c20", "c21", "c22"))}
+FIELDS3.update({"gm": 32, "gmu": 33, "gmv": 34, "gmw": 35, "gu": 36, "gv": 37, "gw": 38})
+
+
+class VfError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{message} (status {code})")
+        self.code = code
+
+
+class IllegalArgumentException(VfError, ValueError):
+    pass
+
+
+class IllegalStateException(VfError):
+    pass
+
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_vp = ctypes.c_void_p
+_LIB = None
+
+
+def build(quiet: bool = True) -> pathlib.Path:
+    """Compiles libvexfluid.so in place (nvcc, sm_100a)."""
+    cmd = ["make", "-s" if quiet else "", "-j8", "-C", str(HERE)]
+    subprocess.run([c for c in cmd if c], check=True)
+    return LIBRARY
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library. Raises if it has not been built: there is no fallback."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIBRARY.exists():
+        raise RuntimeError(f"libvexfluid.so is not built ({LIBRARY}); run build() first")
+    L = ctypes.CDLL(str(LIBRARY))
+    sig = {
+        "vf_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int32),
+        "vf_version": ([], ctypes.c_int32),
+        "vf_device_ok": ([], ctypes.c_int32),
+        "vf_mpm2_create": ([ctypes.c_int32] * 3 + [ctypes.c_uint32, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_mpm2_load": ([_vp] + [_f32p] * 5 + [_i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm2_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm2_advance": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm2_step": ([_vp], ctypes.c_int32),
+        "vf_mpm2_sort": ([_vp], ctypes.c_int32),
+        "vf_mpm2_read": ([_vp, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm2_write": ([_vp, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm2_read_starts": ([_vp, _i32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm2_steps": ([_vp], ctypes.c_int64),
+        "vf_mpm2_on_gpu": ([_vp], ctypes.c_int32),
+        "vf_mpm2_destroy": ([_vp], None),
+        "vf_scatter2": ([ctypes.c_int32] * 3 + [_f32p] * 5 + [ctypes.c_int64] + [_f32p] * 3, ctypes.c_int32),
+        "vf_fixed_scatter2": ([ctypes.c_int32] * 2 + [_f32p] * 5 + [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
+                              + [_i32p] * 3, ctypes.c_int32),
+        "vf_sort2": ([ctypes.c_int32] * 2 + [_f32p] * 2 + [ctypes.c_int64, _i32p, _i32p], ctypes.c_int32),
+        "vf_mpm3_prepare": ([ctypes.c_int32] * 4 + [ctypes.c_uint32, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_mpm3_prepared_close": ([_vp], None),
+        "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_mpm3_load": ([_vp] + [_f32p] * 7 + [_i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_advance": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_run": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+        "vf_mpm3_read": ([_vp, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm3_write": ([_vp, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm3_key_count": ([_vp], ctypes.c_int64),
+        "vf_mpm3_read_starts": ([_vp, _i32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm3_finish": ([_vp], ctypes.c_int32),
+        "vf_mpm3_device_ptr": ([_vp, ctypes.c_char_p, ctypes.POINTER(_vp), _i32p], ctypes.c_int32),
+        "vf_mpm3_stream": ([_vp], _vp),
+        "vf_mpm3_set_p2g": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_touched_nodes": ([_vp, _i64p], ctypes.c_int32),
+        "vf_mpm3_steps": ([_vp], ctypes.c_int64),
+        "vf_mpm3_on_gpu": ([_vp], ctypes.c_int32),
+        "vf_mpm3_destroy": ([_vp], None),
+        "vf_mpm3_particle_diagnostics": ([_vp] + [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)],
+                                         ctypes.c_int32),
+        "vf_swe_create": ([ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_swe_load": ([_vp] + [_f32p] * 3 + [_i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_advance": ([_vp, ctypes.c_int64, ctypes.c_int32, _i32p, _i64p, _i64p], ctypes.c_int32),
+        "vf_swe_read": ([_vp] + [_f32p] * 3, ctypes.c_int32),
+        "vf_swe_fastest_wave": ([_vp, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
+        "vf_swe_clamped": ([_vp, _i32p], ctypes.c_int32),
+        "vf_swe_now": ([_vp], ctypes.c_int64),
+        "vf_swe_steps": ([_vp], ctypes.c_int64),
+        "vf_swe_dispatch": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_dispatched": ([_vp], ctypes.c_int64),
+        "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_read_budget": ([_vp, ctypes.c_int32, _i32p], ctypes.c_int32),
+        "vf_swe_diagnostics": ([_vp, ctypes.c_double, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
+        "vf_swe_stream": ([_vp], _vp),
+        "vf_swe_on_gpu": ([_vp], ctypes.c_int32),
+        "vf_swe_destroy": ([_vp], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().vf_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(code: int) -> None:
+    if code == VF_OK:
+        return
+    msg = last_error()
+    if code == VF_EINVAL:
+        raise IllegalArgumentException(code, msg)
+    if code == VF_ESTATE:
+        raise IllegalStateException(code, msg)
+    raise VfError(code, msg)
+
+
+def _f32(a, n=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if n is not None and a.shape != (n,):
+        raise IllegalArgumentException(VF_EINVAL, f"expected {n} values, got shape {a.shape}")
+    return a
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(_f32p)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_i32p)
+
+
+def _words(params) -> np.ndarray:
+    p = np.asarray(params)
+    if p.dtype == np.float32:
+        return np.ascontiguousarray(p.view(np.int32))
+    return np.ascontiguousarray(p, dtype=np.int32)
+
+
+def _bits(v: float) -> int:
+    return int(np.array([v], dtype=np.float32).view(np.int32)[0])
+
+
+# ------------------------------------------------------------------------------------- params
+
+def flip_params(dt, gx, gy, bulk, rho0, sigma=0.0) -> np.ndarray:
+    """Flip.params (Flip.java:145-211): 28 words of f32 bits."""
+    if not (dt > 0) or not (bulk >= 0) or not (rho0 > 0):
+        raise IllegalArgumentException(VF_EINVAL, f"dt > 0, bulk >= 0 and rho0 > 0, got dt {dt}, bulk {bulk}, "
+                                                  f"rho0 {rho0}")
+    w = np.zeros(28, np.int32)
+    for k, v in enumerate((dt, gx, gy, bulk, rho0, sigma)):
+        w[k] = _bits(v)
+    return w
+
+
+def flip3_params(dt, gx, gy, gz, bulk, rho0, sigma=0.0) -> np.ndarray:
+    """Flip3.params (Flip3.java:89-103): 7 words of f32 bits."""
+    if not (dt > 0) or not (bulk >= 0) or not (rho0 > 0):
+        raise IllegalArgumentException(VF_EINVAL, f"dt > 0, bulk >= 0 and rho0 > 0, got dt {dt}, bulk {bulk}, "
+                                                  f"rho0 {rho0}")
+    return np.array([_bits(v) for v in (dt, gx, gy, gz, bulk, rho0, sigma)], np.int32)
+
+
+def stable_step(bulk, rho0, speed, courant) -> float:
+    """Flip.stableStep (Flip.java:214-216)."""
+    return courant / (math.sqrt(bulk / rho0) + speed)
+
+
+def swe_params(g, courant, dx, dy, dry=1e-6, allow_instability=False) -> np.ndarray:
+    """ShallowWater.params / paramsAllowingInstability (ShallowWater.java:248-271)."""
+    if not allow_instability and not (0 < courant <= 0.5):
+        raise IllegalArgumentException(VF_EINVAL, "a first-order 2D step needs a Courant number in (0, 1/2], got "
+                                       + str(courant))
+    if not courant > 0:
+        raise IllegalArgumentException(VF_EINVAL, f"a Courant number must be positive, got {courant}")
+    return np.array([_bits(v) for v in (g, courant, dx, dy, dry)], np.int32)
+
+
+TICKS_PER_SECOND = 1_000_000
+
+
+def ticks(seconds: float) -> int:
+    """ShallowWater.ticks: seconds to microsecond ticks, Math.round."""
+    return int(math.floor(seconds * TICKS_PER_SECOND + 0.5))
+
+
+def seconds(t: int) -> float:
+    return t / TICKS_PER_SECOND
+
+
+# ------------------------------------------------------------------------------------- 2D
+
+class ParticleSimulation:
+    """ParticleSimulation (ParticleSimulation.java): a 2D particle fluid in one walled box on the GPU."""
+
+    def __init__(self, nx: int, ny: int, particles: int, *, tait: bool = False, sticky: int = 0):
+        L = lib()
+        h = _vp()
+        flags = (VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT)
+        check(L.vf_mpm2_create(nx, ny, particles, flags, ctypes.byref(h)))
+        self._h = h
+        self._nx, self._ny, self._np = nx, ny, particles
+
+    def nx(self):
+        return self._nx
+
+    def ny(self):
+        return self._ny
+
+    def particles(self):
+        return self._np
+
+    def on_gpu(self) -> bool:
+        return bool(lib().vf_mpm2_on_gpu(self._h))
+
+    def load(self, x, y, u, v, m, params) -> None:
+        n = self._np
+        a = [_f32(q, n) for q in (x, y, u, v, m)]
+        w = _words(params)
+        check(lib().vf_mpm2_load(self._h, *[_fp(q) for q in a], _ip(w), len(w)))
+
+    def params(self, params) -> None:
+        w = _words(params)
+        check(lib().vf_mpm2_params(self._h, _ip(w), len(w)))
+
+    def advance(self, count: int, sort_every: int) -> None:
+        check(lib().vf_mpm2_advance(self._h, count, sort_every))
+
+    def step(self) -> None:
+        """One FlipStep.step() without counting it (the test Rig's run(step.step()))."""
+        check(lib().vf_mpm2_step(self._h))
+
+    def sort(self) -> None:
+        """One FlipStep.sort() (the test Rig's run(step.sort()))."""
+        check(lib().vf_mpm2_sort(self._h))
+
+    def read(self, name: str) -> np.ndarray:
+        f = FIELDS2[name]
+        n = self._nx * self._ny if f >= 16 else self._np
+        out = np.empty(n, np.float32)
+        check(lib().vf_mpm2_read(self._h, f, _fp(out), n))
+        return out
+
+    def write(self, name: str, values) -> None:
+        a = _f32(values, self._np)
+        check(lib().vf_mpm2_write(self._h, FIELDS2[name], _fp(a), self._np))
+
+    def grid(self):
+        return [self.read("gm"), self.read("gmu"), self.read("gmv")]
+
+    def masses(self):
+        return self.read("m")
+
+    def velocities(self):
+        return [self.read("u"), self.read("v")]
+
+    def positions(self):
+        return [self.read("x"), self.read("y")]
+
+    def compression(self, j=None):
+        if j is None:
+            return self.read("j")
+        self.write("j", j)
+
+    def starts(self) -> np.ndarray:
+        out = np.empty((self._nx - 1) * (self._ny - 1) + 1, np.int32)
+        check(lib().vf_mpm2_read_starts(self._h, _ip(out), len(out)))
+        return out
+
+    def steps(self) -> int:
+        return int(lib().vf_mpm2_steps(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_mpm2_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def scatter2(mode: int, nx: int, ny: int, x, y, u, v, m):
+    """One bilinear P2G (Scatter.kernel / preReduced / gather / segmented) of host particles."""
+    n = len(x)
+    a = [_f32(q, n) for q in (x, y, u, v, m)]
+    out = [np.zeros(nx * ny, np.float32) for _ in range(3)]
+    check(lib().vf_scatter2(mode, nx, ny, *[_fp(q) for q in a], n, *[_fp(o) for o in out]))
+    return out
+
+
+def fixed_scatter2(nx: int, ny: int, x, y, u, v, m, mass_bits: int, velocity_bits: int):
+    """FixedScatter.kernel: the bilinear P2G in wrapping i32 quanta."""
+    n = len(x)
+    a = [_f32(q, n) for q in (x, y, u, v, m)]
+    out = [np.zeros(nx * ny, np.int32) for _ in range(3)]
+    check(lib().vf_fixed_scatter2(nx, ny, *[_fp(q) for q in a], n, mass_bits, velocity_bits,
+                                  *[_ip(o) for o in out]))
+    return out
+
+
+def sort2(nx: int, ny: int, x, y):
+    """The device's stable sort by Scatter.cell: (perm, starts)."""
+    n = len(x)
+    xs, ys = _f32(x, n), _f32(y, n)
+    perm = np.empty(n, np.int32)
+    starts = np.empty((nx - 1) * (ny - 1) + 1, np.int32)
+    check(lib().vf_sort2(nx, ny, _fp(xs), _fp(ys), n, _ip(perm), _ip(starts)))
+    return perm, starts
+
+
+# ------------------------------------------------------------------------------------- 3D
+
+class Prepared:
+    """ParticleSimulation3.Prepared (ParticleSimulation3.java:51-103)."""
+
+    def __init__(self, handle, nx, ny, nz, particles):
+        self._p = handle
+        self.nx, self.ny, self.nz, self.particles = nx, ny, nz, particles
+
+    def close(self):
+        if self._p:
+            lib().vf_mpm3_prepared_close(self._p)
+            self._p = None
+
+
+class ParticleSimulation3:
+    """ParticleSimulation3 (ParticleSimulation3.java): a 3D particle fluid in one walled box on the GPU.
+
+    ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC or VF_P2G_WARP.
+    ``sort=False`` keeps the particles in load order, as the reference's Flip3Step does.
+    """
+
+    @staticmethod
+    def prepare(nx, ny, nz, particles, *, tait=False, sticky=0, schedule=VF_P2G_TILE, sort=True) -> Prepared:
+        flags = ((VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT) | (schedule << VF_P2G_SHIFT)
+                 | (0 if sort else VF_NO_SORT))
+        p = _vp()
+        check(lib().vf_mpm3_prepare(nx, ny, nz, particles, flags, ctypes.byref(p)))
+        return Prepared(p, nx, ny, nz, particles)
+
+    def __init__(self, nx_or_prepared, ny=None, nz=None, particles=None, **kw):
+        prepared = nx_or_prepared if isinstance(nx_or_prepared, Prepared) else \
+            ParticleSimulation3.prepare(nx_or_prepared, ny, nz, particles, **kw)
+        h = _vp()
+        if not prepared._p:
+            raise IllegalStateException(VF_ESTATE, "this preparation has already been made a simulation, or closed")
+        check(lib().vf_mpm3_create(prepared._p, ctypes.byref(h)))
+        prepared._p = None
+        self._h = h
+        self._nx, self._ny, self._nz, self._np = prepared.nx, prepared.ny, prepared.nz, prepared.particles
+        self._nominal = 0.0
+
+    def nx(self):
+        return self._nx
+
+    def ny(self):
+        return self._ny
+
+    def nz(self):
+        return self._nz
+
+    def particles(self):
+        return self._np
+
+    def on_gpu(self) -> bool:
+        return bool(lib().vf_mpm3_on_gpu(self._h))
+
+    def load(self, at, velocity, mass, params) -> None:
+        n = self._np
+        a = [_f32(q, n) for q in (at[0], at[1], at[2], velocity[0], velocity[1], velocity[2], mass)]
+        w = _words(params)
+        check(lib().vf_mpm3_load(self._h, *[_fp(q) for q in a], _ip(w), len(w)))
+        pos = a[6][a[6] > 0]
+        self._nominal = float(pos.min()) if len(pos) else 0.0
+
+    def params(self, params) -> None:
+        w = _words(params)
+        check(lib().vf_mpm3_params(self._h, _ip(w), len(w)))
+
+    def advance(self, count: int) -> None:
+        check(lib().vf_mpm3_advance(self._h, count))
+
+    def run(self, passes: int) -> None:
+        """Passes of one step (VF3_PASS_*), as the test Rig runs a sub-list of Flip3Step.step()."""
+        check(lib().vf_mpm3_run(self._h, passes))
+
+    def read(self, name: str) -> np.ndarray:
+        f = FIELDS3[name]
+        n = self._nx * self._ny * self._nz if f >= 32 else self._np
+        out = np.empty(n, np.float32)
+        check(lib().vf_mpm3_read(self._h, f, _fp(out), n))
+        return out
+
+    def write(self, name: str, values) -> None:
+        a = _f32(values, self._np)
+        check(lib().vf_mpm3_write(self._h, FIELDS3[name], _fp(a), self._np))
+
+    def grid(self):
+        return [self.read("gm"), self.read("gmu"), self.read("gmv"), self.read("gmw")]
+
+    def velocities(self):
+        return [self.read("u"), self.read("v"), self.read("w")]
+
+    def positions(self):
+        return [self.read("x"), self.read("y"), self.read("z")]
+
+    def compression(self):
+        """ParticleSimulation3.compression (ParticleSimulation3.java:312-333): J of the particles holding at least
+        half the smallest loaded mass."""
+        j = self.read("j")
+        m = self.read("m")
+        keep = m >= 0.5 * self._nominal
+        return j if keep.all() else j[keep]
+
+    def key_count(self) -> int:
+        return int(lib().vf_mpm3_key_count(self._h))
+
+    def starts(self) -> np.ndarray:
+        out = np.empty(self.key_count() + 1, np.int32)
+        check(lib().vf_mpm3_read_starts(self._h, _ip(out), len(out)))
+        return out
+
+    def finish(self) -> None:
+        check(lib().vf_mpm3_finish(self._h))
+
+    def device_ptr(self, name: str):
+        p = _vp()
+        stride = ctypes.c_int32()
+        check(lib().vf_mpm3_device_ptr(self._h, name.encode(), ctypes.byref(p), ctypes.byref(stride)))
+        return p.value, stride.value
+
+    def stream(self) -> int:
+        return lib().vf_mpm3_stream(self._h)
+
+    def set_schedule(self, schedule: int) -> None:
+        check(lib().vf_mpm3_set_p2g(self._h, schedule))
+
+    def touched_nodes(self) -> int:
+        out = ctypes.c_int64()
+        check(lib().vf_mpm3_touched_nodes(self._h, ctypes.byref(out)))
+        return out.value
+
+    def particle_diagnostics(self, speed, sound, dt):
+        out = (ctypes.c_double * 7)()
+        check(lib().vf_mpm3_particle_diagnostics(self._h, speed, sound, dt, out))
+        return list(out)
+
+    def steps(self) -> int:
+        return int(lib().vf_mpm3_steps(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_mpm3_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------- shallow water
+
+@dataclass(frozen=True)
+class Advance:
+    """PatchSimulation.Advance (PatchSimulation.java:33-39)."""
+    steps: int
+    spent_ticks: int
+    behind_ticks: int
+
+    def mean_step(self) -> float:
+        return 0.0 if self.steps == 0 else seconds(self.spent_ticks) / self.steps
+
+
+class PatchSimulation:
+    """PatchSimulation (PatchSimulation.java): one shallow-water patch on the GPU, advanced by slices of time."""
+
+    def __init__(self, nx: int, ny: int, edges: Sequence[int] = (EDGE_WALL,) * 4):
+        e = np.ascontiguousarray(edges, np.int32)
+        if e.shape != (4,):
+            raise IllegalArgumentException(VF_EINVAL, "every side of a patch needs an edge")
+        h = _vp()
+        check(lib().vf_swe_create(nx, ny, _ip(e), ctypes.byref(h)))
+        self._h = h
+        self._nx, self._ny = nx, ny
+
+    def nx(self):
+        return self._nx
+
+    def ny(self):
+        return self._ny
+
+    def on_gpu(self) -> bool:
+        return bool(lib().vf_swe_on_gpu(self._h))
+
+    def load(self, h, hu, hv, params) -> None:
+        n = self._nx * self._ny
+        a = [_f32(q, n) for q in (h, hu, hv)]
+        w = _words(params)
+        check(lib().vf_swe_load(self._h, *[_fp(q) for q in a], _ip(w), len(w)))
+
+    def params(self, params) -> None:
+        w = _words(params)
+        check(lib().vf_swe_params(self._h, _ip(w), len(w)))
+
+    def advance(self, ticks_: int, max_steps: int) -> Advance:
+        steps = ctypes.c_int32()
+        spent = ctypes.c_int64()
+        behind = ctypes.c_int64()
+        check(lib().vf_swe_advance(self._h, ticks_, max_steps, ctypes.byref(steps), ctypes.byref(spent),
+                                   ctypes.byref(behind)))
+        return Advance(steps.value, spent.value, behind.value)
+
+    def read(self):
+        n = self._nx * self._ny
+        out = [np.empty(n, np.float32) for _ in range(3)]
+        check(lib().vf_swe_read(self._h, *[_fp(o) for o in out]))
+        return out
+
+    def fastest_wave(self) -> float:
+        v = ctypes.c_double()
+        check(lib().vf_swe_fastest_wave(self._h, ctypes.byref(v)))
+        return v.value
+
+    def allowed_step(self, courant, dx, dy) -> float:
+        f = self.fastest_wave()
+        return courant * min(dx, dy) / f if f > 0 else 0.0
+
+    def clamped(self) -> int:
+        v = ctypes.c_int32()
+        check(lib().vf_swe_clamped(self._h, ctypes.byref(v)))
+        return v.value
+
+    def now(self) -> int:
+        return int(lib().vf_swe_now(self._h))
+
+    def steps(self) -> int:
+        return int(lib().vf_swe_steps(self._h))
+
+    # the raw rotation, for the reference test harness (Stepper.java)
+    def dispatch(self, n: int = 1) -> None:
+        check(lib().vf_swe_dispatch(self._h, n))
+
+    def dispatched(self) -> int:
+        return int(lib().vf_swe_dispatched(self._h))
+
+    def write_budget(self, slot: int, ticks_: int) -> None:
+        check(lib().vf_swe_write_budget(self._h, slot, ticks_))
+
+    def read_budget(self, slot: int) -> int:
+        v = ctypes.c_int32()
+        check(lib().vf_swe_read_budget(self._h, slot, ctypes.byref(v)))
+        return v.value
+
+    def diagnostics(self, dt: float):
+        out = (ctypes.c_double * 9)()
+        check(lib().vf_swe_diagnostics(self._h, dt, out))
+        return list(out)
+
+    def stream(self) -> int:
+        return lib().vf_swe_stream(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_swe_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

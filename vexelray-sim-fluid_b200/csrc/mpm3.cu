@@ -1,0 +1,552 @@
+// mpm3.cu -- the vf_mpm3_* C-ABI: ParticleSimulation3 (vexelray-sim-fluid-gui/.../gui/
+// ParticleSimulation3.java) over Flip3Step's pass list (Flip3Step.java:81-118), on one CUDA stream.
+//
+// One step, with the default flags (sort every step, tiled scatter):
+//   [sort]    brick scan -> cell scan -> permute -> stable fix-up       (counts from the last G2P)
+//   clear     the node windows the scatter two steps ago touched in this grid buffer
+//   scatter   k_p2g3_tile  (or k_p2g3_atomic / k_p2g3_warp after a dense clear)
+//   grid      fused into k_g2p3_tile (or k_grid3_dense for the other schedules)
+//   advect    k_g2p3_tile  gathers each particle through the sort's permutation, writes it to its
+//             sorted slot in the other particle set, and counts its new key for the next sort
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "mpm3_kernels.cuh"
+
+using namespace vf;
+
+struct vf_mpm3 {
+    int nx, ny, nz, np;
+    uint32_t flags;
+    int p2g;
+    bool sort;
+    Dims3 d;
+    int nbricks;
+    int64_t nkeys, nodes, stride;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer part[2];
+    int cur = 0;
+    DeviceBuffer key, rank, perm;
+    DeviceBuffer cell_count, cell_start;
+    DeviceBuffer brick_count, brick_start;
+    DeviceBuffer active[2];   // the non-empty bricks of the step that scattered into grid[g]
+    DeviceBuffer n_active;    // int[2]
+    DeviceBuffer grid[2];
+    DeviceBuffer vel;
+    DeviceBuffer params;
+    DeviceBuffer status;
+    DeviceBuffer scratch;     // readouts
+    Params3 hparams{};
+    int64_t steps = 0;
+    int64_t passes_run = 0;   // steps run through vf_mpm3_run / advance, for grid parity
+    int grid_last = 1;        // the grid buffer the last scatter wrote
+    // what each grid buffer needs before the next scatter into it: 0 clean, 1 sparse (clear the
+    // windows of active[g]), 2 dense (memset)
+    int grid_dirty[2] = {0, 0};
+    bool counted = false;     // cell/brick counts and key/rank hold the current positions' keys
+    bool sorted_valid = false;
+    bool loaded = false;
+};
+
+struct vf_mpm3_prepared {
+    vf_mpm3* sim = nullptr;
+    bool taken = false;
+};
+
+namespace {
+
+int32_t upload_params(vf_mpm3* h, const int32_t* params, int32_t nparams) {
+    VF_REQUIRE(params && nparams >= 6, VF_EINVAL, "Flip3.params has at least 6 words, got %d", nparams);
+    float w[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 7 && k < nparams; k++) w[k] = bits_to_float(params[k]);
+    // Flip3.params refuses these (Flip3.java:98-101)
+    VF_REQUIRE(w[0] > 0 && w[4] >= 0 && w[5] > 0, VF_EINVAL,
+               "dt > 0, bulk >= 0 and rho0 > 0, got dt %g, bulk %g, rho0 %g", w[0], w[4], w[5]);
+    Params3 p;
+    p.dt = w[0];
+    p.gx = w[1];
+    p.gy = w[2];
+    p.gz = w[3];
+    p.bulk = w[4];
+    p.rho0 = w[5];
+    p.sigma = w[6];
+    p.tait = (h->flags & VF_EOS_TAIT) ? 1 : 0;
+    p.sticky = (int)((h->flags & VF_WALL_STICKY_MASK) >> VF_WALL_STICKY_SHIFT);
+    h->hparams = p;
+    VF_TRY_CUDA(cudaMemcpyAsync(h->params.ptr, &p, sizeof p, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+Step3 make_step(vf_mpm3* h) {
+    Step3 s{};
+    s.out = h->part[h->cur].as<float>();
+    s.in = s.out;
+    s.stride = h->stride;
+    s.np = h->np;
+    s.perm = nullptr;
+    s.vel = h->vel.as<float4>();
+    s.params = h->params.as<Params3>();
+    s.d = h->d;
+    s.status = h->status.as<uint32_t>();
+    s.key = h->key.as<int>();
+    s.rank = h->rank.as<int>();
+    s.cell_count = h->cell_count.as<int>();
+    s.brick_count = h->brick_count.as<int>();
+    s.cell_start = h->cell_start.as<int>();
+    s.brick_start = h->brick_start.as<int>();
+    s.nkeys = h->nkeys;
+    s.nbricks = h->nbricks;
+    return s;
+}
+
+int persistent_blocks(int per_sm) { return sm_count() * per_sm; }
+
+// Zero the counts so the next count pass starts clean (after positions changed under the
+// counts of a G2P that counted ahead).
+int32_t reset_counts(vf_mpm3* h) {
+    VF_TRY_CUDA(cudaMemsetAsync(h->cell_count.ptr, 0, h->cell_count.bytes, h->stream));
+    VF_TRY_CUDA(cudaMemsetAsync(h->brick_count.ptr, 0, h->brick_count.bytes, h->stream));
+    h->counted = false;
+    return VF_OK;
+}
+
+// The sort passes, leaving perm = sorted slot -> particle of the current set. `g` is the grid
+// buffer this step scatters into; its brick list is rebuilt here (after its old windows are cleared).
+int32_t run_sort(vf_mpm3* h, int g, bool will_scatter) {
+    Step3 s = make_step(h);
+    if (!h->counted) {
+        k_key_count3<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+        VF_CHECK_LAUNCH();
+    }
+    // the old windows of grid[g] must be cleared before its brick list is overwritten; a sort with
+    // no scatter after it leaves the grid alone and marks it for a dense clear instead
+    if (h->grid_dirty[g] == 1 && !will_scatter) h->grid_dirty[g] = 2;
+    if (h->grid_dirty[g] == 1) {
+        s.grid = h->grid[g].as<float4>();
+        s.active = h->active[g].as<int>();
+        s.n_active = h->n_active.as<int>() + g;
+        k_clear_bricks3<<<persistent_blocks(8), 256, 0, h->stream>>>(s);
+        VF_CHECK_LAUNCH();
+        h->grid_dirty[g] = 0;
+    }
+    int* active = h->active[g].as<int>();
+    int* n_active = h->n_active.as<int>() + g;
+    k_brick_scan<<<1, 1024, 0, h->stream>>>(h->brick_count.as<int>(), h->brick_start.as<int>(), active, n_active,
+                                           h->nbricks);
+    VF_CHECK_LAUNCH();
+    k_cell_scan<<<persistent_blocks(4), 512, 0, h->stream>>>(h->cell_count.as<int>(), h->cell_start.as<int>(),
+                                                          h->brick_start.as<int>(), active, n_active);
+    VF_CHECK_LAUNCH();
+    k_permute<<<div_up(h->np, 256), 256, 0, h->stream>>>(h->key.as<int>(), h->rank.as<int>(),
+                                                          h->cell_start.as<int>(), h->perm.as<int>(), h->np,
+                                                          h->status.as<uint32_t>());
+    VF_CHECK_LAUNCH();
+    k_fixup_bricks<<<persistent_blocks(2), 512, 12288 * sizeof(int), h->stream>>>(
+        h->perm.as<int>(), h->cell_start.as<int>(), h->brick_start.as<int>(), active, n_active);
+    VF_CHECK_LAUNCH();
+    h->counted = false;
+    h->sorted_valid = true;
+    return VF_OK;
+}
+
+// One step's passes. mask selects them (VF3_PASS_*). The grid buffer alternates per step.
+int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
+    const int g = (int)(h->passes_run & 1);
+    const bool sort = (mask & VF3_PASS_SORT) && h->sort;
+    const bool tile = h->p2g == VF_P2G_TILE && sort;
+    if ((mask & VF3_PASS_ADVECT) && h->counted && !sort) {
+        // counts made ahead for positions this advect is about to move, and no sort to consume them
+        int32_t rc = reset_counts(h);
+        if (rc) return rc;
+    }
+    if (sort) {
+        int32_t rc = run_sort(h, g, (mask & VF3_PASS_SCATTER) != 0);
+        if (rc) return rc;
+    }
+    Step3 s = make_step(h);
+    s.grid = h->grid[g].as<float4>();
+    s.active = h->active[g].as<int>();
+    s.n_active = h->n_active.as<int>() + g;
+    if (sort) {
+        s.perm = h->perm.as<int>();
+        s.out = h->part[h->cur ^ 1].as<float>();
+    }
+    if (mask & VF3_PASS_CLEAR) {
+        if (tile) {
+            if (h->grid_dirty[g] == 2) VF_TRY_CUDA(cudaMemsetAsync(s.grid, 0, h->grid[g].bytes, h->stream));
+            // a sparse-dirty buffer was cleared by run_sort before its list was replaced
+        } else {
+            VF_TRY_CUDA(cudaMemsetAsync(s.grid, 0, h->grid[g].bytes, h->stream));
+        }
+        h->grid_dirty[g] = 0;
+    }
+    if (mask & VF3_PASS_SCATTER) {
+        if (tile) {
+            k_p2g3_tile<<<persistent_blocks(1), 256, 0, h->stream>>>(s);
+        } else if (h->p2g == VF_P2G_WARP) {
+            k_p2g3_warp<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+        } else {
+            k_p2g3_atomic<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+        }
+        VF_CHECK_LAUNCH();
+        h->grid_dirty[g] = tile ? 1 : 2;
+        h->grid_last = g;
+    }
+    if (mask & VF3_PASS_ADVECT) {
+        s.count_next = count_next ? 1 : 0;
+        if (tile) {
+            k_g2p3_tile<<<persistent_blocks(2), 256, 0, h->stream>>>(s);
+            VF_CHECK_LAUNCH();
+        } else {
+            k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
+            VF_CHECK_LAUNCH();
+            k_g2p3<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+            VF_CHECK_LAUNCH();
+        }
+        if (sort) h->cur ^= 1;
+        h->counted = count_next;
+    } else if (mask & VF3_PASS_GRID) {
+        k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
+        VF_CHECK_LAUNCH();
+    }
+    if (sort && !(mask & VF3_PASS_ADVECT)) {
+        // the particles were not moved to their sorted slots; apply the permutation as a copy
+        k_gather_fields<<<div_up(h->np, 256), 256, 0, h->stream>>>(s.in, s.out, s.perm, h->np, h->stride, NF3);
+        VF_CHECK_LAUNCH();
+        h->cur ^= 1;
+    }
+    if (mask & VF3_PASS_SCATTER) h->passes_run++;
+    return VF_OK;
+}
+
+int32_t check_status(vf_mpm3* h) {
+    uint32_t st = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&st, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    if (st) {
+        VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+        set_error("a kernel flagged device status 0x%x (1 index out of range, 2 wait timeout, 4 sort rank)", st);
+        return VF_EDEVICE;
+    }
+    return VF_OK;
+}
+
+int32_t field_pointer(vf_mpm3* h, int32_t field, float** ptr, int64_t* n) {
+    if (field >= VF3_X && field <= VF3_C22) {
+        *ptr = h->part[h->cur].as<float>() + (int64_t)field * h->stride;
+        *n = h->np;
+        return VF_OK;
+    }
+    set_error("no particle field %d", field);
+    return VF_EINVAL;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
+                        vf_mpm3_prepared** out) {
+    VF_REQUIRE(out, VF_EINVAL, "out is null");
+    *out = nullptr;
+    VF_REQUIRE(particles >= 1, VF_EINVAL, "a step needs particles, got %d", particles);
+    VF_REQUIRE(nx >= 3 && ny >= 3 && nz >= 3, VF_EINVAL, "a 3D grid needs at least three nodes each way, got %d x %d x %d",
+               nx, ny, nz);
+    int p2g = (int)((flags & VF_P2G_MASK) >> VF_P2G_SHIFT);
+    VF_REQUIRE(p2g <= VF_P2G_WARP, VF_EINVAL, "no scatter schedule %d", p2g);
+    int32_t rc = require_device();
+    if (rc) return rc;
+    vf_mpm3* h = new vf_mpm3();
+    h->nx = nx;
+    h->ny = ny;
+    h->nz = nz;
+    h->np = particles;
+    h->flags = flags;
+    h->p2g = p2g;
+    h->sort = !(flags & VF_NO_SORT);
+    h->d.nx = nx;
+    h->d.ny = ny;
+    h->d.nz = nz;
+    h->d.nbx = (nx - 2 + BRICK - 1) / BRICK;
+    h->d.nby = (ny - 2 + BRICK - 1) / BRICK;
+    h->d.nbz = (nz - 2 + BRICK - 1) / BRICK;
+    h->nbricks = h->d.nbx * h->d.nby * h->d.nbz;
+    h->nkeys = (int64_t)h->nbricks * 512;
+    h->nodes = (int64_t)nx * ny * nz;
+    h->stride = ((int64_t)particles + 63) / 64 * 64;
+    auto fail = [&](int32_t code) {
+        delete h;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("cudaStreamCreate failed");
+        return fail(VF_ECUDA);
+    }
+    size_t pbytes = (size_t)h->stride * NF3 * sizeof(float);
+    if ((rc = h->part[0].alloc(pbytes)) || (rc = h->part[1].alloc(pbytes)) ||
+        (rc = h->key.alloc((size_t)particles * 4)) || (rc = h->rank.alloc((size_t)particles * 4)) ||
+        (rc = h->perm.alloc((size_t)particles * 4)) || (rc = h->cell_count.alloc((size_t)h->nkeys * 4)) ||
+        (rc = h->cell_start.alloc((size_t)(h->nkeys + 1) * 4)) ||
+        (rc = h->brick_count.alloc((size_t)h->nbricks * 4)) ||
+        (rc = h->brick_start.alloc((size_t)(h->nbricks + 1) * 4)) ||
+        (rc = h->active[0].alloc((size_t)h->nbricks * 4)) || (rc = h->active[1].alloc((size_t)h->nbricks * 4)) ||
+        (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc((size_t)h->nodes * 16)) ||
+        (rc = h->grid[1].alloc((size_t)h->nodes * 16)) || (rc = h->vel.alloc((size_t)h->nodes * 16)) ||
+        (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)))
+        return fail(rc);
+    vf_mpm3_prepared* p = new vf_mpm3_prepared();
+    p->sim = h;
+    *out = p;
+    return VF_OK;
+}
+
+void vf_mpm3_prepared_close(vf_mpm3_prepared* p) {
+    if (!p) return;
+    if (!p->taken && p->sim) {
+        vf_mpm3_destroy(p->sim);
+    }
+    p->sim = nullptr;
+    p->taken = true;
+    delete p;
+}
+
+int32_t vf_mpm3_create(vf_mpm3_prepared* p, vf_mpm3** out) {
+    VF_REQUIRE(p && out, VF_EINVAL, "null argument");
+    VF_REQUIRE(!p->taken && p->sim, VF_ESTATE, "this preparation has already been made a simulation, or closed");
+    vf_mpm3* h = p->sim;
+    p->taken = true;
+    p->sim = nullptr;
+    delete p;
+    // ParticleSimulation3(Prepared) clears every buffer (runner.clear(), ParticleSimulation3.java:189)
+    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->rank, &h->perm, &h->cell_count, &h->cell_start,
+                            &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
+                            &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch}) {
+        if (cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream) != cudaSuccess) {
+            set_error("clearing buffers failed");
+            vf_mpm3_destroy(h);
+            return VF_ECUDA;
+        }
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        set_error("clearing buffers failed");
+        vf_mpm3_destroy(h);
+        return VF_ECUDA;
+    }
+    *out = h;
+    return VF_OK;
+}
+
+int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z, const float* u, const float* v,
+                     const float* w, const float* m, const int32_t* params, int32_t nparams) {
+    VF_REQUIRE(h && x && y && z && u && v && w && m, VF_EINVAL, "null argument");
+    int32_t rc = upload_params(h, params, nparams);
+    if (rc) return rc;
+    float* base = h->part[h->cur].as<float>();
+    const float* src[7] = {x, y, z, u, v, w, m};
+    for (int f = 0; f < 7; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src[f], (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    std::vector<float> ones((size_t)h->np, 1.0f);
+    VF_TRY_CUDA(cudaMemcpyAsync(base + J * h->stride, ones.data(), (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaMemsetAsync(base + C00 * h->stride, 0, (size_t)9 * h->stride * 4, h->stream));
+    rc = reset_counts(h);
+    if (rc) return rc;
+    VF_TRY_CUDA(cudaMemsetAsync(h->grid[0].ptr, 0, h->grid[0].bytes, h->stream));
+    VF_TRY_CUDA(cudaMemsetAsync(h->grid[1].ptr, 0, h->grid[1].bytes, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    h->grid_dirty[0] = h->grid_dirty[1] = 0;
+    h->steps = 0;
+    h->loaded = true;
+    return VF_OK;
+}
+
+int32_t vf_mpm3_params(vf_mpm3* h, const int32_t* params, int32_t nparams) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    return upload_params(h, params, nparams);
+}
+
+int32_t vf_mpm3_advance(vf_mpm3* h, int32_t count) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(count >= 0, VF_EINVAL, "count must be >= 0, got %d", count);
+    for (int k = 0; k < count; k++) {
+        int32_t rc = run_passes(h, VF3_PASS_SORT | VF3_PASS_CLEAR | VF3_PASS_SCATTER | VF3_PASS_GRID | VF3_PASS_ADVECT,
+                                h->sort);
+        if (rc) return rc;
+        h->steps++;
+    }
+    return VF_OK;
+}
+
+int32_t vf_mpm3_run(vf_mpm3* h, uint32_t passes) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    int32_t rc = run_passes(h, passes, false);
+    if (rc) return rc;
+    return check_status(h);
+}
+
+int32_t vf_mpm3_read(vf_mpm3* h, int32_t field, float* out, int64_t n) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    if (field >= VF3_GM && field <= VF3_GW) {
+        VF_REQUIRE(n == h->nodes, VF_EINVAL, "grid fields hold %lld floats, got %lld", (long long)h->nodes, (long long)n);
+        float* tmp = nullptr;
+        VF_TRY_CUDA(cudaMallocAsync((void**)&tmp, (size_t)h->nodes * 4, h->stream));
+        const float4* src = h->grid[h->grid_last].as<float4>();
+        int comp = field - VF3_GM;
+        if (field >= VF3_GU) {
+            Step3 s = make_step(h);
+            s.grid = h->grid[h->grid_last].as<float4>();
+            k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
+            VF_CHECK_LAUNCH();
+            src = h->vel.as<float4>();
+            comp = field - VF3_GU;
+        }
+        k_unpack_grid3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(src, tmp, h->nodes, comp);
+        VF_CHECK_LAUNCH();
+        VF_TRY_CUDA(cudaMemcpyAsync(out, tmp, (size_t)h->nodes * 4, cudaMemcpyDeviceToHost, h->stream));
+        VF_TRY_CUDA(cudaFreeAsync(tmp, h->stream));
+        VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+        return check_status(h);
+    }
+    float* ptr;
+    int64_t len;
+    int32_t rc = field_pointer(h, field, &ptr, &len);
+    if (rc) return rc;
+    VF_REQUIRE(n == len, VF_EINVAL, "particle fields hold %lld floats, got %lld", (long long)len, (long long)n);
+    VF_TRY_CUDA(cudaMemcpyAsync(out, ptr, (size_t)len * 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
+int32_t vf_mpm3_write(vf_mpm3* h, int32_t field, const float* in, int64_t n) {
+    VF_REQUIRE(h && in, VF_EINVAL, "null argument");
+    float* ptr;
+    int64_t len;
+    int32_t rc = field_pointer(h, field, &ptr, &len);
+    if (rc) return rc;
+    VF_REQUIRE(n == len, VF_EINVAL, "particle fields hold %lld floats, got %lld", (long long)len, (long long)n);
+    VF_TRY_CUDA(cudaMemcpyAsync(ptr, in, (size_t)len * 4, cudaMemcpyHostToDevice, h->stream));
+    if (field <= VF3_Z && h->counted) {
+        rc = reset_counts(h);
+        if (rc) return rc;
+    }
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int64_t vf_mpm3_key_count(const vf_mpm3* h) { return h ? h->nkeys : 0; }
+
+int32_t vf_mpm3_read_starts(vf_mpm3* h, int32_t* out, int64_t n) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    VF_REQUIRE(n == h->nkeys + 1, VF_EINVAL, "starts hold %lld words", (long long)(h->nkeys + 1));
+    VF_REQUIRE(h->sorted_valid, VF_ESTATE, "no sort has run");
+    int* tmp = nullptr;
+    VF_TRY_CUDA(cudaMallocAsync((void**)&tmp, (size_t)n * 4, h->stream));
+    k_dense_starts3<<<div_up(n, 256), 256, 0, h->stream>>>(h->cell_start.as<int>(), h->brick_start.as<int>(), tmp,
+                                                            h->nkeys, h->np);
+    VF_CHECK_LAUNCH();
+    VF_TRY_CUDA(cudaMemcpyAsync(out, tmp, (size_t)n * 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaFreeAsync(tmp, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int32_t vf_mpm3_finish(vf_mpm3* h) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
+int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* stride) {
+    VF_REQUIRE(h && name && ptr && stride, VF_EINVAL, "null argument");
+    static const char* grid_names[4] = {"gm", "gmu", "gmv", "gmw"};
+    for (int k = 0; k < 4; k++)
+        if (!strcmp(name, grid_names[k])) {
+            *ptr = h->grid[h->grid_last].as<float>() + k;
+            *stride = 4;
+            return VF_OK;
+        }
+    static const char* part_names[3] = {"x", "y", "z"};
+    for (int k = 0; k < 3; k++)
+        if (!strcmp(name, part_names[k])) {
+            *ptr = h->part[h->cur].as<float>() + (int64_t)k * h->stride;
+            *stride = 1;
+            return VF_OK;
+        }
+    set_error("no buffer named '%s'; it has gm, gmu, gmv, gmw, x, y, z", name);
+    return VF_EINVAL;
+}
+
+void* vf_mpm3_stream(vf_mpm3* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(schedule >= VF_P2G_TILE && schedule <= VF_P2G_WARP, VF_EINVAL, "no scatter schedule %d", schedule);
+    if (schedule == VF_P2G_TILE && h->p2g != VF_P2G_TILE) {
+        // the dense pipeline leaves both grids dense-dirty
+        for (int g = 0; g < 2; g++)
+            if (h->grid_dirty[g]) h->grid_dirty[g] = 2;
+    }
+    h->p2g = schedule;
+    return VF_OK;
+}
+
+int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    unsigned long long* c = h->scratch.as<unsigned long long>();
+    VF_TRY_CUDA(cudaMemsetAsync(c, 0, 8, h->stream));
+    k_touched3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(h->grid[h->grid_last].as<float4>(), h->nodes, c);
+    VF_CHECK_LAUNCH();
+    unsigned long long v = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&v, c, 8, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    *out = (int64_t)v;
+    return VF_OK;
+}
+
+// ParticleDiagnostics.of (ParticleDiagnostics.java:126-148) over the device-resident J: the reference
+// reads J back and reduces on the host; so does this (percentiles need the sorted values).
+int32_t vf_mpm3_particle_diagnostics(vf_mpm3* h, double speed, double sound, double dt, double out[7]) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    std::vector<float> j((size_t)h->np);
+    VF_TRY_CUDA(cudaMemcpyAsync(j.data(), h->part[h->cur].as<float>() + (int64_t)J * h->stride, (size_t)h->np * 4,
+                                cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<float> valid;
+    valid.reserve(j.size());
+    for (float v : j)
+        if (std::isfinite(v) && v > 0) valid.push_back(v);
+    const int64_t n = (int64_t)valid.size();
+    out[4] = speed / sound;
+    out[5] = (speed + sound) * dt;
+    out[6] = (double)(h->np - n);
+    if (n == 0) {
+        out[0] = out[1] = out[2] = out[3] = 0;
+        return VF_OK;
+    }
+    std::sort(valid.begin(), valid.end());
+    auto pct = [&](double p) { int64_t k = (int64_t)(p * n); return k < n - 1 ? k : n - 1; };
+    out[0] = 1.0 / valid[n - 1];
+    out[1] = 1.0 / valid[0];
+    out[2] = 1.0 / valid[pct(0.99)];
+    out[3] = 1.0 / valid[pct(0.01)];
+    return VF_OK;
+}
+
+int64_t vf_mpm3_steps(const vf_mpm3* h) { return h ? h->steps : 0; }
+
+int32_t vf_mpm3_on_gpu(const vf_mpm3* h) { return h ? 1 : 0; }
+
+void vf_mpm3_destroy(vf_mpm3* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->rank, &h->perm, &h->cell_count, &h->cell_start,
+                            &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
+                            &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch})
+        b->release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"

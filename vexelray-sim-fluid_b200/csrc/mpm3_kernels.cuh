@@ -1,0 +1,140 @@
+// mpm3_kernels.cuh -- the 3D MLS-MPM/APIC step's kernels (Flip3.java), for sm_100a.
+//
+// Layout in HBM:
+//   particles  two buffer sets (ping-pong), each 17 SoA f32 fields of `stride` floats:
+//              x y z u v w m j c00 c01 c02 c10 c11 c12 c20 c21 c22   (Flip3.PARTICLE order)
+//   grid       float4 per node {m, mu, mv, mw}, node (k*ny + j)*nx + i, two buffers (one per step
+//              parity, so the last scatter stays readable while the next one accumulates)
+//   velocity   float4 per node {u, v, w, 0} (dense pipeline only; the tiled G2P computes the
+//              grid update into shared memory and never writes velocities to HBM)
+//   sort       key/rank/perm per particle; cell counts/starts over the brick-major keys; brick
+//              counts/starts and the list of non-empty bricks
+#pragma once
+
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace vf {
+
+enum Field3 { X = 0, Y, Z, U, V, W, M, J, C00, C01, C02, C10, C11, C12, C20, C21, C22, NF3 };
+
+struct Dims3 {
+    int nx, ny, nz;
+    int nbx, nby, nbz;   // bricks of 8^3 stencil cells per axis
+};
+
+// Device copy of Flip3.params (Flip3.java:55-64) plus the physics options.
+struct Params3 {
+    float dt, gx, gy, gz, bulk, rho0, sigma;
+    int tait;     // VF_EOS_TAIT
+    int sticky;   // wall thickness in nodes; 0 = the reference's wall ring
+};
+
+constexpr float EMPTY3 = 1e-9f;    // Flip3.java:71
+constexpr float J_BOUND3 = 10.0f;  // Flip3.java:74
+constexpr int BRICK = 8;
+constexpr int WIN = BRICK + 2;                 // nodes per axis a brick's particles reach
+constexpr int WIN3 = WIN * WIN * WIN;          // 1000
+
+// Stencil3.of (Flip3.java:664-679): cell in [0, n-3], offset in [1/2, 3/2].
+__device__ __forceinline__ void stencil_axis(float at, int size, int& cell, float& off) {
+    float x = clampf(at, 0.5f, (float)size - 1.5f);
+    cell = (int)fminf(__fsub_rn(x, 0.5f), (float)(size - 3));
+    off = __fsub_rn(x, (float)cell);
+}
+
+// The brick-major key of a stencil cell (see oracle/mpm3.c or_key3).
+__device__ __forceinline__ int key3_of_cell(int cx, int cy, int cz, const Dims3& d) {
+    int brick = ((cz >> 3) * d.nby + (cy >> 3)) * d.nbx + (cx >> 3);
+    int local = ((cz & 7) * 8 + (cy & 7)) * 8 + (cx & 7);
+    return brick * 512 + local;
+}
+
+__device__ __forceinline__ int key3_of(float x, float y, float z, const Dims3& d) {
+    int c[3];
+    float o;
+    stencil_axis(x, d.nx, c[0], o);
+    stencil_axis(y, d.ny, c[1], o);
+    stencil_axis(z, d.nz, c[2], o);
+    return key3_of_cell(c[0], c[1], c[2], d);
+}
+
+// The grid update of one node (Flip3.grid, Flip3.java:267-311): momentum over mass plus a step of
+// gravity, zero for an empty node; the wall ring drops the velocity into the wall, or a sticky
+// wall of `sticky` nodes stops it.
+__device__ __forceinline__ float3 grid_velocity(float4 g, int i, int j, int k, const Dims3& d, const Params3& p) {
+    float v[3] = {0.0f, 0.0f, 0.0f};
+    const float mass = g.x;
+    if (mass > EMPTY3) {
+        v[0] = __fadd_rn(__fdiv_rn(g.y, mass), __fmul_rn(p.dt, p.gx));
+        v[1] = __fadd_rn(__fdiv_rn(g.z, mass), __fmul_rn(p.dt, p.gy));
+        v[2] = __fadd_rn(__fdiv_rn(g.w, mass), __fmul_rn(p.dt, p.gz));
+    }
+    const int at[3] = {i, j, k};
+    const int size[3] = {d.nx, d.ny, d.nz};
+    if (p.sticky > 0) {
+        bool stuck = false;
+#pragma unroll
+        for (int a = 0; a < 3; a++) stuck |= at[a] < p.sticky || at[a] > size[a] - 1 - p.sticky;
+        if (stuck) v[0] = v[1] = v[2] = 0.0f;
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (!(at[a] > 1)) v[a] = fmaxf(v[a], 0.0f);
+            if (at[a] > size[a] - 3) v[a] = fminf(v[a], 0.0f);
+        }
+    }
+    return make_float3(v[0], v[1], v[2]);
+}
+
+// Flip3.keepInside (Flip3.java:644-655)
+__device__ __forceinline__ void keep_inside(float& at, float& vel, int size) {
+    const float lo = 1.0f, hi = (float)size - 2.0f;
+    if (at < lo) {
+        at = lo;
+        vel = fmaxf(vel, 0.0f);
+    }
+    if (at > hi) {
+        at = hi;
+        vel = fminf(vel, 0.0f);
+    }
+}
+
+// Kernel parameter bundle.
+struct Step3 {
+    const float* in;        // current particle set
+    float* out;             // next particle set (== in when not sorting)
+    int64_t stride;         // floats per field
+    int np;
+    const int* perm;        // sorted slot -> source particle, or null (identity, in place)
+    float4* grid;           // this step's grid {m, mu, mv, mw}
+    float4* vel;            // dense pipeline's node velocities
+    const Params3* params;
+    Dims3 d;
+    uint32_t* status;
+    // sort bookkeeping
+    int* key;               // per particle (indexed by slot in `out`)
+    int* rank;
+    int* cell_count;
+    int* brick_count;
+    const int* cell_start;
+    const int* brick_start;
+    const int* active;
+    const int* n_active;
+    int64_t nkeys;
+    int nbricks;
+    int count_next;         // G2P also counts keys for the next step's sort
+};
+
+__global__ void k_key_count3(Step3 s);
+__global__ void k_p2g3_atomic(Step3 s);
+__global__ void k_p2g3_warp(Step3 s);
+__global__ void k_p2g3_tile(Step3 s);
+__global__ void k_grid3_dense(Step3 s);
+__global__ void k_g2p3(Step3 s);
+__global__ void k_g2p3_tile(Step3 s);
+__global__ void k_clear_bricks3(Step3 s);
+__global__ void k_touched3(const float4* grid, int64_t nodes, unsigned long long* out);
+__global__ void k_unpack_grid3(const float4* grid, float* out, int64_t nodes, int comp);
+
+}  // namespace vf

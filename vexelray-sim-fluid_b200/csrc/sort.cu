@@ -1,0 +1,218 @@
+// sort.cu -- kernels of the stable counting sort by cell (see sort.cuh), and the library's
+// error/device plumbing.
+#include <stdarg.h>
+
+#include "sort.cuh"
+
+namespace vf {
+
+// ------------------------------------------------------------------ errors and device
+
+static thread_local char g_error[1024] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof g_error, fmt, ap);
+    va_end(ap);
+}
+
+const char* last_error() { return g_error; }
+
+int32_t require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        set_error("no CUDA device: %s", e == cudaSuccess ? "none found" : cudaGetErrorString(e));
+        cudaGetLastError();
+        return VF_ENODEV;
+    }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) {
+        set_error("libvexfluid is built for sm_100a (B200); device %d is compute capability %d.x", dev, major);
+        return VF_ENODEV;
+    }
+    return VF_OK;
+}
+
+int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+        if (cached <= 0) cached = 148;
+    }
+    return cached;
+}
+
+// ------------------------------------------------------------------ scans
+
+__global__ void __launch_bounds__(1024) k_scan_single(int* __restrict__ counts, int* __restrict__ starts,
+                                                      int64_t n) {
+    __shared__ int smem[33];
+    const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+    const int64_t lo = threadIdx.x * per;
+    const int64_t hi = lo + per < n ? lo + per : n;
+    int sum = 0;
+    for (int64_t i = lo; i < hi; i++) sum += counts[i];
+    int total;
+    int run = block_exclusive(sum, smem, &total);
+    for (int64_t i = lo; i < hi; i++) {
+        int c = counts[i];
+        starts[i] = run;
+        run += c;
+        counts[i] = 0;
+    }
+    if (threadIdx.x == 0) starts[n] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_brick_scan(int* __restrict__ brick_count, int* __restrict__ brick_start,
+                                                     int* __restrict__ active, int* __restrict__ n_active, int nb) {
+    __shared__ int smem[33];
+    const int per = (nb + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * per;
+    const int hi = lo + per < nb ? lo + per : nb;
+    int sum = 0, live = 0;
+    for (int i = lo; i < hi; i++) {
+        int c = brick_count[i];
+        sum += c;
+        live += c > 0;
+    }
+    int total, total_live;
+    int run = block_exclusive(sum, smem, &total);
+    int slot = block_exclusive(live, smem, &total_live);
+    for (int i = lo; i < hi; i++) {
+        int c = brick_count[i];
+        brick_start[i] = run;
+        run += c;
+        if (c > 0) active[slot++] = i;
+        brick_count[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        brick_start[nb] = total;
+        *n_active = total_live;
+    }
+}
+
+__global__ void __launch_bounds__(512) k_cell_scan(int* __restrict__ cell_count, int* __restrict__ cell_start,
+                                                   const int* __restrict__ brick_start,
+                                                   const int* __restrict__ active,
+                                                   const int* __restrict__ n_active) {
+    __shared__ int smem[33];
+    const int na = *n_active;
+    for (int a = blockIdx.x; a < na; a += gridDim.x) {
+        const int b = active[a];
+        const int64_t key = (int64_t)b * 512 + threadIdx.x;
+        int c = cell_count[key];
+        int total;
+        int ex = block_exclusive(c, smem, &total);
+        cell_start[key] = brick_start[b] + ex;
+        cell_count[key] = 0;
+    }
+}
+
+__global__ void k_permute(const int* __restrict__ key, const int* __restrict__ rank, const int* __restrict__ starts,
+                          int* __restrict__ perm, int n, uint32_t* status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int d = starts[key[i]] + rank[i];
+    if (d < 0 || d >= n) {
+        set_status(status, ST_RANK);
+        return;
+    }
+    perm[d] = i;
+}
+
+// Insertion sort of a short run, ascending.
+__device__ __forceinline__ void insertion_sort(int* a, int n) {
+    for (int i = 1; i < n; i++) {
+        int v = a[i];
+        int j = i - 1;
+        while (j >= 0 && a[j] > v) {
+            a[j + 1] = a[j];
+            j--;
+        }
+        a[j + 1] = v;
+    }
+}
+
+__global__ void k_fixup_cells(int* __restrict__ perm, const int* __restrict__ starts, int64_t cells) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    int s0 = starts[c], s1 = starts[c + 1];
+    if (s1 - s0 > 1) insertion_sort(perm + s0, s1 - s0);
+}
+
+// Runs up to this many particles per brick are fixed up in shared memory.
+constexpr int FIXUP_CAP = 12288;
+
+__global__ void __launch_bounds__(512) k_fixup_bricks(int* __restrict__ perm, const int* __restrict__ cell_start,
+                                                      const int* __restrict__ brick_start,
+                                                      const int* __restrict__ active,
+                                                      const int* __restrict__ n_active) {
+    extern __shared__ int run[];
+    const int na = *n_active;
+    for (int a = blockIdx.x; a < na; a += gridDim.x) {
+        const int b = active[a];
+        const int bs = brick_start[b], be = brick_start[b + 1];
+        const int n = be - bs;
+        const int64_t key = (int64_t)b * 512 + threadIdx.x;
+        int s0 = cell_start[key];
+        int s1 = threadIdx.x < 511 ? cell_start[key + 1] : be;
+        s0 = max(s0, bs);   // a run always lies inside its brick's; clip anything else
+        s1 = min(max(s1, s0), be);
+        if (n <= FIXUP_CAP) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) run[i] = perm[bs + i];
+            __syncthreads();
+            if (s1 - s0 > 1) insertion_sort(run + (s0 - bs), s1 - s0);
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) perm[bs + i] = run[i];
+            __syncthreads();
+        } else {
+            if (s1 - s0 > 1) insertion_sort(perm + s0, s1 - s0);
+        }
+    }
+}
+
+__global__ void k_dense_starts3(const int* __restrict__ cell_start, const int* __restrict__ brick_start,
+                                int* __restrict__ out, int64_t nkeys, int np) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nkeys) return;
+    if (k == nkeys) {
+        out[k] = np;
+        return;
+    }
+    int64_t b = k >> 9;
+    bool live = brick_start[b + 1] > brick_start[b];
+    out[k] = live ? cell_start[k] : brick_start[b];
+}
+
+__global__ void k_gather_fields(const float* __restrict__ in, float* __restrict__ out, const int* __restrict__ perm,
+                                int n, int64_t stride, int nf) {
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    int s = perm[d];
+    for (int f = 0; f < nf; f++) out[f * stride + d] = in[f * stride + s];
+}
+
+}  // namespace vf
+
+// ------------------------------------------------------------------ C-ABI: errors and device
+
+extern "C" int32_t vf_last_error(char* buf, size_t cap) {
+    const char* e = vf::last_error();
+    size_t n = strlen(e);
+    if (buf && cap) {
+        size_t k = n < cap - 1 ? n : cap - 1;
+        memcpy(buf, e, k);
+        buf[k] = 0;
+    }
+    return (int32_t)n;
+}
+
+extern "C" int32_t vf_version(void) { return 1; }
+
+extern "C" int32_t vf_device_ok(void) { return vf::require_device() == VF_OK ? 1 : 0; }

@@ -1,0 +1,702 @@
+// swe.cu -- the shallow-water step (ShallowWater.java) on TMA-staged shared-memory halo tiles,
+// and the vf_swe_* C-ABI: PatchSimulation (vexelray-sim-fluid-gui/.../gui/PatchSimulation.java).
+// Reference paths: vexelray-sim-fluid-core/src/main/java/dev/vexelray/sim/fluid/stencil/.
+//
+// Built with --fmad=false and IEEE division and square root: every operation rounds as the
+// reference's strict f32 (Java) arithmetic does, so a step's output is bit-identical to the
+// reference's CPU semantics (and to the oracle), and so are the tick counts it derives.
+//
+// One CTA per 64 x 16 tile of cells:
+//   1. the tile and a one-cell halo of h, hu, hv land in shared memory by three 2D TMA loads
+//      (the box starts four cells left of the tile so its x coordinate is 16-byte aligned);
+//   2. per cell of tile+halo: u = hu/h, v = hv/h (0 when dry) and c = sqrt(g h), once;
+//   3. every x-face and y-face flux of the tile computed ONCE (the reference computes each face
+//      twice, once from each side, with identical inputs and so identical bits);
+//   4. each cell's update from its four faces, the depth clamp (counted), the stores, and the next
+//      step's speed max-reduced over the CTA before one filtered atomicMax.
+#include <cuda.h>
+
+#include <cmath>
+#include <vector>
+
+#include "sort.cuh"
+
+using namespace vf;
+
+namespace {
+
+constexpr int TX = 64, TY = 16;                 // cells per tile
+constexpr int HX = TX + 8;                      // loaded box width: x0-4 .. x0+TX+3
+constexpr int HY = TY + 2;                      // loaded box height: y0-1 .. y0+TY
+constexpr int PX = TX + 2, PY = TY + 2;         // primitive window: x0-1 .. x0+TX
+constexpr int SWE_THREADS = 256;
+constexpr int BOXF = (HY * HX * 4 + 127) / 128 * 128 / 4;   // floats per staged field, 128-byte padded
+
+struct SweArgs {
+    const float* in[3];
+    float* out[3];
+    const float* params;                        // [g, courant, dx, dy, dry] (ShallowWater.java:120)
+    const int* speed_in;
+    int* speed_out;
+    int* speed_clear;
+    const int* budget_in;
+    int* budget_out;
+    int* clamped;
+    uint32_t* status;
+    int nx, ny;
+    int edge[4];                                // west, east, south, north: VF_EDGE_*
+    int use_tma;
+};
+
+struct SweShared {
+    float box[3][BOXF];                         // h, hu, hv, each [HY][HX] (TMA destinations, 128-byte aligned)
+    float pu[PY][PX], pv[PY][PX], pc[PY][PX];   // primitives
+    float fx[3][TY][TX + 1];                    // x-face fluxes (mass, normal=hu, tangent=hv)
+    float fy[3][TY + 1][TX];                    // y-face fluxes (mass, normal=hv, tangent=hu)
+    unsigned long long bar;
+    int red[SWE_THREADS / 32];
+    int clamps;
+};
+
+struct Face {
+    float mass, normal, tangent;
+};
+
+// ShallowWater.hll (ShallowWater.java:336-378) with the side's velocities and wave speed given.
+__device__ __forceinline__ Face hll(float g, float dry, float hL, float qnL, float qtL, float unL, float utL, float cL,
+                                    float hR, float qnR, float qtR, float unR, float utR, float cR) {
+    float sL = fminf(unL - cL, unR - cR);
+    float sR = fmaxf(unL + cL, unR + cR);
+    if (!(hR > dry)) {
+        sL = unL - cL;
+        sR = unL + 2.0f * cL;
+    }
+    if (!(hL > dry)) {
+        sL = unR - 2.0f * cR;
+        sR = unR + cR;
+    }
+    const float lo = fminf(sL, 0.0f);
+    const float hi = fmaxf(sR, 0.0f);
+    const float span = fmaxf(hi - lo, 1e-30f);
+    const float lohi = lo * hi;
+    const float pL = (0.5f * g) * (hL * hL);
+    const float pR = (0.5f * g) * (hR * hR);
+    Face f;
+    // ShallowWater.combine (381-384): ((hi FL - lo FR) + lo hi (UR - UL)) / span
+    f.mass = ((hi * qnL - lo * qnR) + lohi * (hR - hL)) / span;
+    f.normal = ((hi * (qnL * unL + pL) - lo * (qnR * unR + pR)) + lohi * (qnR - qnL)) / span;
+    f.tangent = ((hi * (qnL * utL) - lo * (qnR * utR)) + lohi * (qtR - qtL)) / span;
+    return f;
+}
+
+__device__ __forceinline__ float velocity(float h, float q, float dry) { return h > dry ? q / h : 0.0f; }
+
+__device__ __forceinline__ bool poll_barrier(uint32_t addr, int phase, int limit) {
+    for (int it = 0; it < limit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Bounded wait on an mbarrier phase. On giving up it sets the status bit, then waits once more,
+// again bounded, so copies still in flight land before the CTA leaves; returns false.
+__device__ __forceinline__ bool wait_barrier(unsigned long long* bar, int phase, uint32_t* status) {
+    const uint32_t addr = (uint32_t)__cvta_generic_to_shared(bar);
+    if (poll_barrier(addr, phase, 1 << 22)) return true;
+    set_status(status, ST_TIMEOUT);
+    poll_barrier(addr, phase, 1 << 22);
+    return false;
+}
+
+__global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
+                                                          const __grid_constant__ CUtensorMap tm_hu,
+                                                          const __grid_constant__ CUtensorMap tm_hv) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t mis = (uint32_t)__cvta_generic_to_shared(smem_raw) & 127u;
+    SweShared& S = *reinterpret_cast<SweShared*>(smem_raw + ((128u - mis) & 127u));
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int nx = a.nx, ny = a.ny;
+
+    // ShallowWater.java:184-192: the step from the fastest wave, in whole ticks, within the budget
+    const float g = a.params[0], courant = a.params[1], dx = a.params[2], dy = a.params[3], dry = a.params[4];
+    const float fastest = __int_as_float(*a.speed_in);
+    const float allowed = fminf((courant * fminf(dx, dy)) / fmaxf(fastest, 1e-30f), 2000.0f);
+    int ticks = (int)(allowed * 1000000.0f);
+    const int budget = *a.budget_in;
+    if (budget < ticks) ticks = budget;
+    const float dt = (float)ticks * (float)(1.0 / 1000000.0);
+    const float rx = dt / dx;
+    const float ry = dt / dy;
+
+    // 1. stage the tile + halo
+    bool loaded = true;
+    if (a.use_tma) {
+        if (tid == 0) {
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            S.clamps = 0;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+            const uint32_t bytes = 3u * HY * HX * 4u;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+            const CUtensorMap* maps[3] = {&tm_h, &tm_hu, &tm_hv};
+            const int bx = x0 - 4, by = y0 - 1;   // bx is a multiple of 4: 16-byte aligned
+            for (int f = 0; f < 3; f++) {
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&S.box[f][0]);
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                    "[%4];" ::"r"(dst),
+                    "l"(maps[f]), "r"(bx), "r"(by), "r"(bar)
+                    : "memory");
+            }
+        }
+        loaded = wait_barrier(&S.bar, 0, a.status);
+    } else {
+        if (tid == 0) S.clamps = 0;
+        for (int i = tid; i < HY * HX; i += SWE_THREADS) {
+            const int ly = i / HX, lx = i % HX;
+            const int gx = x0 - 4 + lx, gy = y0 - 1 + ly;
+            const bool in = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+            const int64_t c = (int64_t)gy * nx + gx;
+            for (int f = 0; f < 3; f++) S.box[f][ly * HX + lx] = in ? a.in[f][c] : 0.0f;
+        }
+    }
+    __syncthreads();
+    if (!loaded) return;   // a TMA that never landed: the status word says so, nothing is written
+
+    // 2. primitives of tile + halo (cells x0-1..x0+TX, y0-1..y0+TY that lie in the domain)
+    for (int i = tid; i < PY * PX; i += SWE_THREADS) {
+        const int ly = i / PX, lx = i % PX;
+        const float h = S.box[0][(ly) * HX + lx + 3];
+        S.pu[ly][lx] = velocity(h, S.box[1][(ly) * HX + lx + 3], dry);
+        S.pv[ly][lx] = velocity(h, S.box[2][(ly) * HX + lx + 3], dry);
+        S.pc[ly][lx] = sqrtf(g * h);
+    }
+    __syncthreads();
+
+    // 3a. x-faces: face fx is the west face of cell fx (left = fx-1, right = fx)
+    for (int i = tid; i < TY * (TX + 1); i += SWE_THREADS) {
+        const int ly = i / (TX + 1), lf = i % (TX + 1);
+        const int gy = y0 + ly, gf = x0 + lf;
+        if (gy >= ny || gf > nx) continue;
+        // local primitive/box column of the left cell is lf (box: lf + 3)
+        int l = lf, r = lf + 1;       // primitive columns of left and right cells
+        float sgnL = 1.0f, sgnR = 1.0f;
+        if (gf == 0) {                // left is the ghost of cell 0
+            l = r;
+            if (a.edge[0] == VF_EDGE_WALL) sgnL = -1.0f;
+        }
+        if (gf == nx) {               // right is the ghost of cell nx-1
+            r = l;
+            if (a.edge[1] == VF_EDGE_WALL) sgnR = -1.0f;
+        }
+        const int py = ly + 1;
+        const float hL = S.box[0][(py) * HX + l + 3], hR = S.box[0][(py) * HX + r + 3];
+        const float qnL = sgnL * S.box[1][(py) * HX + l + 3], qtL = S.box[2][(py) * HX + l + 3];
+        const float qnR = sgnR * S.box[1][(py) * HX + r + 3], qtR = S.box[2][(py) * HX + r + 3];
+        const Face f = hll(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR, qtR,
+                           sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r]);
+        S.fx[0][ly][lf] = f.mass;
+        S.fx[1][ly][lf] = f.normal;
+        S.fx[2][ly][lf] = f.tangent;
+    }
+    // 3b. y-faces: face fy is the south face of cell fy (below = fy-1, above = fy)
+    for (int i = tid; i < (TY + 1) * TX; i += SWE_THREADS) {
+        const int lf = i / TX, lx = i % TX;
+        const int gx = x0 + lx, gf = y0 + lf;
+        if (gx >= nx || gf > ny) continue;
+        int b = lf, t = lf + 1;       // primitive rows of the cells below and above
+        float sgnB = 1.0f, sgnT = 1.0f;
+        if (gf == 0) {
+            b = t;
+            if (a.edge[2] == VF_EDGE_WALL) sgnB = -1.0f;
+        }
+        if (gf == ny) {
+            t = b;
+            if (a.edge[3] == VF_EDGE_WALL) sgnT = -1.0f;
+        }
+        const int px = lx + 1;
+        const float hB = S.box[0][(b) * HX + px + 3], hT = S.box[0][(t) * HX + px + 3];
+        const float qnB = sgnB * S.box[2][(b) * HX + px + 3], qtB = S.box[1][(b) * HX + px + 3];
+        const float qnT = sgnT * S.box[2][(t) * HX + px + 3], qtT = S.box[1][(t) * HX + px + 3];
+        const Face f = hll(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT, qtT,
+                           sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px]);
+        S.fy[0][lf][lx] = f.mass;
+        S.fy[1][lf][lx] = f.normal;
+        S.fy[2][lf][lx] = f.tangent;
+    }
+    __syncthreads();
+
+    // 4. the update (ShallowWater.java:206-235)
+    int best = 0, clamps = 0;
+    for (int i = tid; i < TY * TX; i += SWE_THREADS) {
+        const int ly = i / TX, lx = i % TX;
+        const int gx = x0 + lx, gy = y0 + ly;
+        if (gx >= nx || gy >= ny) continue;
+        const float h0 = S.box[0][(ly + 1) * HX + lx + 4], hu0 = S.box[1][(ly + 1) * HX + lx + 4], hv0 = S.box[2][(ly + 1) * HX + lx + 4];
+        const float h = (h0 - rx * (S.fx[0][ly][lx + 1] - S.fx[0][ly][lx])) - ry * (S.fy[0][ly + 1][lx] - S.fy[0][ly][lx]);
+        const float hu =
+            (hu0 - rx * (S.fx[1][ly][lx + 1] - S.fx[1][ly][lx])) - ry * (S.fy[2][ly + 1][lx] - S.fy[2][ly][lx]);
+        const float hv =
+            (hv0 - rx * (S.fx[2][ly][lx + 1] - S.fx[2][ly][lx])) - ry * (S.fy[1][ly + 1][lx] - S.fy[1][ly][lx]);
+        if (h < 0.0f) clamps++;
+        const float nh = fmaxf(h, 0.0f);
+        const int64_t c = (int64_t)gy * nx + gx;
+        a.out[0][c] = nh;
+        a.out[1][c] = hu;
+        a.out[2][c] = hv;
+        const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
+        const float speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
+        best = max(best, __float_as_int(speed));
+        if (c == 0) {
+            *a.speed_clear = 0;
+            *a.budget_out = budget - ticks;
+        }
+    }
+    // CTA reduction of the speed bits and the clamp count, then one atomic each
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+        clamps += __shfl_xor_sync(0xffffffffu, clamps, o);
+    }
+    if ((tid & 31) == 0) {
+        S.red[tid >> 5] = best;
+        if (clamps) atomicAdd(&S.clamps, clamps);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int m = 0;
+        for (int w = 0; w < SWE_THREADS / 32; w++) m = max(m, S.red[w]);
+        // only a filter: the buffer only grows within a step (ShallowWater.java:227-235)
+        if (m > *(volatile int*)a.speed_out) atomicMax(a.speed_out, m);
+        if (S.clamps) atomicAdd(a.clamped, S.clamps);
+    }
+}
+
+// ------------------------------------------------------------------ diagnostics (Diagnostics.of)
+
+struct DiagPart {
+    double volume, min_depth, max_depth, max_speed, max_froude, max_wave;
+    int non_finite, negative, wet;
+};
+
+__global__ void __launch_bounds__(256) k_swe_diag(const float* h, const float* hu, const float* hv, int64_t n,
+                                                  double g, double dry, DiagPart* parts) {
+    DiagPart p{0.0, INFINITY, 0.0, 0.0, 0.0, 0.0, 0, 0, 0};
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float hk = h[k], uk = hu[k], vk = hv[k];
+        if (!isfinite(hk) || !isfinite(uk) || !isfinite(vk)) {
+            p.non_finite++;
+            continue;
+        }
+        if (hk < 0) p.negative++;
+        p.volume += hk;
+        p.max_depth = fmax(p.max_depth, (double)hk);
+        if ((double)hk <= dry) continue;
+        p.wet++;
+        p.min_depth = fmin(p.min_depth, (double)hk);
+        const double u = (double)uk / hk, v = (double)vk / hk;
+        const double c = sqrt(g * hk);
+        const double speed = sqrt(u * u + v * v);
+        p.max_speed = fmax(p.max_speed, speed);
+        if (hk >= 1e-3) p.max_froude = fmax(p.max_froude, speed / c);
+        p.max_wave = fmax(p.max_wave, fmax(fabs(u), fabs(v)) + c);
+    }
+    __shared__ DiagPart sp[256];
+    sp[threadIdx.x] = p;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            DiagPart& a = sp[threadIdx.x];
+            const DiagPart& b = sp[threadIdx.x + s];
+            a.volume += b.volume;
+            a.min_depth = fmin(a.min_depth, b.min_depth);
+            a.max_depth = fmax(a.max_depth, b.max_depth);
+            a.max_speed = fmax(a.max_speed, b.max_speed);
+            a.max_froude = fmax(a.max_froude, b.max_froude);
+            a.max_wave = fmax(a.max_wave, b.max_wave);
+            a.non_finite += b.non_finite;
+            a.negative += b.negative;
+            a.wet += b.wet;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) parts[blockIdx.x] = sp[0];
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)p;
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// A 2D tensor map over one nx x ny f32 field with an HX x HY box; false if TMA cannot take it
+// (row pitch not a multiple of 16 bytes, or an unaligned base).
+bool make_map(CUtensorMap* m, const float* base, int nx, int ny) {
+    EncodeTiled enc = encode_fn();
+    if (!enc) return false;
+    if (((uintptr_t)base & 15) || ((int64_t)nx * 4) % 16 != 0) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+    cuuint64_t strides[1] = {(cuuint64_t)nx * 4};
+    cuuint32_t box[2] = {(cuuint32_t)HX, (cuuint32_t)HY};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the handle
+
+struct vf_swe {
+    int nx, ny;
+    int edges[4];
+    int64_t cells;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer state[2];    // 3 fields each
+    DeviceBuffer small;       // speed[3], budget[2], clamped, params[5] (as ints/floats)
+    DeviceBuffer status, diag;
+    CUtensorMap maps[2][3];
+    bool tma = false;
+    // PatchSimulation.java:52-56
+    int64_t clock_now = 0;
+    int32_t clock_outstanding = 0;
+    int64_t dispatched = 0;
+    int64_t total_steps = 0;
+    int64_t last_step = 0;
+    float host_params[5];
+};
+
+namespace {
+
+int* small_i(vf_swe* h) { return h->small.as<int>(); }
+int* speed_slot(vf_swe* h, int k) { return small_i(h) + k; }          // 0..2
+int* budget_slot(vf_swe* h, int k) { return small_i(h) + 3 + k; }     // 3..4
+int* clamped_ptr(vf_swe* h) { return small_i(h) + 5; }                // 5
+float* params_ptr(vf_swe* h) { return h->small.as<float>() + 8; }     // 8..12
+
+float* field(vf_swe* h, int s, int f) { return h->state[s].as<float>() + (int64_t)f * h->cells; }
+
+int32_t swe_params_check(const int32_t* params, int32_t n, float out[5]) {
+    VF_REQUIRE(params && n == 5, VF_EINVAL, "ShallowWater.params has 5 words, got %d", n);
+    for (int k = 0; k < 5; k++) out[k] = bits_to_float(params[k]);
+    // ShallowWater.paramsAllowingInstability refuses a Courant number that is not positive (262-264);
+    // above 1/2 is the caller's choice (params vs paramsAllowingInstability).
+    VF_REQUIRE(out[1] > 0, VF_EINVAL, "a Courant number must be positive, got %g", out[1]);
+    return VF_OK;
+}
+
+// One dispatch: step k of the rotation (PatchSimulation.dispatch, PatchSimulation.java:197-205).
+int32_t dispatch(vf_swe* h) {
+    const int64_t k = h->dispatched;
+    const int si = (int)(k % 2), so = (int)((k + 1) % 2);
+    SweArgs a;
+    for (int f = 0; f < 3; f++) {
+        a.in[f] = field(h, si, f);
+        a.out[f] = field(h, so, f);
+    }
+    a.params = params_ptr(h);
+    a.speed_in = speed_slot(h, (int)(k % 3));
+    a.speed_out = speed_slot(h, (int)((k + 1) % 3));
+    a.speed_clear = speed_slot(h, (int)((k + 2) % 3));
+    a.budget_in = budget_slot(h, si);
+    a.budget_out = budget_slot(h, so);
+    a.clamped = clamped_ptr(h);
+    a.status = h->status.as<uint32_t>();
+    a.nx = h->nx;
+    a.ny = h->ny;
+    for (int e = 0; e < 4; e++) a.edge[e] = h->edges[e];
+    a.use_tma = h->tma ? 1 : 0;
+    dim3 grid(div_up(h->nx, TX), div_up(h->ny, TY));
+    const CUtensorMap* m = h->maps[si];
+    k_swe_tile<<<grid, SWE_THREADS, sizeof(SweShared) + 128, h->stream>>>(a, m[0], m[1], m[2]);
+    VF_CHECK_LAUNCH();
+    h->dispatched++;
+    return VF_OK;
+}
+
+int32_t read_budget(vf_swe* h, int slot, int32_t* out) {
+    VF_TRY_CUDA(cudaMemcpyAsync(out, budget_slot(h, slot), 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int32_t write_budget(vf_swe* h, int slot, int32_t v) {
+    VF_TRY_CUDA(cudaMemcpyAsync(budget_slot(h, slot), &v, 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int32_t status_swe(vf_swe* h) {
+    uint32_t st = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&st, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    if (st) {
+        VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+        set_error("a kernel flagged device status 0x%x", st);
+        return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
+    }
+    return VF_OK;
+}
+
+// ShallowWater.fastestWave (ShallowWater.java:287-295), on the host.
+int32_t fastest_wave_bits(const float* h, const float* hu, const float* hv, int64_t n, double g, double dry) {
+    float fastest = 0.0f;
+    for (int64_t k = 0; k < n; k++) {
+        float u = (double)h[k] > dry ? hu[k] / h[k] : 0.0f;
+        float w = (double)h[k] > dry ? hv[k] / h[k] : 0.0f;
+        float c = (float)std::sqrt(g * (double)h[k]);
+        float s = std::fmax(std::fabs(u), std::fabs(w)) + c;
+        if (std::isnan(s) || std::isnan(fastest)) fastest = NAN;
+        else fastest = fastest > s ? fastest : s;
+    }
+    int32_t b;
+    memcpy(&b, &fastest, 4);
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** out) {
+    VF_REQUIRE(out && edges, VF_EINVAL, "null argument");
+    *out = nullptr;
+    VF_REQUIRE(nx >= 1 && ny >= 1, VF_EINVAL, "a patch needs at least one cell each way, got %d x %d", nx, ny);
+    for (int e = 0; e < 4; e++)
+        VF_REQUIRE(edges[e] == VF_EDGE_WALL || edges[e] == VF_EDGE_OPEN, VF_EINVAL, "every side of a patch needs an edge");
+    int32_t rc = require_device();
+    if (rc) return rc;
+    vf_swe* h = new vf_swe();
+    h->nx = nx;
+    h->ny = ny;
+    for (int e = 0; e < 4; e++) h->edges[e] = edges[e];
+    h->cells = (int64_t)nx * ny;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        set_error("cudaStreamCreate failed");
+        return VF_ECUDA;
+    }
+    if ((rc = h->state[0].alloc((size_t)3 * h->cells * 4)) || (rc = h->state[1].alloc((size_t)3 * h->cells * 4)) ||
+        (rc = h->small.alloc(64)) || (rc = h->status.alloc(16)) || (rc = h->diag.alloc(sizeof(DiagPart) * 1184))) {
+        vf_swe_destroy(h);
+        return rc;
+    }
+    for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status}) cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream);
+    if (cudaFuncSetAttribute(k_swe_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SweShared) + 128) !=
+        cudaSuccess) {
+        vf_swe_destroy(h);
+        set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared));
+        return VF_ECUDA;
+    }
+    bool tma = true;
+    for (int s = 0; s < 2; s++)
+        for (int f = 0; f < 3; f++) tma = tma && make_map(&h->maps[s][f], field(h, s, f), nx, ny);
+    h->tma = tma;
+    if (!tma) memset(h->maps, 0, sizeof h->maps);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        vf_swe_destroy(h);
+        set_error("clearing buffers failed");
+        return VF_ECUDA;
+    }
+    *out = h;
+    return VF_OK;
+}
+
+int32_t vf_swe_load(vf_swe* h, const float* hcell, const float* hu, const float* hv, const int32_t* params,
+                    int32_t nparams) {
+    VF_REQUIRE(h && hcell && hu && hv, VF_EINVAL, "null argument");
+    float p[5];
+    int32_t rc = swe_params_check(params, nparams, p);
+    if (rc) return rc;
+    memcpy(h->host_params, p, sizeof p);
+    h->dispatched = 0;
+    h->total_steps = 0;
+    h->last_step = 0;
+    h->clock_now = 0;
+    h->clock_outstanding = 0;
+    const float* src[3] = {hcell, hu, hv};
+    for (int f = 0; f < 3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(field(h, 0, f), src[f], (size_t)h->cells * 4, cudaMemcpyHostToDevice, h->stream));
+    int32_t small[16] = {0};
+    small[0] = fastest_wave_bits(hcell, hu, hv, h->cells, (double)p[0], (double)p[4]);   // PatchSimulation.java:100-102
+    memcpy(small + 8, p, sizeof p);
+    VF_TRY_CUDA(cudaMemcpyAsync(h->small.ptr, small, sizeof small, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int32_t vf_swe_params(vf_swe* h, const int32_t* params, int32_t nparams) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    float p[5];
+    int32_t rc = swe_params_check(params, nparams, p);
+    if (rc) return rc;
+    memcpy(h->host_params, p, sizeof p);
+    VF_TRY_CUDA(cudaMemcpyAsync(params_ptr(h), p, sizeof p, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+// PatchSimulation.advance (PatchSimulation.java:120-145). The clock is the host's i64 tick count:
+// grant gives up to 2^31-1 ticks to the device as its budget; settle moves the clock by what was spent.
+int32_t vf_swe_advance(vf_swe* h, int64_t ticks, int32_t max_steps, int32_t* steps_out, int64_t* spent,
+                       int64_t* behind) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(ticks >= 0 && max_steps >= 0, VF_EINVAL, "ticks and maxSteps must be >= 0");
+    const int64_t before = h->clock_now;
+    const int64_t want = (before + ticks) - h->clock_now;
+    const int32_t granted = (int32_t)(want < 0 ? 0 : want > 2147483647LL ? 2147483647LL : want);
+    h->clock_outstanding = granted;
+    int32_t rc = write_budget(h, (int)(h->dispatched % 2), granted);
+    if (rc) return rc;
+    int32_t left = granted;
+    int32_t steps = 0;
+    while (left > 0 && steps < max_steps) {
+        const int32_t batch =
+            h->last_step > 0 ? (int32_t)std::min<int64_t>(max_steps - steps, ((int64_t)left + h->last_step - 1) / h->last_step)
+                             : 1;
+        for (int s = 0; s < batch; s++)
+            if ((rc = dispatch(h))) return rc;
+        steps += batch;
+        int32_t now = 0;
+        if ((rc = read_budget(h, (int)(h->dispatched % 2), &now))) return rc;
+        if (now > 0 && now < left) h->last_step = (left - now) / batch;
+        left = now;
+    }
+    h->clock_now += h->clock_outstanding - left;   // settle
+    h->clock_outstanding = 0;
+    h->total_steps += steps;
+    if (steps_out) *steps_out = steps;
+    if (spent) *spent = h->clock_now - before;
+    if (behind) *behind = left;
+    return status_swe(h);
+}
+
+int32_t vf_swe_read(vf_swe* h, float* hcell, float* hu, float* hv) {
+    VF_REQUIRE(h && hcell && hu && hv, VF_EINVAL, "null argument");
+    const int s = (int)(h->dispatched % 2);
+    float* dst[3] = {hcell, hu, hv};
+    for (int f = 0; f < 3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(dst[f], field(h, s, f), (size_t)h->cells * 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return status_swe(h);
+}
+
+int32_t vf_swe_fastest_wave(vf_swe* h, double* out) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    int32_t b = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&b, speed_slot(h, (int)(h->dispatched % 3)), 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    *out = (double)bits_to_float(b);
+    return VF_OK;
+}
+
+int32_t vf_swe_clamped(vf_swe* h, int32_t* out) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    VF_TRY_CUDA(cudaMemcpyAsync(out, clamped_ptr(h), 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int64_t vf_swe_now(const vf_swe* h) { return h ? h->clock_now : 0; }
+
+int64_t vf_swe_steps(const vf_swe* h) { return h ? h->total_steps : 0; }
+
+int32_t vf_swe_dispatch(vf_swe* h, int32_t n) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(n >= 0, VF_EINVAL, "n must be >= 0");
+    for (int k = 0; k < n; k++) {
+        int32_t rc = dispatch(h);
+        if (rc) return rc;
+    }
+    return VF_OK;
+}
+
+int64_t vf_swe_dispatched(const vf_swe* h) { return h ? h->dispatched : 0; }
+
+int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks) {
+    VF_REQUIRE(h && (slot == 0 || slot == 1), VF_EINVAL, "budget slot is 0 or 1");
+    return write_budget(h, slot, ticks);
+}
+
+int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks) {
+    VF_REQUIRE(h && ticks && (slot == 0 || slot == 1), VF_EINVAL, "budget slot is 0 or 1");
+    int32_t rc = read_budget(h, slot, ticks);
+    return rc ? rc : status_swe(h);
+}
+
+int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    const int s = (int)(h->dispatched % 2);
+    const int blocks = 1184;
+    k_swe_diag<<<blocks, 256, 0, h->stream>>>(field(h, s, 0), field(h, s, 1), field(h, s, 2), h->cells,
+                                              (double)h->host_params[0], (double)h->host_params[4],
+                                              h->diag.as<DiagPart>());
+    VF_CHECK_LAUNCH();
+    std::vector<DiagPart> parts(blocks);
+    VF_TRY_CUDA(cudaMemcpyAsync(parts.data(), h->diag.ptr, sizeof(DiagPart) * blocks, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    DiagPart t{0.0, INFINITY, 0.0, 0.0, 0.0, 0.0, 0, 0, 0};
+    for (const DiagPart& p : parts) {
+        t.volume += p.volume;
+        t.min_depth = std::fmin(t.min_depth, p.min_depth);
+        t.max_depth = std::fmax(t.max_depth, p.max_depth);
+        t.max_speed = std::fmax(t.max_speed, p.max_speed);
+        t.max_froude = std::fmax(t.max_froude, p.max_froude);
+        t.max_wave = std::fmax(t.max_wave, p.max_wave);
+        t.non_finite += p.non_finite;
+        t.negative += p.negative;
+        t.wet += p.wet;
+    }
+    const double dx = h->host_params[2], dy = h->host_params[3];
+    out[0] = t.volume * dx * dy;
+    out[1] = t.wet == 0 ? 0 : t.min_depth;
+    out[2] = t.max_depth;
+    out[3] = t.max_speed;
+    out[4] = t.max_froude;
+    out[5] = t.max_wave * dt / std::fmin(dx, dy);
+    out[6] = t.non_finite;
+    out[7] = t.negative;
+    out[8] = t.wet;
+    return VF_OK;
+}
+
+void* vf_swe_stream(vf_swe* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t vf_swe_on_gpu(const vf_swe* h) { return h ? 1 : 0; }
+
+void vf_swe_destroy(vf_swe* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status, &h->diag}) b->release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"
