@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""bench.py -- the 3D MLS-MPM dam break at 256^3 (about 8.2M particles), one B200 per rank.
+
+A step is one full ParticleSimulation3.advance(1): the per-step counting sort by stencil cell, the
+sorted brick-tile P2G, the grid update fused into the brick-tile G2P, on inputs resident in HBM.
+The line reports particle-steps/s for the whole job, the P2G+G2P roofline against the measured HBM
+bandwidth, the same metric end to end through the public API (host arrays in, positions out), the
+oracle's threaded CPU step as the CPU baseline, and a shallow-water sub-measurement (4096^2, HLL).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the 3D step does not shard
+across GPUs here: replicas only); the time is the max over ranks and the value the sum of work.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG = ROOT / "vexelray-sim-fluid_b200"
+
+# ---------------------------------------------------------------------------------------------- workload
+
+N3 = 256                    # grid nodes per axis, dx = 1/256
+PPC3 = 8                    # particles per cell
+BOX3 = ((0.05, 0.45), (0.05, 0.4325), (0.05, 0.45))   # 8.16M particles at 8 ppc (the config's "~8.2M")
+DT3 = 5e-5
+G_SI = 9.8
+SEED3 = 1
+WORKLOAD3 = ("3D MLS-MPM APIC dam break, 256^3 nodes, dx=1/256, 8 particles/cell jittered from seed 1 in "
+             "[0.05,0.45]x[0.05,0.4325]x[0.05,0.45] (8,156,736 particles; the [0.05,0.65] y-extent gives 12.9M), "
+             "dt=5e-5, gravity -9.8 m/s^2, p=B(1/J-1) with B=(5 sqrt(2gH))^2, counting sort by stencil cell "
+             "every step, sorted shared-memory-tile P2G")
+
+N_SWE = 4096
+SEED_SWE = 2
+
+
+def package():
+    if "vexfluid" in sys.modules:
+        return sys.modules["vexfluid"]
+    spec = importlib.util.spec_from_file_location("vexfluid", PKG / "__init__.py", submodule_search_locations=[str(PKG)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["vexfluid"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dam3():
+    """Seeded particles of the 3D config: every cell whose centre lies in the box, PPC3 jittered particles
+    each (cell + U*0.999 per axis, as the reference's tests fill cells), z-major order."""
+    n = N3
+    rng = np.random.default_rng(SEED3)
+    ranges = []
+    for lo, hi in BOX3:
+        a, b = lo * n, hi * n
+        c0 = math.ceil(a - 0.5)
+        c1 = math.ceil(b - 0.5)
+        ranges.append(np.arange(c0, c1, dtype=np.float32))
+    cz, cy, cx = np.meshgrid(ranges[2], ranges[1], ranges[0], indexing="ij")
+    cells = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
+    cells = np.repeat(cells, PPC3, axis=0)
+    jitter = (rng.random(cells.shape, dtype=np.float32) * np.float32(0.999)).astype(np.float32)
+    pos = (cells + jitter).astype(np.float32)
+    x, y, z = (np.ascontiguousarray(pos[:, a]) for a in range(3))
+    m = np.full(len(x), np.float32(1.0 / PPC3), np.float32)
+    g = -G_SI * n
+    height = len(ranges[1])
+    fall = math.sqrt(2 * -g * height)
+    bulk = (5 * fall) ** 2
+    return x, y, z, m, (DT3, 0.0, g, 0.0, bulk, 1.0)
+
+
+def swe_bumps():
+    """The shallow-water config: h = 1 + 16 seeded Gaussian bumps (amplitude U(0.1,0.5), sigma U(20,200)
+    cells, centres uniform), hu = hv = 0."""
+    n = N_SWE
+    rng = np.random.default_rng(SEED_SWE)
+    h = np.ones((n, n), np.float32)
+    y = np.arange(n, dtype=np.float32)[:, None]
+    x = np.arange(n, dtype=np.float32)[None, :]
+    for _ in range(16):
+        amp, sig = rng.uniform(0.1, 0.5), rng.uniform(20, 200)
+        cx, cy = rng.uniform(0, n), rng.uniform(0, n)
+        h += (amp * np.exp(-((x - cx) ** 2) / (2 * sig * sig)) * np.exp(-((y - cy) ** 2) / (2 * sig * sig))).astype(np.float32)
+    return h.ravel()
+
+
+# ---------------------------------------------------------------------------------------------- helpers
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """dram bytes per launch of a kernel from the committed ncu summary, scaled to this workload, or None."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    e = d.get(kernel)
+    return None if e is None else e.get("bytes_per_launch_full")
+
+
+class Dist:
+    """torch.distributed plumbing for N ranks (gloo: only a barrier and a max of device times cross ranks)."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------- CPU side
+
+def cpu_step_rate(x, y, z, m, params, budget_s=20.0, max_steps=3):
+    """The oracle's threaded 3D step on the host cores over the full workload: particle-steps/s."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _oracle import Flip3State, OrPhysics, fp, lib as olib
+    n = N3
+    s = Flip3State(n, n, n, x, y, z, m)
+    pw = np.ascontiguousarray(np.array(params, np.float32))
+    threads = olib().or_baseline_threads()
+    t0 = time.perf_counter()
+    olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)   # warm-up (page faults)
+    first = time.perf_counter() - t0
+    steps = max(1, min(max_steps, int(budget_s / max(first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)
+    el = time.perf_counter() - t0
+    return len(x) * steps / el, threads, steps, el
+
+
+# ---------------------------------------------------------------------------------------------- arms
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    x, y, z, m, params = dam3()
+    rate, threads, steps, el = cpu_step_rate(x, y, z, m, params, budget_s=60.0, max_steps=max(1, args.steps))
+    sample = (f"{steps} full steps of the 8.16M-particle 256^3 workload (oracle C port of Flip3Step, OpenMP, "
+              f"{threads} threads), {el:.1f} s")
+    line = {"metric": "MPM particle-steps/s", "value": rate, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered dam break)",
+            "config": {"workload": WORKLOAD3, "particles": len(x), "grid": [N3] * 3},
+            "impl": "reference",
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, dist: Dist):
+    vf = package()
+    vf.set_device(dist.local)
+    x, y, z, m, params = dam3()
+    np3 = len(x)
+    zeros = np.zeros(np3, np.float32)
+    sim = vf.ParticleSimulation3(N3, N3, N3, np3)
+    sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params))
+    stream = sim.stream()
+    ev0, ev1 = vf.Event(), vf.Event()
+
+    sim.advance(args.warmup)
+    sim.finish()
+
+    # timed region: K steps, device events on the handle's stream, barrier + sync on both sides
+    dist.barrier()
+    sim.finish()
+    launches0 = sim.launches()
+    with Clocks(dist.local) as clocks:
+        ev0.record(stream)
+        sim.advance(args.steps)
+        ev1.record(stream)
+        ms = ev0.elapsed_ms(ev1)
+    sim.finish()
+    launches = sim.launches() - launches0
+    dist.barrier()
+    ms_max = dist.max(ms)
+    work = dist.sum(float(np3) * args.steps)
+    value = work / (ms_max / 1e3)
+
+    # per-kernel device times over a second, profiled run of K steps (events around every launch)
+    sim.profile(True)
+    sim.advance(args.steps)
+    sim.finish()
+    prof = sim.profile_read()
+    sim.profile(False)
+    touched = sim.touched_nodes()
+    t_p2g = prof.get("k_p2g3_tile", (0.0, 1))
+    t_g2p = prof.get("k_g2p3_tile", (0.0, 1))
+    per_step_ms = (t_p2g[0] + t_g2p[0]) / args.steps
+    alg_bytes = 152.0 * np3 + 28.0 * touched
+    achieved = alg_bytes / (per_step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    tr_p2g, tr_g2p = profiled_traffic("k_p2g3_tile"), profiled_traffic("k_g2p3_tile")
+    traffic = (tr_p2g + tr_g2p) if (tr_p2g is not None and tr_g2p is not None) else None
+    total_prof = sum(v[0] for v in prof.values())
+    kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1], "share": v[0] / total_prof}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+
+    # end to end through the public API: pinned host arrays in (load), K steps, positions out (read)
+    outs = [np.empty(np3, np.float32) for _ in range(3)]
+    ins = [x, y, z, zeros, zeros, zeros, m]
+    with vf.Pinned(*([a for a in ins[:3]] + [zeros, m] + outs)):
+        dist.barrier()
+        sim.finish()
+        ev0.record(stream)
+        sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params))
+        sim.advance(args.steps)
+        for a, name in zip(outs, ("x", "y", "z")):
+            vf.check(vf.lib().vf_mpm3_read(sim._h, vf.FIELDS3[name], vf._fp(a), np3))
+        ev1.record(stream)
+        e2e_ms = dist.max(ev0.elapsed_ms(ev1))
+    e2e = {"value": dist.sum(float(np3) * args.steps) / (e2e_ms / 1e3), "unit": "particle-steps/s",
+           "h2d_bytes_per_step": 7 * np3 * 4 / args.steps, "d2h_bytes_per_step": 3 * np3 * 4 / args.steps,
+           "job": f"load (7 fields) + {args.steps} steps + read x,y,z, one job per rank"}
+    sim.close()
+
+    # shallow water, 4096^2 HLL, a sub-measurement (cells/s and its own roofline)
+    swe = None
+    if not args.no_swe:
+        h = swe_bumps()
+        zero2 = np.zeros_like(h)
+        with vf.PatchSimulation(N_SWE, N_SWE) as p:
+            p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
+            p.write_budget(0, 2 ** 31 - 1)
+            p.dispatch(3)
+            p.read_budget(0)
+            k_swe = max(10, args.steps)
+            s_stream = p.stream()
+            ev0.record(s_stream)
+            p.dispatch(k_swe)
+            ev1.record(s_stream)
+            swe_ms = ev0.elapsed_ms(ev1)
+            p.profile(True)
+            p.dispatch(k_swe)
+            p.read_budget(0)
+            sp = p.profile_read()
+            p.profile(False)
+        cells = N_SWE * N_SWE
+        k_ms = sp["k_swe_tile"][0] / sp["k_swe_tile"][1]
+        swe = {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)",
+               "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
+               "roofline": {"bound": "hbm", "achieved": 24.0 * cells / (k_ms / 1e3) / 1e9, "peak": peak,
+                            "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
+                            "kernel": "k_swe_tile", "bytes_per_cell": 24}}
+
+    if dist.rank != 0:
+        return
+    cpu_rate, threads, cpu_steps, cpu_el = (None, 0, 0, 0.0)
+    if not args.no_cpu:
+        cpu_rate, threads, cpu_steps, cpu_el = cpu_step_rate(x, y, z, m, params, budget_s=20.0)
+    line = {
+        "metric": "MPM particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered dam break)",
+        "config": {"workload": WORKLOAD3, "particles": np3, "grid": [N3] * 3, "parallelism": f"replicas x{dist.world}",
+                   "l2": "inputs larger than L2 (particles 555 MB per set, grid 268 MB per buffer)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_p2g3_tile + k_g2p3_tile (P2G+G2P)", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_step": alg_bytes, "touched_nodes": touched,
+                     "p2g_g2p_ms_per_step": per_step_ms},
+        "kernels": kernels,
+        "cpu_baseline": None if cpu_rate is None else {
+            "value": cpu_rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{cpu_steps} full steps of the same workload, oracle C port of Flip3Step, OpenMP, {cpu_el:.1f} s"},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "swe": swe,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water sub-measurement")
+    args = ap.parse_args()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -47,6 +47,19 @@ int32_t vf_last_error(char* buf, size_t cap);
 /* Library version, and whether a usable CUDA device is present (1) or not (0). */
 int32_t vf_version(void);
 int32_t vf_device_ok(void);
+/* Selects the CUDA device the calling thread's next handles use (one process per GPU). */
+int32_t vf_set_device(int32_t device);
+
+/* CUDA events on a handle's stream (vf_*_stream), for a caller timing the device work of its calls. */
+int32_t vf_event_create(void** event);
+int32_t vf_event_record(void* event, void* stream);
+/* Waits for `stop` and returns the device time between the two events. */
+int32_t vf_event_elapsed_ms(void* start, void* stop, float* ms);
+void vf_event_destroy(void* event);
+/* Page-locks (pins) a caller's host range so the synchronous copies of load/read run at full PCIe/C2C
+ * speed, and releases it. */
+int32_t vf_host_register(void* ptr, size_t bytes);
+int32_t vf_host_unregister(void* ptr);
 
 /* ------------------------------------------------------------------ physics flags */
 /* Flags for vf_mpm2_create / vf_mpm3_prepare. The reference's physics is the default (0):
@@ -175,6 +188,12 @@ int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
 int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out);
 int64_t vf_mpm3_steps(const vf_mpm3* h);
 int32_t vf_mpm3_on_gpu(const vf_mpm3* h);
+/* Kernel accounting: with profiling on, every launch of the handle is bracketed by CUDA events and its
+ * device time summed per kernel; profile_read returns entry `index` (VF_EINVAL past the last). launches is
+ * the count of kernels the handle has launched since it was made, profiling on or off. */
+int32_t vf_mpm3_profile(vf_mpm3* h, int32_t enable);
+int32_t vf_mpm3_profile_read(vf_mpm3* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches);
+int64_t vf_mpm3_launches(const vf_mpm3* h);
 void vf_mpm3_destroy(vf_mpm3* h);
 
 /* ------------------------------------------------------------------ shallow water (PatchSimulation) */
@@ -205,9 +224,13 @@ int32_t vf_swe_dispatch(vf_swe* h, int32_t n);
 int64_t vf_swe_dispatched(const vf_swe* h);
 int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks);
 int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks);
-/* Diagnostics.of over the current state (Diagnostics.java:43-81), reduced on the device.
- * out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
-int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]);
+/* Diagnostics.of(h, hu, hv, g, dry, dt, dx, dy) over the current state (Diagnostics.java:43-81), reduced on the
+ * device. out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
+int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]);
+/* Kernel accounting, as vf_mpm3_profile. */
+int32_t vf_swe_profile(vf_swe* h, int32_t enable);
+int32_t vf_swe_profile_read(vf_swe* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches);
+int64_t vf_swe_launches(const vf_swe* h);
 void* vf_swe_stream(vf_swe* h);
 int32_t vf_swe_on_gpu(const vf_swe* h);
 void vf_swe_destroy(vf_swe* h);

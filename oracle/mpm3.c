@@ -248,6 +248,20 @@ void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* s
     const int64_t plane = (int64_t)nx * ny, nodes = plane * nz;
     const float dt = params[P_DT], bulk = params[P_BULK], rho0 = params[P_RHO0];
     int nt = or_baseline_threads();
+    /* Private grids: one per thread, allocated once and touched only on the z-planes each thread's
+     * particles reach, so only those pages are ever backed. */
+    static float* own = NULL;
+    static size_t own_floats = 0;
+    if (!scratch) {
+        size_t want = (size_t)nt * 4 * (size_t)nodes;
+        if (own_floats < want) {
+            free(own);
+            own = (float*)malloc(want * sizeof(float));
+            own_floats = own ? want : 0;
+        }
+        scratch = own;
+        if (!scratch) return;
+    }
     int zlo[256], zhi[256];
     if (nt > 256) nt = 256;
 #pragma omp parallel num_threads(nt)

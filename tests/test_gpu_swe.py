@@ -156,7 +156,7 @@ def test_device_diagnostics_match_the_host_readout():
         p.load(h, np.zeros(n * n, F), np.zeros(n * n, F), swe_params(9.81, 0.45, 1, 1, 1e-6).view(np.int32))
         p.advance(vf.ticks(0.5), 1000)
         st = p.read()
-        d = p.diagnostics(0.01)
+        d = p.diagnostics(9.81, float(F(1e-6)), 0.01, 1, 1)
         e = swe_diagnostics(st[0], st[1], st[2], 9.81, float(F(1e-6)), 0.01, 1, 1)
         assert abs(d[0] - e.volume) <= 1e-9 * abs(e.volume)
         for got, want in zip(d[1:6], (e.min_depth, e.max_depth, e.max_speed, e.max_froude, e.max_courant)):

@@ -85,6 +85,21 @@ def lib() -> ctypes.CDLL:
         "vf_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int32),
         "vf_version": ([], ctypes.c_int32),
         "vf_device_ok": ([], ctypes.c_int32),
+        "vf_set_device": ([ctypes.c_int32], ctypes.c_int32),
+        "vf_event_create": ([ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_event_record": ([_vp, _vp], ctypes.c_int32),
+        "vf_event_elapsed_ms": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], ctypes.c_int32),
+        "vf_event_destroy": ([_vp], None),
+        "vf_host_register": ([_vp, ctypes.c_size_t], ctypes.c_int32),
+        "vf_host_unregister": ([_vp], ctypes.c_int32),
+        "vf_mpm3_profile": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_profile_read": ([_vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t,
+                                  ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int32),
+        "vf_mpm3_launches": ([_vp], ctypes.c_int64),
+        "vf_swe_profile": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_profile_read": ([_vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t,
+                                 ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int32),
+        "vf_swe_launches": ([_vp], ctypes.c_int64),
         "vf_mpm2_create": ([ctypes.c_int32] * 3 + [ctypes.c_uint32, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm2_load": ([_vp] + [_f32p] * 5 + [_i32p, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
@@ -135,7 +150,7 @@ def lib() -> ctypes.CDLL:
         "vf_swe_dispatched": ([_vp], ctypes.c_int64),
         "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_read_budget": ([_vp, ctypes.c_int32, _i32p], ctypes.c_int32),
-        "vf_swe_diagnostics": ([_vp, ctypes.c_double, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
+        "vf_swe_diagnostics": ([_vp] + [ctypes.c_double] * 5 + [ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
         "vf_swe_stream": ([_vp], _vp),
         "vf_swe_on_gpu": ([_vp], ctypes.c_int32),
         "vf_swe_destroy": ([_vp], None),
@@ -189,6 +204,64 @@ def _words(params) -> np.ndarray:
 
 def _bits(v: float) -> int:
     return int(np.array([v], dtype=np.float32).view(np.int32)[0])
+
+
+def _profile_read(fn, h):
+    """{kernel name: (total ms, launches)} from a handle's profiler."""
+    out = {}
+    k = 0
+    buf = ctypes.create_string_buffer(128)
+    while True:
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        if fn(h, k, buf, len(buf), ctypes.byref(ms), ctypes.byref(n)) != VF_OK:
+            break
+        out[buf.value.decode()] = (ms.value, n.value)
+        k += 1
+    return out
+
+
+class Event:
+    """A CUDA event, recorded on a handle's stream."""
+
+    def __init__(self):
+        e = _vp()
+        check(lib().vf_event_create(ctypes.byref(e)))
+        self._e = e
+
+    def record(self, stream) -> None:
+        check(lib().vf_event_record(self._e, stream))
+
+    def elapsed_ms(self, stop: "Event") -> float:
+        ms = ctypes.c_float()
+        check(lib().vf_event_elapsed_ms(self._e, stop._e, ctypes.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        try:
+            lib().vf_event_destroy(self._e)
+        except Exception:
+            pass
+
+
+def set_device(device: int) -> None:
+    check(lib().vf_set_device(device))
+
+
+class Pinned:
+    """Pins numpy arrays' host memory for the duration of a with-block (cudaHostRegister)."""
+
+    def __init__(self, *arrays):
+        self.arrays = [a for a in arrays if a.nbytes]
+
+    def __enter__(self):
+        for a in self.arrays:
+            check(lib().vf_host_register(a.ctypes.data, a.nbytes))
+        return self
+
+    def __exit__(self, *exc):
+        for a in self.arrays:
+            lib().vf_host_unregister(a.ctypes.data)
 
 
 # ------------------------------------------------------------------------------------- params
@@ -500,6 +573,15 @@ class ParticleSimulation3:
         check(lib().vf_mpm3_touched_nodes(self._h, ctypes.byref(out)))
         return out.value
 
+    def profile(self, enable: bool) -> None:
+        check(lib().vf_mpm3_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        return _profile_read(lib().vf_mpm3_profile_read, self._h)
+
+    def launches(self) -> int:
+        return int(lib().vf_mpm3_launches(self._h))
+
     def particle_diagnostics(self, speed, sound, dt):
         out = (ctypes.c_double * 7)()
         check(lib().vf_mpm3_particle_diagnostics(self._h, speed, sound, dt, out))
@@ -619,10 +701,20 @@ class PatchSimulation:
         check(lib().vf_swe_read_budget(self._h, slot, ctypes.byref(v)))
         return v.value
 
-    def diagnostics(self, dt: float):
+    def diagnostics(self, g, dry, dt, dx, dy):
+        """Diagnostics.of(h, hu, hv, g, dry, dt, dx, dy) of the current state, reduced on the device."""
         out = (ctypes.c_double * 9)()
-        check(lib().vf_swe_diagnostics(self._h, dt, out))
+        check(lib().vf_swe_diagnostics(self._h, g, dry, dt, dx, dy, out))
         return list(out)
+
+    def profile(self, enable: bool) -> None:
+        check(lib().vf_swe_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        return _profile_read(lib().vf_swe_profile_read, self._h)
+
+    def launches(self) -> int:
+        return int(lib().vf_swe_launches(self._h))
 
     def stream(self) -> int:
         return lib().vf_swe_stream(self._h)

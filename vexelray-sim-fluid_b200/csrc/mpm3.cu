@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "mpm3_kernels.cuh"
+#include "profiler.cuh"
 
 using namespace vf;
 
@@ -48,6 +49,7 @@ struct vf_mpm3 {
     bool counted = false;     // cell/brick counts and key/rank hold the current positions' keys
     bool sorted_valid = false;
     bool loaded = false;
+    Profiler prof;
 };
 
 struct vf_mpm3_prepared {
@@ -118,8 +120,7 @@ int32_t reset_counts(vf_mpm3* h) {
 int32_t run_sort(vf_mpm3* h, int g, bool will_scatter) {
     Step3 s = make_step(h);
     if (!h->counted) {
-        k_key_count3<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
-        VF_CHECK_LAUNCH();
+        VF_LAUNCH(h->prof, "k_key_count3", h->stream, k_key_count3, div_up(h->np, 256), 256, 0, s);
     }
     // the old windows of grid[g] must be cleared before its brick list is overwritten; a sort with
     // no scatter after it leaves the grid alone and marks it for a dense clear instead
@@ -128,25 +129,19 @@ int32_t run_sort(vf_mpm3* h, int g, bool will_scatter) {
         s.grid = h->grid[g].as<float4>();
         s.active = h->active[g].as<int>();
         s.n_active = h->n_active.as<int>() + g;
-        k_clear_bricks3<<<persistent_blocks(8), 256, 0, h->stream>>>(s);
-        VF_CHECK_LAUNCH();
+        VF_LAUNCH(h->prof, "k_clear_bricks3", h->stream, k_clear_bricks3, persistent_blocks(8), 256, 0, s);
         h->grid_dirty[g] = 0;
     }
     int* active = h->active[g].as<int>();
     int* n_active = h->n_active.as<int>() + g;
-    k_brick_scan<<<1, 1024, 0, h->stream>>>(h->brick_count.as<int>(), h->brick_start.as<int>(), active, n_active,
+    VF_LAUNCH(h->prof, "k_brick_scan", h->stream, k_brick_scan, 1, 1024, 0, h->brick_count.as<int>(), h->brick_start.as<int>(), active, n_active,
                                            h->nbricks);
-    VF_CHECK_LAUNCH();
-    k_cell_scan<<<persistent_blocks(4), 512, 0, h->stream>>>(h->cell_count.as<int>(), h->cell_start.as<int>(),
+    VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(), h->cell_start.as<int>(),
                                                           h->brick_start.as<int>(), active, n_active);
-    VF_CHECK_LAUNCH();
-    k_permute<<<div_up(h->np, 256), 256, 0, h->stream>>>(h->key.as<int>(), h->rank.as<int>(),
-                                                          h->cell_start.as<int>(), h->perm.as<int>(), h->np,
-                                                          h->status.as<uint32_t>());
-    VF_CHECK_LAUNCH();
-    k_fixup_bricks<<<persistent_blocks(2), 512, 12288 * sizeof(int), h->stream>>>(
+    VF_LAUNCH(h->prof, "k_permute", h->stream, k_permute, div_up(h->np, 256), 256, 0, h->key.as<int>(),
+              h->rank.as<int>(), h->cell_start.as<int>(), h->perm.as<int>(), h->np, h->status.as<uint32_t>());
+    VF_LAUNCH(h->prof, "k_fixup_bricks", h->stream, k_fixup_bricks, persistent_blocks(2), 512, 12288 * sizeof(int), 
         h->perm.as<int>(), h->cell_start.as<int>(), h->brick_start.as<int>(), active, n_active);
-    VF_CHECK_LAUNCH();
     h->counted = false;
     h->sorted_valid = true;
     return VF_OK;
@@ -185,11 +180,11 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_SCATTER) {
         if (tile) {
-            k_p2g3_tile<<<persistent_blocks(1), 256, 0, h->stream>>>(s);
+            VF_LAUNCH(h->prof, "k_p2g3_tile", h->stream, k_p2g3_tile, persistent_blocks(1), 256, 0, s);
         } else if (h->p2g == VF_P2G_WARP) {
-            k_p2g3_warp<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+            VF_LAUNCH(h->prof, "k_p2g3_warp", h->stream, k_p2g3_warp, div_up(h->np, 256), 256, 0, s);
         } else {
-            k_p2g3_atomic<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
+            VF_LAUNCH(h->prof, "k_p2g3_atomic", h->stream, k_p2g3_atomic, div_up(h->np, 256), 256, 0, s);
         }
         VF_CHECK_LAUNCH();
         h->grid_dirty[g] = tile ? 1 : 2;
@@ -198,24 +193,20 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     if (mask & VF3_PASS_ADVECT) {
         s.count_next = count_next ? 1 : 0;
         if (tile) {
-            k_g2p3_tile<<<persistent_blocks(2), 256, 0, h->stream>>>(s);
-            VF_CHECK_LAUNCH();
+            VF_LAUNCH(h->prof, "k_g2p3_tile", h->stream, k_g2p3_tile, persistent_blocks(2), 256, 0, s);
         } else {
-            k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
-            VF_CHECK_LAUNCH();
-            k_g2p3<<<div_up(h->np, 256), 256, 0, h->stream>>>(s);
-            VF_CHECK_LAUNCH();
+            VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
+            VF_LAUNCH(h->prof, "k_g2p3", h->stream, k_g2p3, div_up(h->np, 256), 256, 0, s);
         }
         if (sort) h->cur ^= 1;
         h->counted = count_next;
     } else if (mask & VF3_PASS_GRID) {
-        k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
-        VF_CHECK_LAUNCH();
+        VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
     }
     if (sort && !(mask & VF3_PASS_ADVECT)) {
         // the particles were not moved to their sorted slots; apply the permutation as a copy
-        k_gather_fields<<<div_up(h->np, 256), 256, 0, h->stream>>>(s.in, s.out, s.perm, h->np, h->stride, NF3);
-        VF_CHECK_LAUNCH();
+        VF_LAUNCH(h->prof, "k_gather_fields", h->stream, k_gather_fields, div_up(h->np, 256), 256, 0, s.in, s.out,
+                  s.perm, h->np, h->stride, (int)NF3);
         h->cur ^= 1;
     }
     if (mask & VF3_PASS_SCATTER) h->passes_run++;
@@ -535,6 +526,20 @@ int32_t vf_mpm3_particle_diagnostics(vf_mpm3* h, double speed, double sound, dou
 }
 
 int64_t vf_mpm3_steps(const vf_mpm3* h) { return h ? h->steps : 0; }
+
+int32_t vf_mpm3_profile(vf_mpm3* h, int32_t enable) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->prof.reset();
+    h->prof.on = enable != 0;
+    return VF_OK;
+}
+
+int32_t vf_mpm3_profile_read(vf_mpm3* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    return h->prof.read(index, name, cap, total_ms, launches);
+}
+
+int64_t vf_mpm3_launches(const vf_mpm3* h) { return h ? h->prof.launches : 0; }
 
 int32_t vf_mpm3_on_gpu(const vf_mpm3* h) { return h ? 1 : 0; }
 

@@ -1,52 +1,7 @@
-// sort.cu -- kernels of the stable counting sort by cell (see sort.cuh), and the library's
-// error/device plumbing.
-#include <stdarg.h>
-
+// sort.cu -- kernels of the stable counting sort by cell (see sort.cuh).
 #include "sort.cuh"
 
 namespace vf {
-
-// ------------------------------------------------------------------ errors and device
-
-static thread_local char g_error[1024] = "";
-
-void set_error(const char* fmt, ...) {
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(g_error, sizeof g_error, fmt, ap);
-    va_end(ap);
-}
-
-const char* last_error() { return g_error; }
-
-int32_t require_device() {
-    int n = 0;
-    cudaError_t e = cudaGetDeviceCount(&n);
-    if (e != cudaSuccess || n == 0) {
-        set_error("no CUDA device: %s", e == cudaSuccess ? "none found" : cudaGetErrorString(e));
-        cudaGetLastError();
-        return VF_ENODEV;
-    }
-    int dev = 0, major = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (major != 10) {
-        set_error("libvexfluid is built for sm_100a (B200); device %d is compute capability %d.x", dev, major);
-        return VF_ENODEV;
-    }
-    return VF_OK;
-}
-
-int sm_count() {
-    static int cached = 0;
-    if (!cached) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
-        if (cached <= 0) cached = 148;
-    }
-    return cached;
-}
 
 // ------------------------------------------------------------------ scans
 
@@ -200,19 +155,3 @@ __global__ void k_gather_fields(const float* __restrict__ in, float* __restrict_
 
 }  // namespace vf
 
-// ------------------------------------------------------------------ C-ABI: errors and device
-
-extern "C" int32_t vf_last_error(char* buf, size_t cap) {
-    const char* e = vf::last_error();
-    size_t n = strlen(e);
-    if (buf && cap) {
-        size_t k = n < cap - 1 ? n : cap - 1;
-        memcpy(buf, e, k);
-        buf[k] = 0;
-    }
-    return (int32_t)n;
-}
-
-extern "C" int32_t vf_version(void) { return 1; }
-
-extern "C" int32_t vf_device_ok(void) { return vf::require_device() == VF_OK ? 1 : 0; }

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <vector>
 
+#include "profiler.cuh"
 #include "sort.cuh"
 
 using namespace vf;
@@ -391,6 +392,7 @@ struct vf_swe {
     int64_t total_steps = 0;
     int64_t last_step = 0;
     float host_params[5];
+    Profiler prof;
 };
 
 namespace {
@@ -435,8 +437,8 @@ int32_t dispatch(vf_swe* h) {
     a.use_tma = h->tma ? 1 : 0;
     dim3 grid(div_up(h->nx, TX), div_up(h->ny, TY));
     const CUtensorMap* m = h->maps[si];
-    k_swe_tile<<<grid, SWE_THREADS, sizeof(SweShared) + 128, h->stream>>>(a, m[0], m[1], m[2]);
-    VF_CHECK_LAUNCH();
+    VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile, grid, SWE_THREADS, sizeof(SweShared) + 128, a, m[0], m[1],
+              m[2]);
     h->dispatched++;
     return VF_OK;
 }
@@ -651,12 +653,12 @@ int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks) {
     return rc ? rc : status_swe(h);
 }
 
-int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]) {
+int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]) {
     VF_REQUIRE(h && out, VF_EINVAL, "null argument");
     const int s = (int)(h->dispatched % 2);
     const int blocks = 1184;
     k_swe_diag<<<blocks, 256, 0, h->stream>>>(field(h, s, 0), field(h, s, 1), field(h, s, 2), h->cells,
-                                              (double)h->host_params[0], (double)h->host_params[4],
+                                              g, dry,
                                               h->diag.as<DiagPart>());
     VF_CHECK_LAUNCH();
     std::vector<DiagPart> parts(blocks);
@@ -674,7 +676,6 @@ int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]) {
         t.negative += p.negative;
         t.wet += p.wet;
     }
-    const double dx = h->host_params[2], dy = h->host_params[3];
     out[0] = t.volume * dx * dy;
     out[1] = t.wet == 0 ? 0 : t.min_depth;
     out[2] = t.max_depth;
@@ -688,6 +689,20 @@ int32_t vf_swe_diagnostics(vf_swe* h, double dt, double out[9]) {
 }
 
 void* vf_swe_stream(vf_swe* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t vf_swe_profile(vf_swe* h, int32_t enable) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->prof.reset();
+    h->prof.on = enable != 0;
+    return VF_OK;
+}
+
+int32_t vf_swe_profile_read(vf_swe* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    return h->prof.read(index, name, cap, total_ms, launches);
+}
+
+int64_t vf_swe_launches(const vf_swe* h) { return h ? h->prof.launches : 0; }
 
 int32_t vf_swe_on_gpu(const vf_swe* h) { return h ? 1 : 0; }
 
