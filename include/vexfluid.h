@@ -134,6 +134,16 @@ int32_t vf_fixed_scatter2(int32_t nx, int32_t ny, const float* x, const float* y
  * SortTest.java:255-313), stable: writes the permutation (perm[d] = source index) and the starts. */
 int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm,
                  int32_t* starts);
+/* vf_sort2 without any device allocation. No counterpart in the reference: it is for callers that must
+ * not allocate device memory while they run -- a host that budgets all device memory up front, or a
+ * real-time loop where cudaMalloc/cudaFree would synchronise the device and stall the frame. Its scratch
+ * is one fixed array in the library (about 7 MB, held on every GPU that loads the library until exit), so
+ * it takes at most 262144 particles and 262144 cells ((nx-1)(ny-1)); larger inputs get VF_EINVAL. Every
+ * call shares that array: calls that overlap on the GPU race, so a caller with several threads or streams
+ * serialises them. The first call on a device looks up the array's device address; make it before any
+ * stream capture. Same outputs as vf_sort2. */
+int32_t vf_sort2_noalloc(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm,
+                         int32_t* starts);
 
 /* ------------------------------------------------------------------ 3D particles (ParticleSimulation3) */
 typedef struct vf_mpm3 vf_mpm3;
