@@ -304,6 +304,28 @@ def run_ours(args, dist: Dist):
     kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1], "share": v[0] / total_prof}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
+    # the three P2G schedules the 3D config compares, each for K profiled steps from the same state
+    variants = {}
+    if not args.no_variants:
+        names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile"}
+        for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_TILE):
+            sim.set_schedule(sched)
+            sim.advance(2)
+            sim.finish()
+            sim.profile(True)
+            ev0.record(stream)
+            sim.advance(args.variant_steps)
+            ev1.record(stream)
+            v_ms = ev0.elapsed_ms(ev1)
+            vp = sim.profile_read()
+            sim.profile(False)
+            p2g = [k for k in vp if k.startswith("k_p2g3")]
+            variants[names[sched]] = {
+                "ms_per_step": v_ms / args.variant_steps,
+                "p2g_ms_per_step": sum(vp[k][0] for k in p2g) / args.variant_steps,
+                "kernels_ms_per_step": {k: v[0] / args.variant_steps for k, v in vp.items()}}
+        sim.set_schedule(vf.VF_P2G_TILE)
+
     # end to end through the public API: pinned host arrays in (load), K steps, positions out (read)
     outs = [np.empty(np3, np.float32) for _ in range(3)]
     ins = [x, y, z, zeros, zeros, zeros, m]
@@ -374,6 +396,7 @@ def run_ours(args, dist: Dist):
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "swe": swe,
+        "p2g_variants": variants,
     }
     print(json.dumps(line), flush=True)
 
@@ -386,6 +409,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water sub-measurement")
+    ap.add_argument("--no-variants", action="store_true", help="skip the comparison of the three P2G schedules")
+    ap.add_argument("--variant-steps", type=int, default=20)
     args = ap.parse_args()
     dist = Dist()
     try:

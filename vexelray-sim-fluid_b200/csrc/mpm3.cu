@@ -29,8 +29,8 @@ struct vf_mpm3 {
     cudaStream_t stream = nullptr;
     DeviceBuffer part[2];
     int cur = 0;
-    DeviceBuffer key, rank, perm;
-    DeviceBuffer cell_count, cell_start;
+    DeviceBuffer key, perm;
+    DeviceBuffer cell_count, cell_start, cursor;
     DeviceBuffer brick_count, brick_start;
     DeviceBuffer active[2];   // the non-empty bricks of the step that scattered into grid[g]
     DeviceBuffer n_active;    // int[2]
@@ -94,7 +94,6 @@ Step3 make_step(vf_mpm3* h) {
     s.d = h->d;
     s.status = h->status.as<uint32_t>();
     s.key = h->key.as<int>();
-    s.rank = h->rank.as<int>();
     s.cell_count = h->cell_count.as<int>();
     s.brick_count = h->brick_count.as<int>();
     s.cell_start = h->cell_start.as<int>();
@@ -117,7 +116,7 @@ int32_t reset_counts(vf_mpm3* h) {
 
 // The sort passes, leaving perm = sorted slot -> particle of the current set. `g` is the grid
 // buffer this step scatters into; its brick list is rebuilt here (after its old windows are cleared).
-int32_t run_sort(vf_mpm3* h, int g, bool will_scatter) {
+int32_t run_sort(vf_mpm3* h, int g, bool will_scatter, bool fused_fixup) {
     Step3 s = make_step(h);
     if (!h->counted) {
         VF_LAUNCH(h->prof, "k_key_count3", h->stream, k_key_count3, div_up(h->np, 256), 256, 0, s);
@@ -136,12 +135,15 @@ int32_t run_sort(vf_mpm3* h, int g, bool will_scatter) {
     int* n_active = h->n_active.as<int>() + g;
     VF_LAUNCH(h->prof, "k_brick_scan", h->stream, k_brick_scan, 1, 1024, 0, h->brick_count.as<int>(), h->brick_start.as<int>(), active, n_active,
                                            h->nbricks);
-    VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(), h->cell_start.as<int>(),
+    VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(),
+              h->cell_start.as<int>(), h->cursor.as<int>(),
                                                           h->brick_start.as<int>(), active, n_active);
-    VF_LAUNCH(h->prof, "k_permute", h->stream, k_permute, div_up(h->np, 256), 256, 0, h->key.as<int>(),
-              h->rank.as<int>(), h->cell_start.as<int>(), h->perm.as<int>(), h->np, h->status.as<uint32_t>());
-    VF_LAUNCH(h->prof, "k_fixup_bricks", h->stream, k_fixup_bricks, persistent_blocks(2), 512, 12288 * sizeof(int), 
-        h->perm.as<int>(), h->cell_start.as<int>(), h->brick_start.as<int>(), active, n_active);
+    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256), 256, 0, h->key.as<int>(),
+              h->cursor.as<int>(), h->perm.as<int>(), h->np, h->nkeys, h->status.as<uint32_t>());
+    // the tiled scatter puts each cell's run in order itself; everything else needs the fix-up pass
+    if (!fused_fixup)
+        VF_LAUNCH(h->prof, "k_fixup_bricks", h->stream, k_fixup_bricks, persistent_blocks(2), 512, 12288 * sizeof(int),
+                  h->perm.as<int>(), h->cell_start.as<int>(), h->brick_start.as<int>(), active, n_active);
     h->counted = false;
     h->sorted_valid = true;
     return VF_OK;
@@ -158,7 +160,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
         if (rc) return rc;
     }
     if (sort) {
-        int32_t rc = run_sort(h, g, (mask & VF3_PASS_SCATTER) != 0);
+        int32_t rc = run_sort(h, g, (mask & VF3_PASS_SCATTER) != 0, tile && (mask & VF3_PASS_SCATTER));
         if (rc) return rc;
     }
     Step3 s = make_step(h);
@@ -180,7 +182,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_SCATTER) {
         if (tile) {
-            VF_LAUNCH(h->prof, "k_p2g3_tile", h->stream, k_p2g3_tile, persistent_blocks(1), 256, 0, s);
+            VF_LAUNCH(h->prof, "k_p2g3_tile", h->stream, k_p2g3_tile, persistent_blocks(2), 128, p2g_tile_smem(), s);
         } else if (h->p2g == VF_P2G_WARP) {
             VF_LAUNCH(h->prof, "k_p2g3_warp", h->stream, k_p2g3_warp, div_up(h->np, 256), 256, 0, s);
         } else {
@@ -193,7 +195,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     if (mask & VF3_PASS_ADVECT) {
         s.count_next = count_next ? 1 : 0;
         if (tile) {
-            VF_LAUNCH(h->prof, "k_g2p3_tile", h->stream, k_g2p3_tile, persistent_blocks(2), 256, 0, s);
+            VF_LAUNCH(h->prof, "k_g2p3_tile", h->stream, k_g2p3_tile, persistent_blocks(4), 256, 0, s);
         } else {
             VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
             VF_LAUNCH(h->prof, "k_g2p3", h->stream, k_g2p3, div_up(h->np, 256), 256, 0, s);
@@ -278,7 +280,7 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
     }
     size_t pbytes = (size_t)h->stride * NF3 * sizeof(float);
     if ((rc = h->part[0].alloc(pbytes)) || (rc = h->part[1].alloc(pbytes)) ||
-        (rc = h->key.alloc((size_t)particles * 4)) || (rc = h->rank.alloc((size_t)particles * 4)) ||
+        (rc = h->key.alloc((size_t)particles * 4)) || (rc = h->cursor.alloc((size_t)h->nkeys * 4)) ||
         (rc = h->perm.alloc((size_t)particles * 4)) || (rc = h->cell_count.alloc((size_t)h->nkeys * 4)) ||
         (rc = h->cell_start.alloc((size_t)(h->nkeys + 1) * 4)) ||
         (rc = h->brick_count.alloc((size_t)h->nbricks * 4)) ||
@@ -288,6 +290,11 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
         (rc = h->grid[1].alloc((size_t)h->nodes * 16)) || (rc = h->vel.alloc((size_t)h->nodes * 16)) ||
         (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)))
         return fail(rc);
+    if (cudaFuncSetAttribute(k_p2g3_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_tile_smem()) !=
+        cudaSuccess) {
+        set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem());
+        return fail(VF_ECUDA);
+    }
     vf_mpm3_prepared* p = new vf_mpm3_prepared();
     p->sim = h;
     *out = p;
@@ -312,7 +319,7 @@ int32_t vf_mpm3_create(vf_mpm3_prepared* p, vf_mpm3** out) {
     p->sim = nullptr;
     delete p;
     // ParticleSimulation3(Prepared) clears every buffer (runner.clear(), ParticleSimulation3.java:189)
-    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->rank, &h->perm, &h->cell_count, &h->cell_start,
+    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->cursor, &h->perm, &h->cell_count, &h->cell_start,
                             &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
                             &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch}) {
         if (cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream) != cudaSuccess) {
@@ -546,7 +553,7 @@ int32_t vf_mpm3_on_gpu(const vf_mpm3* h) { return h ? 1 : 0; }
 void vf_mpm3_destroy(vf_mpm3* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->rank, &h->perm, &h->cell_count, &h->cell_start,
+    for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->cursor, &h->perm, &h->cell_count, &h->cell_start,
                             &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
                             &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch})
         b->release();

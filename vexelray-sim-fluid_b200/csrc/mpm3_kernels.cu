@@ -13,12 +13,9 @@ __global__ void __launch_bounds__(256) k_key_count3(Step3 s) {
     const bool valid = i < s.np;
     int key = 0;
     if (valid) key = key3_of(s.in[X * s.stride + i], s.in[Y * s.stride + i], s.in[Z * s.stride + i], s.d);
-    int r = warp_count(s.cell_count, key, valid, s.nkeys, s.status);
+    warp_tally(s.cell_count, key, valid, s.nkeys, s.status);
     warp_tally(s.brick_count, key >> 9, valid, s.nbricks, s.status);
-    if (valid) {
-        s.key[i] = key;
-        s.rank[i] = r;
-    }
+    if (valid) s.key[i] = key;
 }
 
 // ------------------------------------------------------------------ P2G: direct atomics
@@ -150,122 +147,196 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 
 // ------------------------------------------------------------------ P2G: sorted brick tile
 
-// One CTA per non-empty 8^3-cell brick (persistent over the list). Each thread owns one stencil
-// cell of the brick and sums the 27 x 4 deposits of that cell's particles in registers; the cell
-// sums land in a shared-memory window of the brick's 10^3 nodes (no two lanes of a warp hit one
-// node, since their cells differ), and the window goes to HBM with one vector reduction per
-// touched node. The per-particle arithmetic is Flip3.scatter's, regrouped so each node costs one
-// weight, one mass FMA and three momentum FMAs:
-//   momentum_a(node o) = w(o) * (A_a + sum_e B_ae o_e),
-//   A_a = m (v_a - sum_e C_ae f_e) - s f_a,   B_ae = m C_ae + s [a == e],
-// which is (w m)(v_a + C_a . d) + w s d_a with d = o - f.
-constexpr int P2G_THREADS = 256;
+// Each warp takes work units of (non-empty brick, slab of 8 x 4 x 1 cells), sixteen per brick, with no
+// barrier between warps.
+//
+//  1. Lane l owns cell (l % 8, l / 8) of the slab. It first puts its cell's run of the sort's permutation
+//     in ascending order, in place (the stable sort's fix-up, fused here: G2P then reads the stable
+//     permutation), then sums the 27 x 4 deposits of the cell's particles in registers, loading two
+//     particles ahead of the one it sums. A slab's cells are 32 consecutive keys, so their particle
+//     runs form one contiguous range.
+//  2. The slab's deposits reach a 10 x 6 x 3 node window, private to the warp in shared memory. At one
+//     stencil offset the 32 lanes hit 32 different nodes, so the window takes the cell sums by plain
+//     read-modify-write, a __syncwarp between offsets: no shared-memory atomics.
+//  3. The warp reduces every touched node of its window into the grid with one 16-byte vector
+//     reduction (red.global.add.v4.f32); neighbouring slabs' windows overlap, and the reductions add.
+//
+// The per-particle arithmetic is Flip3.scatter's regrouped so a node costs a weight, one mass FMA and
+// three momentum FMAs:  momentum_a(node o) = w(o) (A_a + sum_e B_ae o_e),
+//   A_a = m (v_a - sum_e C_ae f_e) - s f_a,  B_ae = m C_ae + s [a == e],
+// which is (w m)(v_a + C_a . d) + w s d_a with d = o - f (Flip3.java:225-243).
+constexpr int P2G_THREADS = 128;
+constexpr int P2G_WARPS = P2G_THREADS / 32;
+constexpr int WWX = WIN, WWY = 6, WWZ = 3, WW = WWX * WWY * WWZ;   // a warp's window: 180 nodes
 
-__global__ void __launch_bounds__(P2G_THREADS) k_p2g3_tile(Step3 s) {
-    __shared__ float win[4][WIN3];
+struct P2GShared {
+    float4 wwin[P2G_WARPS][WW];
+};
+constexpr size_t P2G_SMEM = sizeof(P2GShared);
+// One particle's fields, as the scatter reads them.
+struct PIn {
+    float x, y, z, u, v, w, m, j, c[9];
+};
+
+__device__ __forceinline__ void load_pin(PIn& q, const float* __restrict__ in, int64_t st, int src) {
+    const float* b = in + src;
+    q.x = b[X * st];
+    q.y = b[Y * st];
+    q.z = b[Z * st];
+    q.u = b[U * st];
+    q.v = b[V * st];
+    q.w = b[W * st];
+    q.m = b[M * st];
+    q.j = b[J * st];
+#pragma unroll
+    for (int a = 0; a < 9; a++) q.c[a] = b[(C00 + a) * st];
+}
+
+__device__ __forceinline__ int checked_src(const int* run, int i, int np, uint32_t* status) {
+    int src = run[i];
+    if ((unsigned)src >= (unsigned)np) {
+        set_status(status, ST_OOB);
+        src = 0;
+    }
+    return src;
+}
+
+__global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
+    extern __shared__ __align__(16) unsigned char p2g_raw[];
+    P2GShared& S = *reinterpret_cast<P2GShared*>(p2g_raw);
     const Params3 p = *s.params;
+    const float vol = __fdiv_rn(1.0f, p.rho0);                 // V0 = m / rho0 as m * (1/rho0)
+    const float k4dt = 4.0f * p.dt;
     const Dims3 dm = s.d;
     const int64_t st = s.stride;
-    const float* in = s.in;
-    const int na = *s.n_active;
-    for (int a = blockIdx.x; a < na; a += gridDim.x) {
-        const int b = s.active[a];
+    const float* __restrict__ in = s.in;
+    int* __restrict__ perm = s.perm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lx = lane & 7, lyl = lane >> 3;
+    float4* ww = S.wwin[warp];
+    const int units = *s.n_active * 16;
+    const int total_warps = gridDim.x * P2G_WARPS;
+    for (int u = blockIdx.x * P2G_WARPS + warp; u < units; u += total_warps) {
+        const int b = s.active[u >> 4], q = u & 15;
         const int bx = b % dm.nbx, by = (b / dm.nbx) % dm.nby, bz = b / (dm.nbx * dm.nby);
         const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK;
-        for (int i = threadIdx.x; i < 4 * WIN3; i += P2G_THREADS) (&win[0][0])[i] = 0.0f;
-        __syncthreads();
-        const int be = s.brick_start[b + 1];
-        for (int c = threadIdx.x; c < 512; c += P2G_THREADS) {
-            const int64_t key = (int64_t)b * 512 + c;
-            int s0 = s.cell_start[key];
-            int s1 = c < 511 ? s.cell_start[key + 1] : be;
-            if (s0 < 0 || s1 > s.np) {   // a run outside the particles: flagged, and clipped
+        int bs = s.brick_start[b], be = s.brick_start[b + 1];
+        if (bs < 0 || be > s.np || be < bs) {
+            set_status(s.status, ST_OOB);
+            bs = max(bs, 0);
+            be = min(max(be, bs), s.np);
+        }
+        const int lz = q >> 1, ly0 = (q & 1) * 4, ly = ly0 + lyl;
+        const int c = (lz * 8 + ly) * 8 + lx;
+        const int64_t key = (int64_t)b * 512 + c;
+        const int s0 = min(max(s.cell_start[key], bs), be);
+        const int s1 = min(max(c < 511 ? s.cell_start[key + 1] : be, s0), be);
+        if (!__any_sync(0xffffffffu, s1 > s0)) continue;          // an empty slab (warp-uniform)
+
+        // 1. the stable order of this cell's run, then its particles summed in registers
+        if (s1 - s0 > 1) insertion_sort_run(perm + s0, s1 - s0);
+        float acc[27][4];
+#pragma unroll
+        for (int k = 0; k < 27; k++) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+        PIn nxt, nxt2;
+        if (s0 < s1) load_pin(nxt, in, st, checked_src(perm, s0, s.np, s.status));
+        if (s0 + 1 < s1) load_pin(nxt2, in, st, checked_src(perm, s0 + 1, s.np, s.status));
+        for (int i = s0; i < s1; i++) {
+            const PIn qq = nxt;
+            nxt = nxt2;
+            if (i + 2 < s1) load_pin(nxt2, in, st, checked_src(perm, i + 2, s.np, s.status));
+            if (!(qq.m > 0.0f)) continue;
+            int cell[3];
+            float f[3];
+            stencil_axis(qq.x, dm.nx, cell[0], f[0]);
+            stencil_axis(qq.y, dm.ny, cell[1], f[1]);
+            stencil_axis(qq.z, dm.nz, cell[2], f[2]);
+            if (cell[0] != cx0 + lx || cell[1] != cy0 + ly || cell[2] != cz0 + lz) {
                 set_status(s.status, ST_OOB);
-                s0 = max(s0, 0);
-                s1 = min(s1, s.np);
+                continue;
             }
-            if (s0 >= s1) continue;
-            const int lx = c & 7, ly = (c >> 3) & 7, lz = c >> 6;
-            float acc[27][4];
+            float wx[3], wy[3], wz[3];
 #pragma unroll
-            for (int k = 0; k < 27; k++) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
-            for (int i = s0; i < s1; i++) {
-                const int src = s.perm ? s.perm[i] : i;
-                if ((unsigned)src >= (unsigned)s.np) {
-                    set_status(s.status, ST_OOB);
-                    continue;
-                }
-                const float m = in[M * st + src];
-                if (!(m > 0.0f)) continue;
-                int cell[3];
-                float f[3];
-                stencil_axis(in[X * st + src], dm.nx, cell[0], f[0]);
-                stencil_axis(in[Y * st + src], dm.ny, cell[1], f[1]);
-                stencil_axis(in[Z * st + src], dm.nz, cell[2], f[2]);
-                if (cell[0] != cx0 + lx || cell[1] != cy0 + ly || cell[2] != cz0 + lz) {
-                    set_status(s.status, ST_OOB);
-                    continue;
-                }
-                float wx[3], wy[3], wz[3];
-                bspline_weights(f[0], wx);
-                bspline_weights(f[1], wy);
-                bspline_weights(f[2], wz);
-                const float sp = impulse_factor(p.dt, m, p.rho0, p.bulk, in[J * st + src], p.tait);
-                const float vel[3] = {in[U * st + src], in[V * st + src], in[W * st + src]};
-                float A[3], B[3][3];
+            for (int e = 0; e < 3; e++) {
+                float* we = e == 0 ? wx : e == 1 ? wy : wz;
+                const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
+                we[0] = 0.5f * (ta * ta);
+                we[1] = 0.75f - tc * tc;
+                we[2] = 0.5f * (te * te);
+            }
+            float jp;
+            if (p.tait) {
+                const float r = __frcp_rn(qq.j), r2 = r * r;
+                jp = p.bulk * ((r2 * r2) * r2 - qq.j);
+            } else {
+                jp = p.bulk * (1.0f - qq.j);
+            }
+            const float sp = (k4dt * (qq.m * vol)) * jp;
+            const float vel[3] = {qq.u, qq.v, qq.w};
+            float A[3], B[3][3];
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    const float c0 = in[(C00 + 3 * q) * st + src], c1 = in[(C00 + 3 * q + 1) * st + src],
-                                c2 = in[(C00 + 3 * q + 2) * st + src];
-                    const float cf = c0 * f[0] + c1 * f[1] + c2 * f[2];
-                    A[q] = m * (vel[q] - cf) - sp * f[q];
-                    B[q][0] = m * c0;
-                    B[q][1] = m * c1;
-                    B[q][2] = m * c2;
-                    B[q][q] += sp;
-                }
+            for (int r = 0; r < 3; r++) {
+                const float c0 = qq.c[3 * r], c1 = qq.c[3 * r + 1], c2 = qq.c[3 * r + 2];
+                A[r] = qq.m * (vel[r] - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[r];
+                B[r][0] = qq.m * c0;
+                B[r][1] = qq.m * c1;
+                B[r][2] = qq.m * c2;
+                B[r][r] += sp;
+            }
 #pragma unroll
-                for (int oz = 0; oz < 3; oz++) {
+            for (int oz = 0; oz < 3; oz++) {
 #pragma unroll
-                    for (int oy = 0; oy < 3; oy++) {
-                        const float wyz = wy[oy] * wz[oz];
-                        const float mw = m * wyz;
-                        float T[3];
+                for (int oy = 0; oy < 3; oy++) {
+                    const float wyz = wy[oy] * wz[oz];
+                    const float mw = qq.m * wyz;
+                    float T[3];
 #pragma unroll
-                        for (int q = 0; q < 3; q++) T[q] = A[q] + (float)oy * B[q][1] + (float)oz * B[q][2];
+                    for (int r = 0; r < 3; r++) T[r] = A[r] + (float)oy * B[r][1] + (float)oz * B[r][2];
 #pragma unroll
-                        for (int ox = 0; ox < 3; ox++) {
-                            const int k = (oz * 3 + oy) * 3 + ox;
-                            const float w = wx[ox] * wyz;
-                            acc[k][0] += wx[ox] * mw;
+                    for (int ox = 0; ox < 3; ox++) {
+                        const int k = (oz * 3 + oy) * 3 + ox;
+                        const float w = wx[ox] * wyz;
+                        acc[k][0] += wx[ox] * mw;
 #pragma unroll
-                            for (int q = 0; q < 3; q++) acc[k][1 + q] += w * (T[q] + (float)ox * B[q][0]);
-                        }
+                        for (int r = 0; r < 3; r++) acc[k][1 + r] += w * (T[r] + (float)ox * B[r][0]);
                     }
                 }
             }
-#pragma unroll
-            for (int k = 0; k < 27; k++) {
-                const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
-                const int wi = ((lz + oz) * WIN + (ly + oy)) * WIN + (lx + ox);
-#pragma unroll
-                for (int q = 0; q < 4; q++) atomicAdd(&win[q][wi], acc[k][q]);
-            }
         }
-        __syncthreads();
-        for (int wi = threadIdx.x; wi < WIN3; wi += P2G_THREADS) {
-            const float m = win[0][wi];
-            if (m == 0.0f && win[1][wi] == 0.0f && win[2][wi] == 0.0f && win[3][wi] == 0.0f) continue;
-            const int gx = cx0 + wi % WIN, gy = cy0 + (wi / WIN) % WIN, gz = cz0 + wi / (WIN * WIN);
+
+        // 2. into the warp's window (__syncwarp orders each offset's writes before the next's reads)
+        __syncwarp();
+        for (int j = lane; j < WW; j += 32) ww[j] = make_float4(0, 0, 0, 0);
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 27; k++) {
+            const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
+            const int wi = (oz * WWY + lyl + oy) * WWX + lx + ox;
+            float4 v = ww[wi];
+            v.x += acc[k][0];
+            v.y += acc[k][1];
+            v.z += acc[k][2];
+            v.w += acc[k][3];
+            ww[wi] = v;
+            __syncwarp();
+        }
+
+        // 3. the window's touched nodes into the grid
+        for (int j = lane; j < WW; j += 32) {
+            const float4 t = ww[j];
+            if (t.x == 0.0f && t.y == 0.0f && t.z == 0.0f && t.w == 0.0f) continue;
+            const int gx = cx0 + j % WWX, gy = cy0 + ly0 + (j / WWX) % WWY, gz = cz0 + lz + j / (WWX * WWY);
             if (gx >= dm.nx || gy >= dm.ny || gz >= dm.nz) {
                 set_status(s.status, ST_OOB);
                 continue;
             }
-            red_add_v4(&s.grid[((int64_t)gz * dm.ny + gy) * dm.nx + gx], m, win[1][wi], win[2][wi], win[3][wi]);
+            red_add_v4(&s.grid[((int64_t)gz * dm.ny + gy) * dm.nx + gx], t.x, t.y, t.z, t.w);
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
+
+size_t p2g_tile_smem() { return P2G_SMEM; }
 
 // ------------------------------------------------------------------ grid update (dense)
 
@@ -302,12 +373,9 @@ __device__ __forceinline__ void g2p_store(const Step3& s, int d, const float pos
 __device__ __forceinline__ void g2p_count(const Step3& s, int d, bool valid, const float pos[3]) {
     if (!s.count_next) return;
     int key = valid ? key3_of(pos[0], pos[1], pos[2], s.d) : 0;
-    int r = warp_count(s.cell_count, key, valid, s.nkeys, s.status);
+    warp_tally(s.cell_count, key, valid, s.nkeys, s.status);
     warp_tally(s.brick_count, key >> 9, valid, s.nbricks, s.status);
-    if (valid) {
-        s.key[d] = key;
-        s.rank[d] = r;
-    }
+    if (valid) s.key[d] = key;
 }
 
 // A particle the reference's advect skips (m <= 0, Flip3.java:342) keeps its state; when the
@@ -412,27 +480,53 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
         }
         __syncthreads();
         int bs = s.brick_start[b], be = s.brick_start[b + 1];
-        if (bs < 0 || be > s.np) {
+        if (bs < 0 || be > s.np || be < bs) {
             set_status(s.status, ST_OOB);
             bs = max(bs, 0);
-            be = min(be, s.np);
+            be = min(max(be, bs), s.np);
         }
-        // Every thread walks the same number of iterations so the warp-level count is converged.
-        const int span = be - bs;
-        const int iters = (span + G2P_THREADS - 1) / G2P_THREADS;
+        // Every thread walks the same number of iterations so the warp-level count is converged. The
+        // permutation is read two iterations ahead and the particle one iteration ahead of its use.
+        const int iters = (be - bs + G2P_THREADS - 1) / G2P_THREADS;
+        const int d0 = bs + threadIdx.x;
+        auto src_of = [&](int d) {
+            int v = d < be ? (s.perm ? s.perm[d] : d) : -1;
+            if (d < be && (unsigned)v >= (unsigned)s.np) {
+                set_status(s.status, ST_OOB);
+                v = -1;
+            }
+            return v;
+        };
+        int src_a = src_of(d0);
+        int src_b = src_of(d0 + G2P_THREADS);
+        float nx_ = 0, ny_ = 0, nz_ = 0, nm_ = 0, nj_ = 0;
+        if (src_a >= 0) {
+            nx_ = s.in[X * st + src_a];
+            ny_ = s.in[Y * st + src_a];
+            nz_ = s.in[Z * st + src_a];
+            nm_ = s.in[M * st + src_a];
+            nj_ = s.in[J * st + src_a];
+        }
         for (int it = 0; it < iters; it++) {
-            const int d = bs + it * G2P_THREADS + threadIdx.x;
-            const bool valid = d < be;
+            const int d = d0 + it * G2P_THREADS;
+            const bool valid = d < be && src_a >= 0;
+            const int src = src_a;
+            const float at[3] = {nx_, ny_, nz_};
+            const float m = nm_, jold = nj_;
+            if (src_b >= 0) {
+                nx_ = s.in[X * st + src_b];
+                ny_ = s.in[Y * st + src_b];
+                nz_ = s.in[Z * st + src_b];
+                nm_ = s.in[M * st + src_b];
+                nj_ = s.in[J * st + src_b];
+            }
+            src_a = src_b;
+            src_b = src_of(d + 2 * G2P_THREADS);
             float pos[3] = {0, 0, 0};
             if (valid) {
-                const int src = s.perm ? s.perm[d] : d;
-                const float m = (unsigned)src < (unsigned)s.np ? s.in[M * st + src] : 0.0f;
-                if ((unsigned)src >= (unsigned)s.np) {
-                    set_status(s.status, ST_OOB);
-                } else if (!(m > 0.0f)) {
+                if (!(m > 0.0f)) {
                     g2p_copy(s, d, src, pos);
                 } else {
-                    const float at[3] = {s.in[X * st + src], s.in[Y * st + src], s.in[Z * st + src]};
                     int cell[3];
                     float f[3];
                     stencil_axis(at[0], dm.nx, cell[0], f[0]);
@@ -480,7 +574,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
                             pos[q] = at[q] + p.dt * vel[q];
                             keep_inside(pos[q], vel[q], size[q]);
                         }
-                        float j = s.in[J * st + src] * (1.0f + p.dt * (c[0] + (c[4] + c[8])));
+                        float j = jold * (1.0f + p.dt * (c[0] + (c[4] + c[8])));
                         j = clampf(j, 1.0f / J_BOUND3, J_BOUND3);
                         g2p_store(s, d, pos, vel, c, m, j);
                     }

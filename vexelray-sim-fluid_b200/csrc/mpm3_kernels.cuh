@@ -7,7 +7,7 @@
 //              parity, so the last scatter stays readable while the next one accumulates)
 //   velocity   float4 per node {u, v, w, 0} (dense pipeline only; the tiled G2P computes the
 //              grid update into shared memory and never writes velocities to HBM)
-//   sort       key/rank/perm per particle; cell counts/starts over the brick-major keys; brick
+//   sort       key/perm per particle; cell counts/starts/cursors over the brick-major keys; brick
 //              counts/starts and the list of non-empty bricks
 #pragma once
 
@@ -106,7 +106,8 @@ struct Step3 {
     float* out;             // next particle set (== in when not sorting)
     int64_t stride;         // floats per field
     int np;
-    const int* perm;        // sorted slot -> source particle, or null (identity, in place)
+    int* perm;              // sorted slot -> source particle, or null (identity, in place); the tiled
+                            // scatter puts each cell's run in ascending order in place
     float4* grid;           // this step's grid {m, mu, mv, mw}
     float4* vel;            // dense pipeline's node velocities
     const Params3* params;
@@ -114,7 +115,6 @@ struct Step3 {
     uint32_t* status;
     // sort bookkeeping
     int* key;               // per particle (indexed by slot in `out`)
-    int* rank;
     int* cell_count;
     int* brick_count;
     const int* cell_start;
@@ -130,6 +130,7 @@ __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
 __global__ void k_p2g3_warp(Step3 s);
 __global__ void k_p2g3_tile(Step3 s);
+size_t p2g_tile_smem();
 __global__ void k_grid3_dense(Step3 s);
 __global__ void k_g2p3(Step3 s);
 __global__ void k_g2p3_tile(Step3 s);

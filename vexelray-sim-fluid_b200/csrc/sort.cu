@@ -24,27 +24,46 @@ __global__ void __launch_bounds__(1024) k_scan_single(int* __restrict__ counts, 
     if (threadIdx.x == 0) starts[n] = total;
 }
 
+// One block of 32 warps; warp w owns the contiguous segment [w*seg, (w+1)*seg) of the bricks and walks
+// it 32 bricks at a time, so every load and store of a warp is one coalesced 128-byte line. Pass 1 sums
+// each segment; a block scan gives each warp its offsets; pass 2 scans each 32-brick chunk with
+// shuffles, writes the starts, appends the non-empty bricks in order and zeroes the counts.
 __global__ void __launch_bounds__(1024) k_brick_scan(int* __restrict__ brick_count, int* __restrict__ brick_start,
                                                      int* __restrict__ active, int* __restrict__ n_active, int nb) {
     __shared__ int smem[33];
-    const int per = (nb + blockDim.x - 1) / blockDim.x;
-    const int lo = threadIdx.x * per;
-    const int hi = lo + per < nb ? lo + per : nb;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = (nb + 31) / 32;
+    const int lo = warp * seg, hi = min(lo + seg, nb);
     int sum = 0, live = 0;
-    for (int i = lo; i < hi; i++) {
-        int c = brick_count[i];
+    for (int base = lo; base < hi; base += 32) {
+        const int i = base + lane;
+        const int c = i < hi ? brick_count[i] : 0;
         sum += c;
         live += c > 0;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        live += __shfl_xor_sync(0xffffffffu, live, o);
+    }
+    // one value per warp into the block scan (lane 0 carries it, the rest add nothing)
     int total, total_live;
-    int run = block_exclusive(sum, smem, &total);
-    int slot = block_exclusive(live, smem, &total_live);
-    for (int i = lo; i < hi; i++) {
-        int c = brick_count[i];
-        brick_start[i] = run;
-        run += c;
-        if (c > 0) active[slot++] = i;
-        brick_count[i] = 0;
+    int run = block_exclusive(lane == 0 ? sum : 0, smem, &total);
+    int slot = block_exclusive(lane == 0 ? live : 0, smem, &total_live);
+    run = __shfl_sync(0xffffffffu, run, 0);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    for (int base = lo; base < hi; base += 32) {
+        const int i = base + lane;
+        const int c = i < hi ? brick_count[i] : 0;
+        const int inc = warp_inclusive(c);
+        const unsigned nz = __ballot_sync(0xffffffffu, c > 0);
+        if (i < hi) {
+            brick_start[i] = run + inc - c;
+            if (c > 0) active[slot + __popc(nz & ((1u << lane) - 1u))] = i;
+            brick_count[i] = 0;
+        }
+        run += __shfl_sync(0xffffffffu, inc, 31);
+        slot += __popc(nz);
     }
     if (threadIdx.x == 0) {
         brick_start[nb] = total;
@@ -53,7 +72,7 @@ __global__ void __launch_bounds__(1024) k_brick_scan(int* __restrict__ brick_cou
 }
 
 __global__ void __launch_bounds__(512) k_cell_scan(int* __restrict__ cell_count, int* __restrict__ cell_start,
-                                                   const int* __restrict__ brick_start,
+                                                   int* __restrict__ cursor, const int* __restrict__ brick_start,
                                                    const int* __restrict__ active,
                                                    const int* __restrict__ n_active) {
     __shared__ int smem[33];
@@ -65,6 +84,7 @@ __global__ void __launch_bounds__(512) k_cell_scan(int* __restrict__ cell_count,
         int total;
         int ex = block_exclusive(c, smem, &total);
         cell_start[key] = brick_start[b] + ex;
+        if (cursor) cursor[key] = brick_start[b] + ex;
         cell_count[key] = 0;
     }
 }
@@ -74,6 +94,20 @@ __global__ void k_permute(const int* __restrict__ key, const int* __restrict__ r
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int d = starts[key[i]] + rank[i];
+    if (d < 0 || d >= n) {
+        set_status(status, ST_RANK);
+        return;
+    }
+    perm[d] = i;
+}
+
+__global__ void __launch_bounds__(256) k_permute_cursor(const int* __restrict__ key, int* __restrict__ cursor,
+                                                       int* __restrict__ perm, int n, int64_t nkeys, uint32_t* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const int k = valid ? key[i] : 0;
+    const int d = warp_count(cursor, k, valid, nkeys, status);
+    if (!valid) return;
     if (d < 0 || d >= n) {
         set_status(status, ST_RANK);
         return;

@@ -92,10 +92,28 @@ __global__ void k_brick_scan(int* __restrict__ brick_count, int* __restrict__ br
                              int* __restrict__ active, int* __restrict__ n_active, int nb);
 
 // The 3D cell level, one block of 512 threads per non-empty brick: the brick's 512 cell counts
-// -> cell_start (offset by brick_start), counts zeroed.
-__global__ void k_cell_scan(int* __restrict__ cell_count, int* __restrict__ cell_start,
+// -> cell_start (offset by brick_start) and, if given, a copy in cursor; counts zeroed.
+__global__ void k_cell_scan(int* __restrict__ cell_count, int* __restrict__ cell_start, int* __restrict__ cursor,
                             const int* __restrict__ brick_start, const int* __restrict__ active,
                             const int* __restrict__ n_active);
+
+// perm[cursor[key[i]]++] = i, the cursor bumped once per distinct key in a warp: the permutation with
+// provisional (unstable) order within a cell, for counts that were tallied without ranks.
+__global__ void k_permute_cursor(const int* __restrict__ key, int* __restrict__ cursor, int* __restrict__ perm, int n,
+                                 int64_t nkeys, uint32_t* status);
+
+// Insertion sort of a short run, ascending (the stable order's fix-up of one cell).
+__device__ __forceinline__ void insertion_sort_run(int* a, int n) {
+    for (int i = 1; i < n; i++) {
+        int v = a[i];
+        int j = i - 1;
+        while (j >= 0 && a[j] > v) {
+            a[j + 1] = a[j];
+            j--;
+        }
+        a[j + 1] = v;
+    }
+}
 
 // perm[starts[key[i]] + rank[i]] = i.
 __global__ void k_permute(const int* __restrict__ key, const int* __restrict__ rank,
