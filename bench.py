@@ -99,6 +99,56 @@ def swe_bumps():
     return h.ravel()
 
 
+N_BATCH = 256
+SEED_BATCH = 3
+BATCH_GRIDS = (64, 128, 256, 512)
+BATCH_NP = (4096, 262144)
+K_TAIT = 50.0               # Tait k in m^2/s^2 (rho0 = 1); in node units k n^2
+WALL_BATCH = 3              # sticky wall thickness in nodes
+
+
+def dam2_scene(rng, n, count, ppc=4):
+    """One dam-break scene of the 2D config's physics on an n x n grid (dx = 1/n): `count` particles filling a
+    box at the lower-left corner, `ppc` per cell where the box fits (more where it cannot), its aspect
+    ratio drawn from rng; each cell's particles jittered (cell + U*0.999). Returns x, y, m, Flip.params values:
+    g = -9.8 n node/s^2, Tait k = 50 n^2, rho0 = 1, dt = 1e-4 capped at a Courant number of 0.4 of the Tait
+    sound speed sqrt(7k) (so the 512^2 scenes step 4.2e-5)."""
+    area = count / ppc
+    aspect = math.exp(rng.uniform(math.log(0.5), math.log(2.0)))
+    lo = WALL_BATCH + 1
+    span = n - 2 * lo
+    w = int(min(span, max(1, round(math.sqrt(area * aspect)))))
+    h = int(min(span, max(1, math.ceil(area / w))))
+    cells = w * h
+    k = np.arange(count)
+    cell = k % cells
+    cx = (lo + cell % w).astype(np.float32)
+    cy = (lo + cell // w).astype(np.float32)
+    j = rng.random((2, count), dtype=np.float32) * np.float32(0.999)
+    x = (cx + j[0]).astype(np.float32)
+    y = (cy + j[1]).astype(np.float32)
+    m = np.full(count, np.float32(cells / count), np.float32)
+    bulk = K_TAIT * n * n
+    dt = min(1e-4, 0.4 / (math.sqrt(7 * K_TAIT) * n))
+    return x, y, m, (dt, 0.0, -G_SI * n, bulk, 1.0)
+
+
+def batch_scenes(seed=SEED_BATCH, count=N_BATCH, np_range=BATCH_NP, grids=BATCH_GRIDS):
+    """The batched config: `count` dam-break scenes, grids uniform over `grids`, particle counts log-uniform in
+    np_range, box aspect from the seed. Returns (scenes as (n, particles, params)), x, y, m concatenated."""
+    rng = np.random.default_rng(seed)
+    scenes, xs, ys, ms = [], [], [], []
+    for _ in range(count):
+        n = int(rng.choice(grids))
+        npart = int(round(math.exp(rng.uniform(math.log(np_range[0]), math.log(np_range[1])))))
+        x, y, m, params = dam2_scene(rng, n, npart)
+        scenes.append((n, npart, params))
+        xs.append(x)
+        ys.append(y)
+        ms.append(m)
+    return scenes, np.concatenate(xs), np.concatenate(ys), np.concatenate(ms)
+
+
 # ---------------------------------------------------------------------------------------------- helpers
 
 class Clocks:
@@ -373,6 +423,8 @@ def run_ours(args, dist: Dist):
                             "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
                             "kernel": "k_swe_tile", "bytes_per_cell": 24}}
 
+    batch = None if args.no_batch else run_batch(args, vf, dist, peak)
+
     if dist.rank != 0:
         return
     cpu_rate, threads, cpu_steps, cpu_el = (None, 0, 0, 0.0)
@@ -396,9 +448,94 @@ def run_ours(args, dist: Dist):
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "swe": swe,
+        "batch": batch,
         "p2g_variants": variants,
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_batch_rate(scenes, x, y, m, budget_s=10.0):
+    """The oracle's 2D step, one scene after another on one host core, over the first scenes of the batch
+    until the budget is spent: particle-steps/s."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _oracle import Flip2State
+    done, spent, at, used = 0, 0.0, 0, 0
+    for n, count, params in scenes:
+        s = Flip2State(n, n, x[at:at + count], y[at:at + count], m[at:at + count])
+        pw = np.array(params, np.float32)
+        t0 = time.perf_counter()
+        s.step(pw, (1, WALL_BATCH))
+        s.step(pw, (1, WALL_BATCH))
+        spent += time.perf_counter() - t0
+        done += 2 * count
+        at += count
+        used += 1
+        if spent > budget_s:
+            break
+    return done / spent, used, spent
+
+
+def run_batch(args, vf, dist: Dist, peak):
+    """The batched 2D config: 256 dam-break scenes in one cooperative launch per step, replayed from CUDA graphs,
+    tiles and block size from the autotuner (its JSON cache). Scenes are dealt round-robin to the ranks."""
+    scenes, x, y, m = batch_scenes()
+    first = np.concatenate([[0], np.cumsum([c for _, c, _ in scenes])])
+    mine = list(range(dist.rank, len(scenes), dist.world))
+    table = [vf.Scene(n, n, c, vf.flip_params(*p)) for n, c, p in (scenes[k] for k in mine)]
+    pick = lambda a: [a[first[k]:first[k + 1]] for k in mine]
+    xs, ys, ms = pick(x), pick(y), pick(m)
+    zs = [np.zeros_like(a) for a in xs]
+    nparts = sum(len(a) for a in xs)
+    t0 = time.perf_counter()
+    table, block, trials = vf.autotune(table, xs, ys, zs, zs, ms, tait=True, sticky=WALL_BATCH,
+                                       cache=args.tune_cache)
+    tune_s = time.perf_counter() - t0
+    b = vf.BatchSimulation(table, tait=True, sticky=WALL_BATCH, block=block)
+    b.load(xs, ys, zs, zs, ms)
+    b.advance(max(3, args.warmup))
+    b.finish()
+    k = max(32, args.steps)
+    ev0, ev1 = vf.Event(), vf.Event()
+    stream = b.stream()
+    dist.barrier()
+    launches0 = b.launches()
+    ev0.record(stream)
+    b.advance(k)
+    ev1.record(stream)
+    ms = ev0.elapsed_ms(ev1)
+    b.finish()
+    launches = b.launches() - launches0
+    ms_max = dist.max(ms)
+    total = dist.sum(float(nparts))
+    touched = 0
+    for s in range(len(table)):
+        touched += int(np.count_nonzero(b.read(s, "gm")))
+    touched = dist.sum(float(touched))
+    cfg = b.config(0)
+    tiles = {}
+    for s in table:
+        tiles[f"{s.tile[0]}x{s.tile[1]}"] = tiles.get(f"{s.tile[0]}x{s.tile[1]}", 0) + 1
+    b.close()
+    # P2G reads 10 f32 per particle and writes m, mu, mv per touched node; G2P reads x, y, m, j and writes 10
+    # f32 per particle and reads m, mu, mv per touched node: 96 Np + 24 N_t, over the whole step's time
+    alg = 96.0 * total + 24.0 * touched
+    achieved = alg / (ms_max / k / 1e3) / 1e9
+    out = {"workload": (f"{N_BATCH} 2D dam-break scenes (seed {SEED_BATCH}), grids uniform over {BATCH_GRIDS}^2, "
+                        f"particles log-uniform in [{BATCH_NP[0]}, {BATCH_NP[1]}], 4 per cell where the box fits, "
+                        f"Tait k=50 m^2/s^2, rho0=1, sticky walls {WALL_BATCH}, dt 1e-4 (Courant-capped on 512^2)"),
+           "scenes": len(scenes), "particles": int(total), "steps": k, "ms_per_step": ms_max / k,
+           "particle_steps_per_s": total * k / (ms_max / 1e3), "launches_per_step": launches / k,
+           "block": cfg["block"], "ctas": cfg["ctas"], "tiles": tiles, "tuner_trials": trials,
+           "tuner_s": tune_s,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": None, "kernel": "k_batch2_step (whole step)",
+                        "algorithmic_bytes_per_step": alg, "touched_nodes": touched}}
+    if dist.rank == 0 and not args.no_cpu:
+        rate, used, spent = cpu_batch_rate(scenes, x, y, m)
+        out["cpu_baseline"] = {"value": rate, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+                               "sample": f"2 steps of each of the first {used} scenes, one after another, "
+                                         f"oracle C port of FlipStep.step, 1 thread, {spent:.1f} s"}
+    return out
 
 
 def main():
@@ -411,6 +548,9 @@ def main():
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water sub-measurement")
     ap.add_argument("--no-variants", action="store_true", help="skip the comparison of the three P2G schedules")
     ap.add_argument("--variant-steps", type=int, default=20)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes sub-measurement")
+    ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
+                    help="the batched step's autotune cache (JSON)")
     args = ap.parse_args()
     dist = Dist()
     try:

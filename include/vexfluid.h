@@ -145,6 +145,58 @@ int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t
 int32_t vf_sort2_noalloc(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm,
                          int32_t* starts);
 
+/* ------------------------------------------------------------------ batched 2D scenes */
+/* Many independent 2D scenes (each a ParticleSimulation's FlipStep: sort by cell, scatter, grid, advect)
+ * stepped together: one cooperative persistent kernel launch per step over every scene, with CUDA graphs
+ * replaying the launches. No counterpart in the reference. Scenes of one batch share the physics flags
+ * (VF_EOS_TAIT, VF_WALL_STICKY(t)); each has its own grid, particle count and Flip.params words. */
+typedef struct vf_mpm2_batch vf_mpm2_batch;
+
+typedef struct {
+    int32_t nx, ny;          /* grid nodes, >= 3 each */
+    int32_t particles;       /* >= 1 */
+    int32_t tile_x, tile_y;  /* P2G/G2P tile in stencil cells: one of the VF_BATCH_TILES shapes (0, 0 = 16 x 16) */
+    int32_t params[5];       /* Flip.params words [dt, gx, gy, bulk, rho0] (Flip.java:145-211) */
+} vf_scene2;
+
+/* The tile shapes a scene may use (x, y pairs), and the block sizes a batch may launch with. */
+#define VF_BATCH_TILES {{8, 8}, {16, 8}, {16, 16}, {32, 8}, {32, 16}}
+#define VF_BATCH_BLOCKS {128, 256, 512}
+
+/* Builds a batch: scenes are copied; block is the CTA size (one of VF_BATCH_BLOCKS, 0 = 256). */
+int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t flags, int32_t block,
+                             vf_mpm2_batch** out);
+/* Loads every scene's particles: each array holds the scenes' particles one scene after another (sum of
+ * particles floats). J = 1, C = 0; the step count restarts at zero. */
+int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, const float* u, const float* v,
+                           const float* m);
+/* count steps of every scene (FlipStep.step with a sort every step), submitted as CUDA graph replays.
+ * Returns when submitted; vf_mpm2_batch_finish waits and reports device errors. */
+int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count);
+int32_t vf_mpm2_batch_finish(vf_mpm2_batch* h);
+/* One scene's particle field (VF2_X..VF2_C11, in the batch's sorted order) or the last step's grid
+ * (VF2_GM, VF2_GMU, VF2_GMV; nx*ny floats). Blocking. */
+int32_t vf_mpm2_batch_read(vf_mpm2_batch* h, int32_t scene, int32_t field, float* out, int64_t n);
+/* The tile shape a scene runs with, and the batch's block size and persistent grid size (CTAs). */
+int32_t vf_mpm2_batch_config(const vf_mpm2_batch* h, int32_t scene, int32_t* tile_x, int32_t* tile_y,
+                             int32_t* block, int32_t* ctas);
+int64_t vf_mpm2_batch_particles(const vf_mpm2_batch* h);
+int64_t vf_mpm2_batch_steps(const vf_mpm2_batch* h);
+int64_t vf_mpm2_batch_launches(const vf_mpm2_batch* h);
+void* vf_mpm2_batch_stream(vf_mpm2_batch* h);
+void vf_mpm2_batch_destroy(vf_mpm2_batch* h);
+
+/* The tile-shape and block-size autotuner. Each scene is keyed by (particles per occupied cell rounded to a
+ * power of two, max(nx, ny) rounded up to a power of two). For every key not found in the JSON cache at
+ * cache_path, it times a batch of up to 8 of that key's scenes with each VF_BATCH_TILES shape. It then times
+ * the scenes with each VF_BATCH_BLOCKS size, unless the cache holds a block size for this batch's key set.
+ * The winners are written to the cache (created if absent; cache_path NULL = no cache). On return, scenes[i]'s
+ * tile_x/tile_y and *block hold the choices. Particles are given as for vf_mpm2_batch_load. trials counts the
+ * timed configurations (0 when everything came from the cache). */
+int32_t vf_mpm2_autotune(vf_scene2* scenes, int32_t nscenes, uint32_t flags, const float* x, const float* y,
+                         const float* u, const float* v, const float* m, const char* cache_path, int32_t* block,
+                         int32_t* trials);
+
 /* ------------------------------------------------------------------ 3D particles (ParticleSimulation3) */
 typedef struct vf_mpm3 vf_mpm3;
 typedef struct vf_mpm3_prepared vf_mpm3_prepared;

@@ -73,6 +73,16 @@ def build(quiet: bool = True) -> pathlib.Path:
     return LIBRARY
 
 
+class Scene2(ctypes.Structure):
+    """vf_scene2: one scene of a batch (grid, particle count, tile shape, Flip.params' first five words)."""
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("particles", ctypes.c_int32),
+                ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("params", ctypes.c_int32 * 5)]
+
+
+BATCH_TILES = ((8, 8), (16, 8), (16, 16), (32, 8), (32, 16))   # VF_BATCH_TILES
+BATCH_BLOCKS = (128, 256, 512)                                 # VF_BATCH_BLOCKS
+
+
 def lib() -> ctypes.CDLL:
     """The loaded library. Raises if it has not been built: there is no fallback."""
     global _LIB
@@ -137,6 +147,20 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_destroy": ([_vp], None),
         "vf_mpm3_particle_diagnostics": ([_vp] + [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)],
                                          ctypes.c_int32),
+        "vf_mpm2_batch_create": ([ctypes.POINTER(Scene2), ctypes.c_int32, ctypes.c_uint32, ctypes.c_int32,
+                                  ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_mpm2_batch_load": ([_vp] + [_f32p] * 5, ctypes.c_int32),
+        "vf_mpm2_batch_advance": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm2_batch_finish": ([_vp], ctypes.c_int32),
+        "vf_mpm2_batch_read": ([_vp, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm2_batch_config": ([_vp, ctypes.c_int32] + [_i32p] * 4, ctypes.c_int32),
+        "vf_mpm2_batch_particles": ([_vp], ctypes.c_int64),
+        "vf_mpm2_batch_steps": ([_vp], ctypes.c_int64),
+        "vf_mpm2_batch_launches": ([_vp], ctypes.c_int64),
+        "vf_mpm2_batch_stream": ([_vp], _vp),
+        "vf_mpm2_batch_destroy": ([_vp], None),
+        "vf_mpm2_autotune": ([ctypes.POINTER(Scene2), ctypes.c_int32, ctypes.c_uint32] + [_f32p] * 5 +
+                             [ctypes.c_char_p, _i32p, _i32p], ctypes.c_int32),
         "vf_swe_create": ([ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_swe_load": ([_vp] + [_f32p] * 3 + [_i32p, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
@@ -410,6 +434,119 @@ class ParticleSimulation:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class Scene:
+    """One scene of a batch: an nx x ny grid, its particles' count, the Flip.params words it steps with
+    (the first five are used) and its tile shape (None: the default, or the tuner's choice)."""
+    nx: int
+    ny: int
+    particles: int
+    params: Sequence[int]
+    tile: tuple | None = None
+
+    def _c(self) -> Scene2:
+        w = _words(self.params)
+        if len(w) < 5:
+            raise IllegalArgumentException(VF_EINVAL, f"Flip.params has at least 5 words, got {len(w)}")
+        tx, ty = self.tile or (0, 0)
+        return Scene2(self.nx, self.ny, self.particles, tx, ty, (ctypes.c_int32 * 5)(*[int(v) for v in w[:5]]))
+
+
+def _scene_table(scenes: Sequence[Scene]):
+    return (Scene2 * len(scenes))(*[s._c() for s in scenes])
+
+
+def _concat(scenes, arrays, name):
+    total = sum(s.particles for s in scenes)
+    a = np.ascontiguousarray(np.concatenate([np.asarray(q, np.float32).ravel() for q in arrays])
+                             if isinstance(arrays, (list, tuple)) else np.asarray(arrays, np.float32).ravel())
+    if a.size != total:
+        raise IllegalArgumentException(VF_EINVAL, f"{name} holds {a.size} floats for {total} particles")
+    return a
+
+
+class BatchSimulation:
+    """Many independent 2D scenes stepped together: one cooperative persistent kernel launch per step over
+    every scene, replayed from CUDA graphs (vf_mpm2_batch_*). Particle arrays are the scenes' particles one
+    scene after another (or a list of per-scene arrays)."""
+
+    def __init__(self, scenes: Sequence[Scene], *, tait: bool = False, sticky: int = 0, block: int = 0):
+        self._scenes = list(scenes)
+        self._flags = (VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT)
+        h = _vp()
+        check(lib().vf_mpm2_batch_create(_scene_table(self._scenes), len(self._scenes), self._flags, block,
+                                         ctypes.byref(h)))
+        self._h = h
+
+    def load(self, x, y, u, v, m) -> None:
+        a = [_concat(self._scenes, q, n) for q, n in ((x, "x"), (y, "y"), (u, "u"), (v, "v"), (m, "m"))]
+        check(lib().vf_mpm2_batch_load(self._h, *[_fp(q) for q in a]))
+
+    def advance(self, count: int) -> None:
+        check(lib().vf_mpm2_batch_advance(self._h, count))
+
+    def finish(self) -> None:
+        check(lib().vf_mpm2_batch_finish(self._h))
+
+    def read(self, scene: int, name: str) -> np.ndarray:
+        f = FIELDS2[name]
+        sc = self._scenes[scene]
+        n = sc.nx * sc.ny if f >= 16 else sc.particles
+        out = np.empty(n, np.float32)
+        check(lib().vf_mpm2_batch_read(self._h, scene, f, _fp(out), n))
+        return out
+
+    def config(self, scene: int = 0) -> dict:
+        v = [np.zeros(1, np.int32) for _ in range(4)]
+        check(lib().vf_mpm2_batch_config(self._h, scene, *[_ip(q) for q in v]))
+        return {"tile": (int(v[0][0]), int(v[1][0])), "block": int(v[2][0]), "ctas": int(v[3][0])}
+
+    def particles(self) -> int:
+        return int(lib().vf_mpm2_batch_particles(self._h))
+
+    def steps(self) -> int:
+        return int(lib().vf_mpm2_batch_steps(self._h))
+
+    def launches(self) -> int:
+        return int(lib().vf_mpm2_batch_launches(self._h))
+
+    def stream(self):
+        return lib().vf_mpm2_batch_stream(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_mpm2_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(scenes: Sequence[Scene], x, y, u, v, m, *, tait: bool = False, sticky: int = 0,
+             cache: str | os.PathLike | None = None):
+    """vf_mpm2_autotune: picks each scene's tile shape and the batch's block size, timing what the JSON cache
+    does not hold. Returns (scenes with their tiles set, block, trials timed)."""
+    table = _scene_table(scenes)
+    a = [_concat(scenes, q, n) for q, n in ((x, "x"), (y, "y"), (u, "u"), (v, "v"), (m, "m"))]
+    block = np.zeros(1, np.int32)
+    trials = np.zeros(1, np.int32)
+    flags = (VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT)
+    path = None if cache is None else os.fsencode(os.fspath(cache))
+    check(lib().vf_mpm2_autotune(table, len(scenes), flags, *[_fp(q) for q in a], path, _ip(block), _ip(trials)))
+    tuned = [Scene(s.nx, s.ny, s.particles, s.params, (int(table[k].tile_x), int(table[k].tile_y)))
+             for k, s in enumerate(scenes)]
+    return tuned, int(block[0]), int(trials[0])
 
 
 def scatter2(mode: int, nx: int, ny: int, x, y, u, v, m):

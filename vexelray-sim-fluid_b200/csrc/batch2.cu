@@ -1,0 +1,775 @@
+// batch2.cu -- many independent 2D scenes (each a FlipStep: sort by cell, scatter, grid, advect;
+// FlipStep.java:81-193, Flip.java) stepped by ONE cooperative persistent kernel launch per step,
+// the launches replayed from a CUDA graph. No counterpart in the reference, which steps one scene
+// per ParticleSimulation; the per-particle and per-node arithmetic is the single-scene step's
+// (mpm2_device.cuh), so each scene computes what vf_mpm2 computes for it.
+//
+// Layout in HBM (scenes side by side, no per-scene allocation):
+//   particles   two sets (ping-pong by step parity) of 10 SoA f32 fields x y u v m j c00 c01 c10 c11;
+//               scene s owns slots [p0, p0 + np) of every field, and keeps them: the sort is by
+//               (scene, tile, cell), so a scene's particles never leave its range
+//   grid        two buffers (by step parity) of float4 {m, mu, mv, 0} per node; scene s's nodes at
+//               g0 + j*nx + i
+//   tiles       a scene's (nx-2) x (ny-2) stencil cells are cut into tiles of tx x ty cells, ntx x nty
+//               of them; the tile entries of all scenes, each scene's followed by a sentinel, hold the
+//               per-step counts and the run starts (by parity)
+//   cells       cell keys tile-major: key = c0 + tile * tx*ty + (ly * tx + lx), one count and one cursor
+//               per key
+//
+// One step = five phases separated by a grid-wide barrier (the launch is cooperative, so every CTA is
+// resident; the barrier's wait is bounded and sets a status bit rather than hang):
+//   1  tile scan     per scene: tile counts -> run starts (parity buffer), counts zeroed
+//   2  cell scan     per non-empty tile: cell counts -> cursors (cell starts), counts zeroed
+//   3  permute       per slot: perm[cursor[key]++] = slot, one cursor bump per distinct key of a warp
+//   4  scatter       per tile, work-stealing: the tile's cell runs put in ascending order (the stable
+//                    sort's fix-up), then warps over contiguous chunks of the tile's run: Flip.scatter's
+//                    27 amounts per particle, summed over each cell's run across the warp
+//                    (Scatter.segmentedDeposit), the run tails adding into a warp-private node window
+//                    (distinct cells, so distinct nodes at each stencil offset: plain read-modify-write);
+//                    the warps' windows summed per node and reduced into the grid with one 16-byte
+//                    red.global.add.v4.f32 per touched node. The other parity's grid is cleared here,
+//                    over the windows of the tiles the previous step scattered into.
+//   5  gather        per tile, work-stealing: the window's node velocities (Flip.grid, fused) into shared
+//                    memory, then per particle Flip.advectBody; the particle is written to its sorted
+//                    slot of the other set, and its next cell key tallied for the next step's sort.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "mpm2_device.cuh"
+#include "sort.cuh"
+
+using namespace vf;
+
+namespace {
+
+struct Scene2 {
+    int nx, ny, np;
+    int tx, ty, ntx, nty, tc;   // tile shape in cells, tiles per axis, cells per tile
+    int p0;                     // first particle slot
+    int t0;                     // first tile entry: ntx*nty tiles, then a sentinel
+    int c0;                     // first cell key
+    int64_t g0;                 // first grid node
+    Params2 prm;
+};
+
+struct GridBarrier {
+    unsigned count, gen;
+};
+
+// The batch's device state, passed by value to the step kernel.
+struct Batch2 {
+    const Scene2* scene;
+    int nscenes;
+    const int* tile_scene;     // tile entry -> scene, -1 for a sentinel
+    int nentries;              // tile entries (every scene's tiles and its sentinel)
+    float* part[2];
+    int64_t stride;            // floats per field
+    int np;                    // all scenes' particles
+    int ncells;                // all scenes' cell keys
+    int* key;                  // per slot of the current set: the cell key for this step's sort
+    int* perm;                 // sorted slot -> slot of the current set
+    int* cell_count;
+    int* cursor;               // per cell: its run's start after the cell scan, its end after the permute
+    int* tile_count;
+    int* tile_start[2];        // per tile entry, by step parity: run start; the sentinel holds the scene's end
+    float4* grid[2];
+    unsigned* step;            // device step counter (its parity picks the buffers)
+    unsigned* work;            // work-stealing counters: [0] scatter, [1] gather
+    GridBarrier* bar;
+    uint32_t* status;
+};
+
+constexpr int BATCH_MAX_THREADS = 512;
+constexpr int BAR_SPINS = 1 << 24;   // x ~64 ns of __nanosleep: about a second
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs co-resident). The last CTA to arrive resets the
+// count and advances the generation; the others wait for the generation to change, at most BAR_SPINS
+// polls, after which they set ST_TIMEOUT and go on (the host reports the status; the kernel ends).
+__device__ void grid_barrier(GridBarrier* b, uint32_t* status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&b->gen);
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            int spins = 0;
+            while (ld_acquire(&b->gen) == gen) {
+                if (++spins > BAR_SPINS) {
+                    set_status(status, ST_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// The next-step cell key and tile entry of a particle at (x, y) in scene sc.
+__device__ __forceinline__ void batch_key(const Scene2& sc, float x, float y, int& key, int& tile) {
+    int col, row;
+    stencil_cell2(x, y, sc.nx, sc.ny, col, row);
+    const int tix = col / sc.tx, tiy = row / sc.ty;
+    const int local = tiy * sc.ntx + tix;
+    tile = sc.t0 + local;
+    key = sc.c0 + local * sc.tc + (row - tiy * sc.ty) * sc.tx + (col - tix * sc.tx);
+}
+
+// Takes the next work item for the CTA from a work-stealing counter.
+__device__ __forceinline__ int next_item(unsigned* counter, int* slot) {
+    __syncthreads();   // every thread has read the previous item
+    if (threadIdx.x == 0) *slot = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    return *slot;
+}
+
+__global__ void __launch_bounds__(BATCH_MAX_THREADS) k_batch2_step(Batch2 B) {
+    extern __shared__ __align__(16) float dyn[];
+    __shared__ int scan_smem[33];
+    __shared__ int item;
+    const unsigned par = *B.step & 1u;   // read before the first barrier; CTA 0 advances it after
+    const float* __restrict__ in = B.part[par];
+    float* __restrict__ out = B.part[par ^ 1u];
+    int* ts_cur = B.tile_start[par];
+    const int* ts_prev = B.tile_start[par ^ 1u];
+    float4* g_cur = B.grid[par];
+    float4* g_next = B.grid[par ^ 1u];
+    const int64_t st = B.stride;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+    // ---- 1. tile scan, per scene
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.work[1] = 0;   // the previous launch's gather counter
+    for (int s = blockIdx.x; s < B.nscenes; s += gridDim.x) {
+        const Scene2 sc = B.scene[s];
+        const int nt = sc.ntx * sc.nty;
+        int carry = 0;
+        for (int base = 0; base < nt; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const int c = i < nt ? B.tile_count[sc.t0 + i] : 0;
+            int total;
+            const int ex = block_exclusive(c, scan_smem, &total);
+            if (i < nt) {
+                ts_cur[sc.t0 + i] = sc.p0 + carry + ex;
+                B.tile_count[sc.t0 + i] = 0;
+            }
+            carry += total;
+        }
+        if (threadIdx.x == 0) {
+            ts_cur[sc.t0 + nt] = sc.p0 + carry;
+            if (carry != sc.np) set_status(B.status, ST_RANK);
+        }
+    }
+    grid_barrier(B.bar, B.status);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(B.step, 1u);
+
+    // ---- 2. cell scan, per non-empty tile
+    for (int t = blockIdx.x; t < B.nentries; t += gridDim.x) {
+        const int s = B.tile_scene[t];
+        if (s < 0) continue;
+        const int ts = ts_cur[t], te = ts_cur[t + 1];
+        if (te <= ts) continue;
+        if (ts < B.scene[s].p0 || te > B.scene[s].p0 + B.scene[s].np) {   // counts that do not add up
+            if (threadIdx.x == 0) set_status(B.status, ST_RANK);
+            continue;
+        }
+        const int tc = B.scene[s].tc;
+        const int cb = B.scene[s].c0 + (t - B.scene[s].t0) * tc;
+        int carry = 0;
+        for (int base = 0; base < tc; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const int c = i < tc ? B.cell_count[cb + i] : 0;
+            int total;
+            const int ex = block_exclusive(c, scan_smem, &total);
+            if (i < tc) {
+                B.cursor[cb + i] = ts + carry + ex;
+                B.cell_count[cb + i] = 0;
+            }
+            carry += total;
+        }
+        if (threadIdx.x == 0 && ts + carry != te) set_status(B.status, ST_RANK);
+    }
+    grid_barrier(B.bar, B.status);
+
+    // ---- 3. permute: perm[cursor[key]++] = slot (provisional order within a cell)
+    {
+        const int n32 = (B.np + 31) & ~31;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n32; i += gridDim.x * blockDim.x) {
+            const bool valid = i < B.np;
+            const int k = valid ? B.key[i] : -1;
+            const bool ok = valid && k >= 0 && k < B.ncells;
+            if (valid && !ok) set_status(B.status, ST_OOB);
+            const unsigned peers = __match_any_sync(0xffffffffu, ok ? k : -1);
+            const int leader = __ffs(peers) - 1;
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            int base = 0;
+            if (lane == leader && ok) base = atomicAdd(&B.cursor[k], __popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (ok) {
+                const int d = base + rank;
+                if (d >= 0 && d < B.np) B.perm[d] = i;
+                else set_status(B.status, ST_RANK);
+            }
+        }
+    }
+    grid_barrier(B.bar, B.status);
+
+    // ---- 4. scatter, per tile
+    for (;;) {
+        const int t = next_item(&B.work[0], &item);
+        if (t >= B.nentries) break;
+        const int s = B.tile_scene[t];
+        if (s < 0) continue;
+        const Scene2 sc = B.scene[s];
+        const int lt = t - sc.t0;
+        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;   // the tile's first cell = first node
+        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
+        // the other parity's grid: clear this tile's window if the previous step scattered into it
+        if (ts_prev[t + 1] > ts_prev[t]) {
+            for (int j = threadIdx.x; j < wn; j += blockDim.x) {
+                const int gi = x0 + j % wx, gj = y0 + j / wx;
+                if (gi < sc.nx && gj < sc.ny) g_next[sc.g0 + (int64_t)gj * sc.nx + gi] = make_float4(0, 0, 0, 0);
+            }
+        }
+        const int ts = ts_cur[t], te = ts_cur[t + 1];
+        if (te <= ts || ts < sc.p0 || te > sc.p0 + sc.np) continue;   // empty, or flagged in the cell scan
+        const int cb = sc.c0 + lt * sc.tc;
+        // the stable order: each cell's run of perm ascending
+        for (int c = threadIdx.x; c < sc.tc; c += blockDim.x) {
+            const int cs = c == 0 ? ts : B.cursor[cb + c - 1];
+            const int ce = B.cursor[cb + c];
+            if (cs < ts || ce > te || ce < cs) set_status(B.status, ST_RANK);
+            else if (ce - cs > 1) insertion_sort_run(B.perm + cs, ce - cs);
+        }
+        for (int j = threadIdx.x; j < nwarps * 3 * wn; j += blockDim.x) dyn[j] = 0.0f;
+        __syncthreads();
+        float* ww = dyn + warp * 3 * wn;   // this warp's window: m, mu, mv arrays of wn nodes
+        const int chunk = ((te - ts + nwarps - 1) / nwarps + 31) & ~31;
+        const int w0 = ts + warp * chunk, w1 = min(te, w0 + chunk);
+        for (int b = w0; b < w1; b += 32) {
+            const int slot = b + lane;
+            float amt[27];
+#pragma unroll
+            for (int k = 0; k < 27; k++) amt[k] = 0.0f;
+            int key = -1;
+            if (slot < w1) {
+                const int src = B.perm[slot];
+                if (src < sc.p0 || src >= sc.p0 + sc.np) {
+                    set_status(B.status, ST_OOB);
+                } else {
+                    const float px = in[PX * st + src], py = in[PY * st + src];
+                    const float m = in[PM * st + src], u = in[PU * st + src], v = in[PV * st + src];
+                    const float pj = in[PJ * st + src];
+                    const float c00 = in[PC00 * st + src], c01 = in[PC01 * st + src];
+                    const float c10 = in[PC10 * st + src], c11 = in[PC11 * st + src];
+                    const Stencil2 sn = stencil2(px, py, sc.nx, sc.ny);
+                    const int lx = sn.col - x0, ly = sn.row - y0;
+                    if (lx >= 0 && lx < sc.tx && ly >= 0 && ly < sc.ty) {
+                        const float sp = impulse_factor(sc.prm.dt, m, sc.prm.rho0, sc.prm.bulk, pj, sc.prm.tait);
+                        scatter_amounts2(sn, m, u, v, c00, c01, c10, c11, sp, amt);
+                        key = ly * wx + lx;   // the window index of the stencil's lower-left node
+                    } else {
+                        set_status(B.status, ST_OOB);
+                    }
+                }
+            }
+            const bool tail = segmented_sum<27>(amt, key) && key >= 0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                if (tail) {
+                    const int wi = key + (k / 3) * wx + k % 3;
+                    ww[wi] += amt[3 * k];
+                    ww[wn + wi] += amt[3 * k + 1];
+                    ww[2 * wn + wi] += amt[3 * k + 2];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < wn; j += blockDim.x) {
+            float a = 0.0f, bu = 0.0f, bv = 0.0f;
+            for (int w = 0; w < nwarps; w++) {
+                const float* o = dyn + w * 3 * wn;
+                a += o[j];
+                bu += o[wn + j];
+                bv += o[2 * wn + j];
+            }
+            if (a == 0.0f && bu == 0.0f && bv == 0.0f) continue;
+            const int gi = x0 + j % wx, gj = y0 + j / wx;
+            if (gi >= sc.nx || gj >= sc.ny) {
+                set_status(B.status, ST_OOB);
+                continue;
+            }
+            red_add_v4(&g_cur[sc.g0 + (int64_t)gj * sc.nx + gi], a, bu, bv, 0.0f);
+        }
+    }
+    grid_barrier(B.bar, B.status);
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.work[0] = 0;
+
+    // ---- 5. gather, per tile: grid update into shared memory, then advect
+    float2* vw = reinterpret_cast<float2*>(dyn);
+    for (;;) {
+        const int t = next_item(&B.work[1], &item);
+        if (t >= B.nentries) break;
+        const int s = B.tile_scene[t];
+        if (s < 0) continue;
+        const Scene2 sc = B.scene[s];
+        const int ts = ts_cur[t], te = ts_cur[t + 1];
+        if (te <= ts || ts < sc.p0 || te > sc.p0 + sc.np) continue;
+        const int lt = t - sc.t0;
+        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;
+        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
+        for (int j = threadIdx.x; j < wn; j += blockDim.x) {
+            const int gi = x0 + j % wx, gj = y0 + j / wx;
+            float2 v = make_float2(0.0f, 0.0f);
+            if (gi < sc.nx && gj < sc.ny) {
+                const float4 g = g_cur[sc.g0 + (int64_t)gj * sc.nx + gi];
+                v = grid_velocity2(g.x, g.y, g.z, gi, gj, sc.nx, sc.ny, sc.prm);
+            }
+            vw[j] = v;
+        }
+        __syncthreads();
+        for (int b = ts; b < te; b += blockDim.x) {
+            const int slot = b + threadIdx.x;
+            int nkey = -1, ntile = -1;
+            if (slot < te) {
+                int src = B.perm[slot];
+                if (src < sc.p0 || src >= sc.p0 + sc.np) {
+                    set_status(B.status, ST_OOB);
+                    src = slot;
+                }
+                const float px = in[PX * st + src], py = in[PY * st + src];
+                const float pj = in[PJ * st + src], pm = in[PM * st + src];
+                const Stencil2 sn = stencil2(px, py, sc.nx, sc.ny);
+                const int lx = sn.col - x0, ly = sn.row - y0;
+                Advected2 a;
+                if (lx >= 0 && lx < sc.tx && ly >= 0 && ly < sc.ty) {
+                    const int wb = ly * wx + lx;
+                    a = advect2(sn, px, py, pj, sc.nx, sc.ny, sc.prm,
+                                [&](int k) { return vw[wb + (k / 3) * wx + k % 3]; });
+                } else {
+                    set_status(B.status, ST_OOB);
+                    a = Advected2{px, py, in[PU * st + src], in[PV * st + src], in[PC00 * st + src],
+                                  in[PC01 * st + src], in[PC10 * st + src], in[PC11 * st + src], pj};
+                }
+                out[PX * st + slot] = a.x;
+                out[PY * st + slot] = a.y;
+                out[PU * st + slot] = a.u;
+                out[PV * st + slot] = a.w;
+                out[PM * st + slot] = pm;
+                out[PJ * st + slot] = a.j;
+                out[PC00 * st + slot] = a.c00;
+                out[PC01 * st + slot] = a.c01;
+                out[PC10 * st + slot] = a.c10;
+                out[PC11 * st + slot] = a.c11;
+                batch_key(sc, a.x, a.y, nkey, ntile);
+                B.key[slot] = nkey;
+            }
+            warp_tally(B.cell_count, nkey, nkey >= 0, B.ncells, B.status);
+            warp_tally(B.tile_count, ntile, ntile >= 0, B.nentries, B.status);
+        }
+    }
+}
+
+// After a load: every particle's first cell key, tallied (the step's first phase expects the counts).
+__global__ void __launch_bounds__(256) k_batch2_tally(Batch2 B) {
+    const int n32 = (B.np + 31) & ~31;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n32; i += gridDim.x * blockDim.x) {
+        int key = -1, tile = -1;
+        if (i < B.np) {
+            int lo = 0, hi = B.nscenes - 1;   // the scene owning slot i: the last with p0 <= i
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (B.scene[mid].p0 <= i) lo = mid;
+                else hi = mid - 1;
+            }
+            const Scene2 sc = B.scene[lo];
+            batch_key(sc, B.part[0][PX * B.stride + i], B.part[0][PY * B.stride + i], key, tile);
+            B.key[i] = key;
+        }
+        warp_tally(B.cell_count, key, key >= 0, B.ncells, B.status);
+        warp_tally(B.tile_count, tile, tile >= 0, B.nentries, B.status);
+    }
+}
+
+// Grid readback: one float of every node of one scene.
+__global__ void k_batch2_unpack(const float4* grid, float* out, int64_t nodes, int comp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const float4 g = grid[i];
+    out[i] = comp == 0 ? g.x : comp == 1 ? g.y : g.z;
+}
+
+const int TILES[][2] = VF_BATCH_TILES;
+const int BLOCKS[] = VF_BATCH_BLOCKS;
+constexpr int GRAPH_STEPS = 16;   // launches per graph replay
+
+bool tile_ok(int tx, int ty) {
+    for (auto& t : TILES)
+        if (t[0] == tx && t[1] == ty) return true;
+    return false;
+}
+
+bool block_ok(int b) {
+    for (int x : BLOCKS)
+        if (x == b) return true;
+    return false;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the handle
+
+struct vf_mpm2_batch {
+    std::vector<Scene2> scenes;
+    uint32_t flags = 0;
+    int block = 256, ctas = 0;
+    size_t smem = 0;
+    int64_t np = 0, stride = 0;
+    int ncells = 0, nentries = 0;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer scene_d, tile_scene, part[2], key, perm, cell_count, cursor, tile_count, tile_start[2], grid[2];
+    DeviceBuffer ctl;      // step counter, two work counters, the barrier
+    DeviceBuffer status;
+    int64_t nodes = 0;
+    int64_t steps = 0, launches = 0;
+    bool loaded = false;
+    cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+Batch2 view(vf_mpm2_batch* h) {
+    Batch2 b;
+    b.scene = h->scene_d.as<Scene2>();
+    b.nscenes = (int)h->scenes.size();
+    b.tile_scene = h->tile_scene.as<int>();
+    b.nentries = h->nentries;
+    b.part[0] = h->part[0].as<float>();
+    b.part[1] = h->part[1].as<float>();
+    b.stride = h->stride;
+    b.np = (int)h->np;
+    b.ncells = h->ncells;
+    b.key = h->key.as<int>();
+    b.perm = h->perm.as<int>();
+    b.cell_count = h->cell_count.as<int>();
+    b.cursor = h->cursor.as<int>();
+    b.tile_count = h->tile_count.as<int>();
+    b.tile_start[0] = h->tile_start[0].as<int>();
+    b.tile_start[1] = h->tile_start[1].as<int>();
+    b.grid[0] = h->grid[0].as<float4>();
+    b.grid[1] = h->grid[1].as<float4>();
+    unsigned* ctl = h->ctl.as<unsigned>();
+    b.step = ctl;
+    b.work = ctl + 1;
+    b.bar = reinterpret_cast<GridBarrier*>(ctl + 4);
+    b.status = h->status.as<uint32_t>();
+    return b;
+}
+
+int32_t launch_step(vf_mpm2_batch* h) {
+    Batch2 b = view(h);
+    void* args[] = {&b};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->ctas);
+    cfg.blockDim = dim3(h->block);
+    cfg.dynamicSmemBytes = h->smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    VF_TRY_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_batch2_step, args));
+    h->launches++;
+    return VF_OK;
+}
+
+int32_t batch_status(vf_mpm2_batch* h) {
+    uint32_t st = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&st, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    if (st) {
+        VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+        set_error("a batch kernel flagged device status 0x%x%s", st,
+                  (st & ST_TIMEOUT) ? " (a grid barrier timed out)" : "");
+        return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
+    }
+    return VF_OK;
+}
+
+// Captures GRAPH_STEPS step launches into one graph.
+int32_t build_graph(vf_mpm2_batch* h) {
+    if (h->graph) return VF_OK;
+    cudaGraph_t g = nullptr;
+    VF_TRY_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int32_t rc = VF_OK;
+    for (int k = 0; k < GRAPH_STEPS && rc == VF_OK; k++) rc = launch_step(h);
+    h->launches -= GRAPH_STEPS;   // captured, not run
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        set_error("capturing the batch step failed: %s", cudaGetErrorString(e));
+        return VF_ECUDA;
+    }
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->graph = nullptr;
+        set_error("instantiating the batch step graph failed: %s", cudaGetErrorString(e));
+        return VF_ECUDA;
+    }
+    return VF_OK;
+}
+
+int32_t params_of(const vf_scene2& s, uint32_t flags, Params2* p) {
+    float w[5];
+    for (int k = 0; k < 5; k++) w[k] = bits_to_float(s.params[k]);
+    VF_REQUIRE(w[0] > 0 && w[3] >= 0 && w[4] > 0, VF_EINVAL,   // Flip.java:204-207
+               "dt > 0, bulk >= 0 and rho0 > 0, got dt %g, bulk %g, rho0 %g", w[0], w[3], w[4]);
+    *p = Params2{w[0], w[1], w[2], w[3], w[4], (flags & VF_EOS_TAIT) ? 1 : 0,
+                 (int)((flags & VF_WALL_STICKY_MASK) >> VF_WALL_STICKY_SHIFT)};
+    return VF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t flags, int32_t block,
+                             vf_mpm2_batch** out) {
+    VF_REQUIRE(out, VF_EINVAL, "out is null");
+    *out = nullptr;
+    VF_REQUIRE(scenes && nscenes >= 1, VF_EINVAL, "a batch needs scenes, got %d", nscenes);
+    if (block == 0) block = 256;
+    VF_REQUIRE(block_ok(block), VF_EINVAL, "block %d is not one of VF_BATCH_BLOCKS", block);
+    std::vector<Scene2> sc((size_t)nscenes);
+    int64_t np = 0, cells = 0, nodes = 0, entries = 0;
+    int wmax = 0;
+    for (int s = 0; s < nscenes; s++) {
+        const vf_scene2& d = scenes[s];
+        VF_REQUIRE(d.nx >= 3 && d.ny >= 3, VF_EINVAL, "scene %d: a grid needs at least three nodes each way, got %d x %d",
+                   s, d.nx, d.ny);
+        VF_REQUIRE(d.particles >= 1, VF_EINVAL, "scene %d: a step needs particles, got %d", s, d.particles);
+        int tx = d.tile_x, ty = d.tile_y;
+        if (tx == 0 && ty == 0) tx = ty = 16;
+        VF_REQUIRE(tile_ok(tx, ty), VF_EINVAL, "scene %d: tile %d x %d is not one of VF_BATCH_TILES", s, tx, ty);
+        Scene2& c = sc[s];
+        int32_t rc = params_of(d, flags, &c.prm);
+        if (rc) {
+            set_error("scene %d: %s", s, last_error());
+            return rc;
+        }
+        c.nx = d.nx;
+        c.ny = d.ny;
+        c.np = d.particles;
+        c.tx = tx;
+        c.ty = ty;
+        c.ntx = (d.nx - 2 + tx - 1) / tx;
+        c.nty = (d.ny - 2 + ty - 1) / ty;
+        c.tc = tx * ty;
+        c.p0 = (int)np;
+        c.g0 = nodes;
+        np += d.particles;
+        nodes += (int64_t)d.nx * d.ny;
+        cells += (int64_t)c.ntx * c.nty * c.tc;
+        entries += (int64_t)c.ntx * c.nty + 1;
+        wmax = std::max(wmax, (tx + 2) * (ty + 2));
+    }
+    VF_REQUIRE(np < (1ll << 31) - 64 && cells < (1ll << 31) && entries < (1ll << 30), VF_EINVAL,
+               "a batch holds fewer than 2^31 particles and cell keys, got %lld and %lld", (long long)np,
+               (long long)cells);
+    // tile entries and cell keys laid out densest scene first, so the work-stealing phases take the
+    // heaviest tiles first
+    std::vector<int> order((size_t)nscenes);
+    for (int s = 0; s < nscenes; s++) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (double)sc[a].np / ((double)sc[a].nx * sc[a].ny) > (double)sc[b].np / ((double)sc[b].nx * sc[b].ny);
+    });
+    std::vector<int> tile_scene((size_t)entries, -1);
+    int t0 = 0, c0 = 0;
+    for (int s : order) {
+        Scene2& c = sc[s];
+        c.t0 = t0;
+        c.c0 = c0;
+        const int nt = c.ntx * c.nty;
+        for (int i = 0; i < nt; i++) tile_scene[(size_t)t0 + i] = s;
+        t0 += nt + 1;
+        c0 += nt * c.tc;
+    }
+    int32_t rc = require_device();
+    if (rc) return rc;
+    vf_mpm2_batch* h = new vf_mpm2_batch();
+    h->scenes = sc;
+    h->flags = flags;
+    h->block = block;
+    h->np = np;
+    h->stride = (np + 63) / 64 * 64;
+    h->ncells = (int)cells;
+    h->nentries = (int)entries;
+    h->nodes = nodes;
+    h->smem = std::max((size_t)(block / 32) * 3 * wmax * sizeof(float), (size_t)wmax * sizeof(float2));
+    auto fail = [&](int32_t code) {
+        vf_mpm2_batch_destroy(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("cudaStreamCreate failed");
+        return fail(VF_ECUDA);
+    }
+    if (h->smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_batch2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem) != cudaSuccess) {
+        set_error("cannot give the batch step %zu bytes of shared memory", h->smem);
+        return fail(VF_ECUDA);
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2_step, block, h->smem) != cudaSuccess ||
+        per_sm < 1) {
+        set_error("the batch step does not fit on an SM with %d threads and %zu bytes of shared memory", block, h->smem);
+        return fail(VF_ECUDA);
+    }
+    h->ctas = per_sm * sm_count();
+    const size_t pb = (size_t)h->stride * NF2 * 4;
+    if ((rc = h->scene_d.alloc(sc.size() * sizeof(Scene2))) || (rc = h->tile_scene.alloc((size_t)entries * 4)) ||
+        (rc = h->part[0].alloc(pb)) || (rc = h->part[1].alloc(pb)) || (rc = h->key.alloc((size_t)np * 4)) ||
+        (rc = h->perm.alloc((size_t)np * 4)) || (rc = h->cell_count.alloc((size_t)cells * 4)) ||
+        (rc = h->cursor.alloc((size_t)cells * 4)) || (rc = h->tile_count.alloc((size_t)entries * 4)) ||
+        (rc = h->tile_start[0].alloc((size_t)entries * 4)) || (rc = h->tile_start[1].alloc((size_t)entries * 4)) ||
+        (rc = h->grid[0].alloc((size_t)nodes * 16)) || (rc = h->grid[1].alloc((size_t)nodes * 16)) ||
+        (rc = h->ctl.alloc(64)) || (rc = h->status.alloc(16)))
+        return fail(rc);
+    if (cudaMemcpyAsync(h->scene_d.ptr, sc.data(), sc.size() * sizeof(Scene2), cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(h->tile_scene.ptr, tile_scene.data(), (size_t)entries * 4, cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess ||
+        cudaMemsetAsync(h->status.ptr, 0, h->status.bytes, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        set_error("uploading the scene table failed");
+        return fail(VF_ECUDA);
+    }
+    *out = h;
+    return VF_OK;
+}
+
+int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, const float* u, const float* v,
+                           const float* m) {
+    VF_REQUIRE(h && x && y && u && v && m, VF_EINVAL, "null argument");
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    float* base = h->part[0].as<float>();
+    const float* src[5] = {x, y, u, v, m};
+    for (int f = 0; f < 5; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src[f], (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    std::vector<float> ones((size_t)h->np, 1.0f);
+    VF_TRY_CUDA(cudaMemcpyAsync(base + PJ * h->stride, ones.data(), (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaMemsetAsync(base + PC00 * h->stride, 0, (size_t)4 * h->stride * 4, h->stream));
+    for (DeviceBuffer* b : {&h->cell_count, &h->tile_count, &h->tile_start[0], &h->tile_start[1], &h->grid[0],
+                            &h->grid[1], &h->ctl, &h->status})
+        VF_TRY_CUDA(cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream));
+    Batch2 b = view(h);
+    k_batch2_tally<<<std::max(1, std::min(div_up(h->np, 256), sm_count() * 8)), 256, 0, h->stream>>>(b);
+    VF_CHECK_LAUNCH();
+    h->launches++;
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    h->steps = 0;
+    h->loaded = true;
+    return batch_status(h);
+}
+
+int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(count >= 0, VF_EINVAL, "count >= 0, got %d", count);
+    VF_REQUIRE(h->loaded, VF_ESTATE, "load the batch before stepping it");
+    int32_t rc;
+    int left = count;
+    if (left >= GRAPH_STEPS) {
+        if ((rc = build_graph(h))) return rc;
+        for (; left >= GRAPH_STEPS; left -= GRAPH_STEPS) {
+            VF_TRY_CUDA(cudaGraphLaunch(h->graph, h->stream));
+            h->launches += GRAPH_STEPS;
+        }
+    }
+    for (; left > 0; left--)
+        if ((rc = launch_step(h))) return rc;
+    h->steps += count;
+    return VF_OK;
+}
+
+int32_t vf_mpm2_batch_finish(vf_mpm2_batch* h) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    return batch_status(h);
+}
+
+int32_t vf_mpm2_batch_read(vf_mpm2_batch* h, int32_t scene, int32_t field, float* out, int64_t n) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    VF_REQUIRE(scene >= 0 && scene < (int)h->scenes.size(), VF_EINVAL, "no scene %d", scene);
+    VF_REQUIRE(h->loaded, VF_ESTATE, "the batch holds no particles yet");
+    const Scene2& sc = h->scenes[scene];
+    int32_t rc = batch_status(h);
+    if (rc) return rc;
+    if (field >= VF2_X && field <= VF2_C11) {
+        VF_REQUIRE(n == sc.np, VF_EINVAL, "scene %d holds %d particles, got %lld", scene, sc.np, (long long)n);
+        const float* src = h->part[h->steps & 1].as<float>() + (int64_t)field * h->stride + sc.p0;
+        VF_TRY_CUDA(cudaMemcpyAsync(out, src, (size_t)n * 4, cudaMemcpyDeviceToHost, h->stream));
+    } else if (field >= VF2_GM && field <= VF2_GMV) {
+        const int64_t nodes = (int64_t)sc.nx * sc.ny;
+        VF_REQUIRE(n == nodes, VF_EINVAL, "scene %d has %lld nodes, got %lld", scene, (long long)nodes, (long long)n);
+        VF_REQUIRE(h->steps > 0, VF_ESTATE, "no step has run");
+        DeviceBuffer tmp;
+        if ((rc = tmp.alloc((size_t)nodes * 4))) return rc;
+        const float4* g = h->grid[(h->steps - 1) & 1].as<float4>() + sc.g0;
+        k_batch2_unpack<<<div_up(nodes, 256), 256, 0, h->stream>>>(g, tmp.as<float>(), nodes, field - VF2_GM);
+        VF_CHECK_LAUNCH();
+        VF_TRY_CUDA(cudaMemcpyAsync(out, tmp.ptr, (size_t)nodes * 4, cudaMemcpyDeviceToHost, h->stream));
+        VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    } else {
+        set_error("no field %d", field);
+        return VF_EINVAL;
+    }
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+int32_t vf_mpm2_batch_config(const vf_mpm2_batch* h, int32_t scene, int32_t* tile_x, int32_t* tile_y, int32_t* block,
+                             int32_t* ctas) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(scene >= 0 && scene < (int)h->scenes.size(), VF_EINVAL, "no scene %d", scene);
+    if (tile_x) *tile_x = h->scenes[scene].tx;
+    if (tile_y) *tile_y = h->scenes[scene].ty;
+    if (block) *block = h->block;
+    if (ctas) *ctas = h->ctas;
+    return VF_OK;
+}
+
+int64_t vf_mpm2_batch_particles(const vf_mpm2_batch* h) { return h ? h->np : 0; }
+int64_t vf_mpm2_batch_steps(const vf_mpm2_batch* h) { return h ? h->steps : 0; }
+int64_t vf_mpm2_batch_launches(const vf_mpm2_batch* h) { return h ? h->launches : 0; }
+void* vf_mpm2_batch_stream(vf_mpm2_batch* h) { return h ? (void*)h->stream : nullptr; }
+
+void vf_mpm2_batch_destroy(vf_mpm2_batch* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    for (DeviceBuffer* b : {&h->scene_d, &h->tile_scene, &h->part[0], &h->part[1], &h->key, &h->perm, &h->cell_count,
+                            &h->cursor, &h->tile_count, &h->tile_start[0], &h->tile_start[1], &h->grid[0], &h->grid[1],
+                            &h->ctl, &h->status})
+        b->release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"

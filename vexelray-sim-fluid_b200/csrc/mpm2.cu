@@ -11,45 +11,16 @@
 // (FlipStep.java:95-98); the grid is SoA gm gmu gmv gu gv over nx*ny nodes, row-major.
 #include <vector>
 
+#include "mpm2_device.cuh"
 #include "sort.cuh"
 
 using namespace vf;
 
 namespace {
 
-enum Field2 { PX = 0, PY, PU, PV, PM, PJ, PC00, PC01, PC10, PC11, NF2 };
-
-struct Params2 {
-    float dt, gx, gy, bulk, rho0;
-    int tait, sticky;
-};
-
 struct Grid2 {
     float *gm, *gmu, *gmv, *gu, *gv;
 };
-
-constexpr float EMPTY2 = 1e-9f;     // Flip.java:316
-constexpr float J_BOUND2 = 10.0f;   // Flip.java:430
-
-// Flip.Stencil.of (Flip.java:572-581)
-struct Stencil2 {
-    int base;
-    float fx, fy, wx[3], wy[3];
-};
-
-__device__ __forceinline__ Stencil2 stencil2(float px, float py, int nx, int ny) {
-    Stencil2 s;
-    float x = clampf(px, 0.5f, (float)nx - 1.5f);
-    float y = clampf(py, 0.5f, (float)ny - 1.5f);
-    int col = (int)fminf(__fsub_rn(x, 0.5f), (float)(nx - 3));
-    int row = (int)fminf(__fsub_rn(y, 0.5f), (float)(ny - 3));
-    s.fx = __fsub_rn(x, (float)col);
-    s.fy = __fsub_rn(y, (float)row);
-    s.base = row * nx + col;
-    bspline_weights(s.fx, s.wx);
-    bspline_weights(s.fy, s.wy);
-    return s;
-}
 
 // Scatter.cell (Scatter.java:473-477): the bilinear cell, row-major over (nx-1)(ny-1).
 __device__ __forceinline__ int cell2(float x, float y, int nx, int ny) {
@@ -75,34 +46,6 @@ __global__ void __launch_bounds__(256) k_key_count2(const float* x, const float*
 
 // ------------------------------------------------------------------ the step
 
-// A segmented warp sum of `N` amounts per lane, by key (Scatter.segmentedDeposit,
-// Scatter.java:385-439): run starts by a max-scan of the lanes that begin a run, Hillis-Steele
-// rounds that add only from lanes at or after the run start; returns whether this lane is its
-// run's last (and so holds the run's sum).
-template <int N>
-__device__ __forceinline__ bool segmented_sum(float (&amt)[N], int key) {
-    const unsigned all = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    int below = __shfl_up_sync(all, key, 1);
-    int head = (lane > 0 && below == key) ? 0 : lane;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int h = __shfl_up_sync(all, head, o);
-        if (lane >= o) head = max(head, h);
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const bool take = lane - o >= head;
-#pragma unroll
-        for (int j = 0; j < N; j++) {
-            float from = __shfl_up_sync(all, amt[j], o);
-            if (take) amt[j] += from;
-        }
-    }
-    int above = __shfl_down_sync(all, key, 1);
-    return lane == 31 || above != key;
-}
-
 // Flip.scatter (Flip.java:269-303): mass, APIC momentum and the pressure's impulse on the 3x3
 // stencil, segmented by the stencil's lower-left node.
 __global__ void __launch_bounds__(256) k_flip2_scatter(const float* __restrict__ p, int64_t st, int np, int nx, int ny,
@@ -119,17 +62,7 @@ __global__ void __launch_bounds__(256) k_flip2_scatter(const float* __restrict__
         const float c00 = p[PC00 * st + i], c01 = p[PC01 * st + i], c10 = p[PC10 * st + i], c11 = p[PC11 * st + i];
         const float sp = impulse_factor(q.dt, m, q.rho0, q.bulk, p[PJ * st + i], q.tait);
         key = s.base;
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const float wgt = s.wx[k % 3] * s.wy[k / 3];
-            const float wm = wgt * m;
-            const float dx = (float)(k % 3) - s.fx, dy = (float)(k / 3) - s.fy;
-            const float velU = u + (c00 * dx + c01 * dy);
-            const float velV = w + (c10 * dx + c11 * dy);
-            amt[3 * k] = wm;
-            amt[3 * k + 1] = wm * velU + wgt * (sp * dx);
-            amt[3 * k + 2] = wm * velV + wgt * (sp * dy);
-        }
+        scatter_amounts2(s, m, u, w, c00, c01, c10, c11, sp, amt);
     }
     if (segmented_sum<27>(amt, key) && key >= 0) {
 #pragma unroll
@@ -146,37 +79,9 @@ __global__ void __launch_bounds__(256) k_flip2_scatter(const float* __restrict__
 __global__ void __launch_bounds__(256) k_flip2_grid(int nx, int ny, const Params2* __restrict__ prm, Grid2 g) {
     const int node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= nx * ny) return;
-    const Params2 q = *prm;
-    const int ni = node % nx, nj = node / nx;
-    const float m = g.gm[node];
-    float u = 0.0f, w = 0.0f;
-    if (m > EMPTY2) {
-        u = __fadd_rn(__fdiv_rn(g.gmu[node], m), __fmul_rn(q.dt, q.gx));
-        w = __fadd_rn(__fdiv_rn(g.gmv[node], m), __fmul_rn(q.dt, q.gy));
-    }
-    if (q.sticky > 0) {
-        const int t = q.sticky;
-        if (ni < t || ni > nx - 1 - t || nj < t || nj > ny - 1 - t) u = w = 0.0f;
-    } else {
-        if (!(ni > 1)) u = fmaxf(u, 0.0f);
-        if (ni > nx - 3) u = fminf(u, 0.0f);
-        if (!(nj > 1)) w = fmaxf(w, 0.0f);
-        if (nj > ny - 3) w = fminf(w, 0.0f);
-    }
-    g.gu[node] = u;
-    g.gv[node] = w;
-}
-
-__device__ __forceinline__ void keep_inside2(float& at, float& vel, int size) {   // Flip.java:548-559
-    const float lo = 1.0f, hi = (float)size - 2.0f;
-    if (at < lo) {
-        at = lo;
-        vel = fmaxf(vel, 0.0f);
-    }
-    if (at > hi) {
-        at = hi;
-        vel = fminf(vel, 0.0f);
-    }
+    const float2 v = grid_velocity2(g.gm[node], g.gmu[node], g.gmv[node], node % nx, node / nx, nx, ny, *prm);
+    g.gu[node] = v.x;
+    g.gv[node] = v.y;
 }
 
 // Flip.advectBody (Flip.java:494-545)
@@ -185,36 +90,21 @@ __global__ void __launch_bounds__(256) k_flip2_advect(float* __restrict__ p, int
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     const Params2 q = *prm;
-    Stencil2 s = stencil2(p[PX * st + i], p[PY * st + i], nx, ny);
-    float u = 0, w = 0, b00 = 0, b01 = 0, b10 = 0, b11 = 0;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        const float wgt = s.wx[k % 3] * s.wy[k / 3];
-        const float dx = (float)(k % 3) - s.fx, dy = (float)(k / 3) - s.fy;
+    const float px = p[PX * st + i], py = p[PY * st + i];
+    const Stencil2 s = stencil2(px, py, nx, ny);
+    const Advected2 a = advect2(s, px, py, p[PJ * st + i], nx, ny, q, [&](int k) {
         const int node = s.base + (k / 3) * nx + k % 3;
-        const float ui = wgt * g.gu[node], vi = wgt * g.gv[node];
-        u += ui;
-        w += vi;
-        b00 += ui * dx;
-        b01 += ui * dy;
-        b10 += vi * dx;
-        b11 += vi * dy;
-    }
-    const float c00 = 4.0f * b00, c01 = 4.0f * b01, c10 = 4.0f * b10, c11 = 4.0f * b11;
-    float x = p[PX * st + i] + q.dt * u;
-    float y = p[PY * st + i] + q.dt * w;
-    keep_inside2(x, u, nx);
-    keep_inside2(y, w, ny);
-    p[PX * st + i] = x;
-    p[PY * st + i] = y;
-    p[PU * st + i] = u;
-    p[PV * st + i] = w;
-    p[PC00 * st + i] = c00;
-    p[PC01 * st + i] = c01;
-    p[PC10 * st + i] = c10;
-    p[PC11 * st + i] = c11;
-    const float j = p[PJ * st + i] * (1.0f + q.dt * (c00 + c11));
-    p[PJ * st + i] = clampf(j, 1.0f / J_BOUND2, J_BOUND2);
+        return make_float2(g.gu[node], g.gv[node]);
+    });
+    p[PX * st + i] = a.x;
+    p[PY * st + i] = a.y;
+    p[PU * st + i] = a.u;
+    p[PV * st + i] = a.w;
+    p[PC00 * st + i] = a.c00;
+    p[PC01 * st + i] = a.c01;
+    p[PC10 * st + i] = a.c10;
+    p[PC11 * st + i] = a.c11;
+    p[PJ * st + i] = a.j;
 }
 
 // ------------------------------------------------------------------ bilinear schedules (Scatter)
