@@ -494,6 +494,7 @@ def run_batch(args, vf, dist: Dist, peak):
     b.load(xs, ys, zs, zs, ms)
     b.advance(max(3, args.warmup))
     b.finish()
+    b.phases()
     k = max(32, args.steps)
     ev0, ev1 = vf.Event(), vf.Event()
     stream = b.stream()
@@ -507,6 +508,9 @@ def run_batch(args, vf, dist: Dist, peak):
     launches = b.launches() - launches0
     ms_max = dist.max(ms)
     total = dist.sum(float(nparts))
+    ph = b.phases()   # the kernel's own per-phase clock over the timed steps
+    nl = max(1, ph.pop("launches"))
+    phases = {k: v / nl for k, v in ph.items()}
     touched = 0
     for s in range(len(table)):
         touched += int(np.count_nonzero(b.read(s, "gm")))
@@ -526,6 +530,7 @@ def run_batch(args, vf, dist: Dist, peak):
            "scenes": len(scenes), "particles": int(total), "steps": k, "ms_per_step": ms_max / k,
            "particle_steps_per_s": total * k / (ms_max / 1e3), "launches_per_step": launches / k,
            "block": cfg["block"], "ctas": cfg["ctas"], "tiles": tiles, "tuner_trials": trials,
+           "phases_ms_per_step": phases,
            "tuner_s": tune_s,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "traffic": None, "kernel": "k_batch2_step (whole step)",

@@ -174,12 +174,16 @@ int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, con
  * Returns when submitted; vf_mpm2_batch_finish waits and reports device errors. */
 int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count);
 int32_t vf_mpm2_batch_finish(vf_mpm2_batch* h);
-/* One scene's particle field (VF2_X..VF2_C11, in the batch's sorted order) or the last step's grid
+/* One scene's particle field (VF2_X..VF2_C11, in the batch's sorted order: by tile and cell, the order within a
+ * cell unspecified) or the last step's grid
  * (VF2_GM, VF2_GMU, VF2_GMV; nx*ny floats). Blocking. */
 int32_t vf_mpm2_batch_read(vf_mpm2_batch* h, int32_t scene, int32_t field, float* out, int64_t n);
 /* The tile shape a scene runs with, and the batch's block size and persistent grid size (CTAs). */
 int32_t vf_mpm2_batch_config(const vf_mpm2_batch* h, int32_t scene, int32_t* tile_x, int32_t* tile_y,
                              int32_t* block, int32_t* ctas);
+/* Device time of the step's five phases (tile scan, cell scan, permute, scatter, gather) summed over the launches
+ * since the last call, from the kernel's own clock (%globaltimer at every grid barrier), and those launches. */
+int32_t vf_mpm2_batch_phases(vf_mpm2_batch* h, double ms[5], int64_t* launches);
 int64_t vf_mpm2_batch_particles(const vf_mpm2_batch* h);
 int64_t vf_mpm2_batch_steps(const vf_mpm2_batch* h);
 int64_t vf_mpm2_batch_launches(const vf_mpm2_batch* h);

@@ -154,6 +154,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm2_batch_finish": ([_vp], ctypes.c_int32),
         "vf_mpm2_batch_read": ([_vp, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
         "vf_mpm2_batch_config": ([_vp, ctypes.c_int32] + [_i32p] * 4, ctypes.c_int32),
+        "vf_mpm2_batch_phases": ([_vp, ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int32),
         "vf_mpm2_batch_particles": ([_vp], ctypes.c_int64),
         "vf_mpm2_batch_steps": ([_vp], ctypes.c_int64),
         "vf_mpm2_batch_launches": ([_vp], ctypes.c_int64),
@@ -502,6 +503,17 @@ class BatchSimulation:
         v = [np.zeros(1, np.int32) for _ in range(4)]
         check(lib().vf_mpm2_batch_config(self._h, scene, *[_ip(q) for q in v]))
         return {"tile": (int(v[0][0]), int(v[1][0])), "block": int(v[2][0]), "ctas": int(v[3][0])}
+
+    PHASES = ("tile_scan", "cell_scan", "permute", "scatter", "gather")
+
+    def phases(self) -> dict:
+        """Device ms of each phase of the step summed over the launches since the last call, and the launches."""
+        ms = (ctypes.c_double * 5)()
+        n = np.zeros(1, np.int64)
+        check(lib().vf_mpm2_batch_phases(self._h, ms, n.ctypes.data_as(_i64p)))
+        out = {k: ms[i] for i, k in enumerate(self.PHASES)}
+        out["launches"] = int(n[0])
+        return out
 
     def particles(self) -> int:
         return int(lib().vf_mpm2_batch_particles(self._h))

@@ -18,20 +18,24 @@
 //
 // One step = five phases separated by a grid-wide barrier (the launch is cooperative, so every CTA is
 // resident; the barrier's wait is bounded and sets a status bit rather than hang):
-//   1  tile scan     per scene: tile counts -> run starts (parity buffer), counts zeroed
-//   2  cell scan     per non-empty tile: cell counts -> cursors (cell starts), counts zeroed
-//   3  permute       per slot: perm[cursor[key]++] = slot, one cursor bump per distinct key of a warp
-//   4  scatter       per tile, work-stealing: the tile's cell runs put in ascending order (the stable
-//                    sort's fix-up), then warps over contiguous chunks of the tile's run: Flip.scatter's
-//                    27 amounts per particle, summed over each cell's run across the warp
-//                    (Scatter.segmentedDeposit), the run tails adding into a warp-private node window
-//                    (distinct cells, so distinct nodes at each stencil offset: plain read-modify-write);
-//                    the warps' windows summed per node and reduced into the grid with one 16-byte
-//                    red.global.add.v4.f32 per touched node. The other parity's grid is cleared here,
-//                    over the windows of the tiles the previous step scattered into.
-//   5  gather        per tile, work-stealing: the window's node velocities (Flip.grid, fused) into shared
-//                    memory, then per particle Flip.advectBody; the particle is written to its sorted
-//                    slot of the other set, and its next cell key tallied for the next step's sort.
+//   1  tile scan     per scene: tile counts -> run starts (parity buffer), counts zeroed; each tile's run cut
+//                    into chunks of at most CHUNK particles, counted per scene
+//   2  cell scan     a warp per non-empty tile: cell counts -> cursors (cell starts), counts zeroed; CTA 0 lays
+//                    the scenes' chunks out one after another
+//   3  permute       per slot: perm[cursor[key]++] = slot, one cursor bump per distinct key of a warp. Within a
+//                    cell the order is the atomics' (unspecified, as in the reference's CountingSort,
+//                    SortTest.java:121-134); what the scatter needs is each cell's particles contiguous. The
+//                    chunks enter the item list, and the other parity's grid is cleared over the windows of
+//                    the tiles the previous step scattered into.
+//   4  scatter       a warp per chunk, work-stealing: Flip.scatter's 27 amounts per particle, summed over each
+//                    cell's run across the warp (Scatter.segmentedDeposit), the run tails adding into the warp's
+//                    private node window (distinct cells, so distinct nodes at each stencil offset: plain
+//                    read-modify-write); then one 16-byte red.global.add.v4.f32 per touched window node
+//   5  gather        a warp per chunk, work-stealing: the tile window's node velocities (Flip.grid, fused) into
+//                    the warp's shared memory, then per particle Flip.advectBody; the particle is written to its
+//                    sorted slot of the other set, and its next cell key tallied for the next step's sort.
+// Chunks bound a work item, so a dense tile (tens of thousands of particles in the 64^2 scenes) spreads over
+// many warps instead of one.
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -75,14 +79,52 @@ struct Batch2 {
     int* cursor;               // per cell: its run's start after the cell scan, its end after the permute
     int* tile_count;
     int* tile_start[2];        // per tile entry, by step parity: run start; the sentinel holds the scene's end
+    int* chunk_start;          // per tile entry: its first chunk within its scene; the sentinel the scene's chunks
+    int* scene_chunks;         // per scene: its chunks
+    int* scene_chunk_start;    // per scene (and one past): its first chunk in the item list
+    int* item_tile;            // per chunk: its tile entry
+    int item_cap;              // item_tile's length
     float4* grid[2];
     unsigned* step;            // device step counter (its parity picks the buffers)
     unsigned* work;            // work-stealing counters: [0] scatter, [1] gather
     GridBarrier* bar;
+    int wmax;                  // window nodes of the largest tile (the shared-memory windows' stride)
+    unsigned* done;            // CTAs finished with the launch (the last one closes the phase clock)
+    unsigned long long* phase_ns;   // device time per phase summed over launches, the launch count, a stamp
     uint32_t* status;
 };
 
 constexpr int BATCH_MAX_THREADS = 512;
+#ifndef BATCH_MIN_BLOCKS
+#define BATCH_MIN_BLOCKS 1
+#endif
+constexpr int NPHASE = 5;         // tile scan, cell scan, permute, scatter, gather
+constexpr int CHUNK = 1024;       // particles of a work item of the scatter and gather: a tile's run in chunks
+// Shared memory of one warp of the step: its node window (m, mu, mv arrays of the largest tile's window; the
+// gather reuses it for float2 velocities).
+__host__ __device__ constexpr int warp_smem_floats(int wmax) { return 3 * wmax; }
+
+// One particle's fields as the scatter reads them (source slot < 0: none, zeros).
+struct Part2 {
+    float x, y, u, v, m, j, c00, c01, c10, c11;
+};
+
+__device__ __forceinline__ void load_part2(Part2& q, const float* __restrict__ in, int64_t st, int src) {
+    if (src < 0) {
+        q = Part2{0, 0, 0, 0, 0, 1, 0, 0, 0, 0};
+        return;
+    }
+    q.x = in[PX * st + src];
+    q.y = in[PY * st + src];
+    q.u = in[PU * st + src];
+    q.v = in[PV * st + src];
+    q.m = in[PM * st + src];
+    q.j = in[PJ * st + src];
+    q.c00 = in[PC00 * st + src];
+    q.c01 = in[PC01 * st + src];
+    q.c10 = in[PC10 * st + src];
+    q.c11 = in[PC11 * st + src];
+}
 constexpr int BAR_SPINS = 1 << 24;   // x ~64 ns of __nanosleep: about a second
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -118,6 +160,12 @@ __device__ void grid_barrier(GridBarrier* b, uint32_t* status) {
     __syncthreads();
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // The next-step cell key and tile entry of a particle at (x, y) in scene sc.
 __device__ __forceinline__ void batch_key(const Scene2& sc, float x, float y, int& key, int& tile) {
     int col, row;
@@ -128,18 +176,9 @@ __device__ __forceinline__ void batch_key(const Scene2& sc, float x, float y, in
     key = sc.c0 + local * sc.tc + (row - tiy * sc.ty) * sc.tx + (col - tix * sc.tx);
 }
 
-// Takes the next work item for the CTA from a work-stealing counter.
-__device__ __forceinline__ int next_item(unsigned* counter, int* slot) {
-    __syncthreads();   // every thread has read the previous item
-    if (threadIdx.x == 0) *slot = (int)atomicAdd(counter, 1u);
-    __syncthreads();
-    return *slot;
-}
-
-__global__ void __launch_bounds__(BATCH_MAX_THREADS) k_batch2_step(Batch2 B) {
+__global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_step(Batch2 B) {
     extern __shared__ __align__(16) float dyn[];
     __shared__ int scan_smem[33];
-    __shared__ int item;
     const unsigned par = *B.step & 1u;   // read before the first barrier; CTA 0 advances it after
     const float* __restrict__ in = B.part[par];
     float* __restrict__ out = B.part[par ^ 1u];
@@ -149,216 +188,301 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) k_batch2_step(Batch2 B) {
     float4* g_next = B.grid[par ^ 1u];
     const int64_t st = B.stride;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int gwarp = blockIdx.x * nwarps + warp, nwarps_all = gridDim.x * nwarps;
+    float* ww = dyn + warp * warp_smem_floats(B.wmax);          // this warp's node window
+    // the phase clock: CTA 0 stamps the start and every barrier, the last CTA to finish the end
+    __shared__ unsigned long long stamp;
+    if (blockIdx.x == 0 && threadIdx.x == 0) stamp = global_ns();
+    auto phase_done = [&](int k) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long now = global_ns();
+            atomicAdd(&B.phase_ns[k], now - stamp);
+            stamp = now;
+            if (k == NPHASE - 2) B.phase_ns[NPHASE + 1] = now;   // the last phase's start
+        }
+    };
 
-    // ---- 1. tile scan, per scene
+    // ---- 1. tile scan, per scene: tile counts -> run starts, and the tiles' chunks of <= CHUNK particles
     if (blockIdx.x == 0 && threadIdx.x == 0) B.work[1] = 0;   // the previous launch's gather counter
     for (int s = blockIdx.x; s < B.nscenes; s += gridDim.x) {
         const Scene2 sc = B.scene[s];
         const int nt = sc.ntx * sc.nty;
-        int carry = 0;
+        int carry = 0, ccarry = 0;
         for (int base = 0; base < nt; base += blockDim.x) {
             const int i = base + threadIdx.x;
             const int c = i < nt ? B.tile_count[sc.t0 + i] : 0;
-            int total;
+            int total, ctotal;
             const int ex = block_exclusive(c, scan_smem, &total);
+            const int cex = block_exclusive((c + CHUNK - 1) / CHUNK, scan_smem, &ctotal);
             if (i < nt) {
                 ts_cur[sc.t0 + i] = sc.p0 + carry + ex;
+                B.chunk_start[sc.t0 + i] = ccarry + cex;
                 B.tile_count[sc.t0 + i] = 0;
             }
             carry += total;
+            ccarry += ctotal;
         }
         if (threadIdx.x == 0) {
             ts_cur[sc.t0 + nt] = sc.p0 + carry;
+            B.chunk_start[sc.t0 + nt] = ccarry;
+            B.scene_chunks[s] = ccarry;
             if (carry != sc.np) set_status(B.status, ST_RANK);
         }
     }
     grid_barrier(B.bar, B.status);
+    phase_done(0);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(B.step, 1u);
 
-    // ---- 2. cell scan, per non-empty tile
-    for (int t = blockIdx.x; t < B.nentries; t += gridDim.x) {
+    // ---- 2. cell scan, a warp per non-empty tile: the tile's cell counts -> cursors (cell starts); CTA 0 first
+    // lays out the scenes' chunks one scene after another
+    if (blockIdx.x == 0) {
+        int carry = 0;
+        for (int base = 0; base < B.nscenes; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            int total;
+            const int ex = block_exclusive(i < B.nscenes ? B.scene_chunks[i] : 0, scan_smem, &total);
+            if (i < B.nscenes) B.scene_chunk_start[i] = carry + ex;
+            carry += total;
+        }
+        if (threadIdx.x == 0) B.scene_chunk_start[B.nscenes] = carry;
+    }
+    for (int t = gwarp; t < B.nentries; t += nwarps_all) {
         const int s = B.tile_scene[t];
         if (s < 0) continue;
         const int ts = ts_cur[t], te = ts_cur[t + 1];
         if (te <= ts) continue;
         if (ts < B.scene[s].p0 || te > B.scene[s].p0 + B.scene[s].np) {   // counts that do not add up
-            if (threadIdx.x == 0) set_status(B.status, ST_RANK);
+            if (lane == 0) set_status(B.status, ST_RANK);
             continue;
         }
-        const int tc = B.scene[s].tc;
-        const int cb = B.scene[s].c0 + (t - B.scene[s].t0) * tc;
-        int carry = 0;
-        for (int base = 0; base < tc; base += blockDim.x) {
-            const int i = base + threadIdx.x;
-            const int c = i < tc ? B.cell_count[cb + i] : 0;
-            int total;
-            const int ex = block_exclusive(c, scan_smem, &total);
-            if (i < tc) {
-                B.cursor[cb + i] = ts + carry + ex;
-                B.cell_count[cb + i] = 0;
-            }
-            carry += total;
+        const int tc = B.scene[s].tc;                 // 64 .. 512 cells: per = 2 .. 16 per lane
+        const int per = tc >> 5;
+        const int cb = B.scene[s].c0 + (t - B.scene[s].t0) * tc + lane * per;
+        int c[16], sum = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            c[k] = k < per ? B.cell_count[cb + k] : 0;
+            sum += c[k];
         }
-        if (threadIdx.x == 0 && ts + carry != te) set_status(B.status, ST_RANK);
+        int run = ts + warp_inclusive(sum) - sum;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            if (k < per) {
+                B.cursor[cb + k] = run;
+                B.cell_count[cb + k] = 0;
+                run += c[k];
+            }
+        }
+        if (lane == 31 && run != te) set_status(B.status, ST_RANK);
     }
     grid_barrier(B.bar, B.status);
+    phase_done(1);
 
-    // ---- 3. permute: perm[cursor[key]++] = slot (provisional order within a cell)
+    // ---- 3. permute: perm[cursor[key]++] = slot, four slots per thread, one cursor bump per distinct key of a
+    // warp (the order within a cell is the atomics' order: unspecified, as in the reference's CountingSort); the
+    // tiles' chunks entered in the item list; and the other parity's grid cleared over the windows of the tiles
+    // the previous step scattered into
     {
         const int n32 = (B.np + 31) & ~31;
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n32; i += gridDim.x * blockDim.x) {
-            const bool valid = i < B.np;
-            const int k = valid ? B.key[i] : -1;
-            const bool ok = valid && k >= 0 && k < B.ncells;
-            if (valid && !ok) set_status(B.status, ST_OOB);
-            const unsigned peers = __match_any_sync(0xffffffffu, ok ? k : -1);
-            const int leader = __ffs(peers) - 1;
-            const int rank = __popc(peers & ((1u << lane) - 1u));
-            int base = 0;
-            if (lane == leader && ok) base = atomicAdd(&B.cursor[k], __popc(peers));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (ok) {
-                const int d = base + rank;
-                if (d >= 0 && d < B.np) B.perm[d] = i;
-                else set_status(B.status, ST_RANK);
+        const int stride = gridDim.x * blockDim.x;
+        for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n32; i0 += 4 * stride) {
+            int k[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = i0 + u * stride;
+                k[u] = i < B.np ? B.key[i] : -1;
+                if (i < B.np && (k[u] < 0 || k[u] >= B.ncells)) {
+                    set_status(B.status, ST_OOB);
+                    k[u] = -1;
+                }
+            }
+            int base[4], rank[4], leader[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {   // the atomics of the four slots in flight together
+                const unsigned peers = __match_any_sync(0xffffffffu, k[u]);
+                leader[u] = __ffs(peers) - 1;
+                rank[u] = __popc(peers & ((1u << lane) - 1u));
+                base[u] = (lane == leader[u] && k[u] >= 0) ? atomicAdd(&B.cursor[k[u]], __popc(peers)) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int d = __shfl_sync(0xffffffffu, base[u], leader[u]) + rank[u];
+                if (k[u] >= 0) {
+                    if (d >= 0 && d < B.np) B.perm[d] = i0 + u * stride;
+                    else set_status(B.status, ST_RANK);
+                }
             }
         }
     }
-    grid_barrier(B.bar, B.status);
-
-    // ---- 4. scatter, per tile
-    for (;;) {
-        const int t = next_item(&B.work[0], &item);
-        if (t >= B.nentries) break;
+    for (int t = gwarp; t < B.nentries; t += nwarps_all) {
         const int s = B.tile_scene[t];
         if (s < 0) continue;
-        const Scene2 sc = B.scene[s];
-        const int lt = t - sc.t0;
-        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;   // the tile's first cell = first node
-        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
-        // the other parity's grid: clear this tile's window if the previous step scattered into it
-        if (ts_prev[t + 1] > ts_prev[t]) {
-            for (int j = threadIdx.x; j < wn; j += blockDim.x) {
-                const int gi = x0 + j % wx, gj = y0 + j / wx;
-                if (gi < sc.nx && gj < sc.ny) g_next[sc.g0 + (int64_t)gj * sc.nx + gi] = make_float4(0, 0, 0, 0);
+        const Scene2& sc = B.scene[s];
+        const int ts = ts_cur[t], te = ts_cur[t + 1];
+        if (te > ts && ts >= sc.p0 && te <= sc.p0 + sc.np) {   // the tile's chunks into the item list
+            const int item0 = B.scene_chunk_start[s] + B.chunk_start[t];
+            const int nch = (te - ts + CHUNK - 1) / CHUNK;
+            for (int q = lane; q < nch; q += 32) {
+                if (item0 + q >= 0 && item0 + q < B.item_cap) B.item_tile[item0 + q] = t;
+                else set_status(B.status, ST_OOB);
             }
         }
-        const int ts = ts_cur[t], te = ts_cur[t + 1];
-        if (te <= ts || ts < sc.p0 || te > sc.p0 + sc.np) continue;   // empty, or flagged in the cell scan
-        const int cb = sc.c0 + lt * sc.tc;
-        // the stable order: each cell's run of perm ascending
-        for (int c = threadIdx.x; c < sc.tc; c += blockDim.x) {
-            const int cs = c == 0 ? ts : B.cursor[cb + c - 1];
-            const int ce = B.cursor[cb + c];
-            if (cs < ts || ce > te || ce < cs) set_status(B.status, ST_RANK);
-            else if (ce - cs > 1) insertion_sort_run(B.perm + cs, ce - cs);
+        if (!(ts_prev[t + 1] > ts_prev[t])) continue;
+        const int lt = t - sc.t0;
+        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;
+        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
+        for (int j = lane; j < wn; j += 32) {
+            const int gi = x0 + j % wx, gj = y0 + j / wx;
+            if (gi < sc.nx && gj < sc.ny) g_next[sc.g0 + (int64_t)gj * sc.nx + gi] = make_float4(0, 0, 0, 0);
         }
-        for (int j = threadIdx.x; j < nwarps * 3 * wn; j += blockDim.x) dyn[j] = 0.0f;
-        __syncthreads();
-        float* ww = dyn + warp * 3 * wn;   // this warp's window: m, mu, mv arrays of wn nodes
-        const int chunk = ((te - ts + nwarps - 1) / nwarps + 31) & ~31;
-        const int w0 = ts + warp * chunk, w1 = min(te, w0 + chunk);
-        for (int b = w0; b < w1; b += 32) {
-            const int slot = b + lane;
+    }
+    grid_barrier(B.bar, B.status);
+    phase_done(2);
+    const int items = min(B.scene_chunk_start[B.nscenes], B.item_cap);
+
+    // ---- 4. scatter: each warp takes chunks (<= CHUNK particles of one tile) from the work counter and scatters
+    // one alone through its own node window
+    for (;;) {
+        int k = 0;
+        if (lane == 0) k = (int)atomicAdd(&B.work[0], 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= items) break;
+        const int t = B.item_tile[k];
+        const int s = t >= 0 && t < B.nentries ? B.tile_scene[t] : -1;
+        if (s < 0) {
+            if (lane == 0) set_status(B.status, ST_OOB);
+            continue;
+        }
+        const Scene2& sc = B.scene[s];
+        const int q = k - B.scene_chunk_start[s] - B.chunk_start[t];
+        const int ts = ts_cur[t], te = ts_cur[t + 1];
+        const int p0 = sc.p0, p1 = sc.p0 + sc.np;
+        const int c0 = ts + q * CHUNK, c1 = min(te, c0 + CHUNK);
+        if (q < 0 || c0 >= c1 || ts < p0 || te > p1) {
+            if (lane == 0) set_status(B.status, ST_OOB);
+            continue;
+        }
+        const int lt = t - sc.t0;
+        const int tx = sc.tx, ty = sc.ty, nx = sc.nx, ny = sc.ny;
+        const int x0 = (lt % sc.ntx) * tx, y0 = (lt / sc.ntx) * ty;   // the tile's first cell = first node
+        const int wx = tx + 2, wn = wx * (ty + 2);
+        const Params2 prm = sc.prm;
+        for (int j = lane; j < 3 * wn; j += 32) ww[j] = 0.0f;
+        __syncwarp();
+        // software pipeline: the next batch's fields and the one after's source slots in flight
+        auto source = [&](int slot) {
+            if (slot >= c1) return -1;
+            const int src = B.perm[slot];
+            if (src < p0 || src >= p1) {
+                set_status(B.status, ST_OOB);
+                return -1;
+            }
+            return src;
+        };
+        Part2 cur, nxt;
+        int s_cur = source(c0 + lane);
+        load_part2(cur, in, st, s_cur);
+        int s_nxt = source(c0 + 32 + lane);
+        for (int b = c0; b < c1; b += 32) {
+            load_part2(nxt, in, st, s_nxt);
+            const int s_after = source(b + 64 + lane);
             float amt[27];
 #pragma unroll
-            for (int k = 0; k < 27; k++) amt[k] = 0.0f;
+            for (int a = 0; a < 27; a++) amt[a] = 0.0f;
             int key = -1;
-            if (slot < w1) {
-                const int src = B.perm[slot];
-                if (src < sc.p0 || src >= sc.p0 + sc.np) {
-                    set_status(B.status, ST_OOB);
+            if (s_cur >= 0) {
+                const Stencil2 sn = stencil2(cur.x, cur.y, nx, ny);
+                const int lx = sn.col - x0, ly = sn.row - y0;
+                if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
+                    const float sp = impulse_factor(prm.dt, cur.m, prm.rho0, prm.bulk, cur.j, prm.tait);
+                    scatter_amounts2(sn, cur.m, cur.u, cur.v, cur.c00, cur.c01, cur.c10, cur.c11, sp, amt);
+                    key = ly * wx + lx;   // the window index of the stencil's lower-left node
                 } else {
-                    const float px = in[PX * st + src], py = in[PY * st + src];
-                    const float m = in[PM * st + src], u = in[PU * st + src], v = in[PV * st + src];
-                    const float pj = in[PJ * st + src];
-                    const float c00 = in[PC00 * st + src], c01 = in[PC01 * st + src];
-                    const float c10 = in[PC10 * st + src], c11 = in[PC11 * st + src];
-                    const Stencil2 sn = stencil2(px, py, sc.nx, sc.ny);
-                    const int lx = sn.col - x0, ly = sn.row - y0;
-                    if (lx >= 0 && lx < sc.tx && ly >= 0 && ly < sc.ty) {
-                        const float sp = impulse_factor(sc.prm.dt, m, sc.prm.rho0, sc.prm.bulk, pj, sc.prm.tait);
-                        scatter_amounts2(sn, m, u, v, c00, c01, c10, c11, sp, amt);
-                        key = ly * wx + lx;   // the window index of the stencil's lower-left node
-                    } else {
-                        set_status(B.status, ST_OOB);
-                    }
+                    set_status(B.status, ST_OOB);
                 }
             }
             const bool tail = segmented_sum<27>(amt, key) && key >= 0;
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
+            for (int o = 0; o < 9; o++) {
                 if (tail) {
-                    const int wi = key + (k / 3) * wx + k % 3;
-                    ww[wi] += amt[3 * k];
-                    ww[wn + wi] += amt[3 * k + 1];
-                    ww[2 * wn + wi] += amt[3 * k + 2];
+                    const int wi = key + (o / 3) * wx + o % 3;
+                    ww[wi] += amt[3 * o];
+                    ww[wn + wi] += amt[3 * o + 1];
+                    ww[2 * wn + wi] += amt[3 * o + 2];
                 }
                 __syncwarp();
             }
+            cur = nxt;
+            s_cur = s_nxt;
+            s_nxt = s_after;
         }
-        __syncthreads();
-        for (int j = threadIdx.x; j < wn; j += blockDim.x) {
-            float a = 0.0f, bu = 0.0f, bv = 0.0f;
-            for (int w = 0; w < nwarps; w++) {
-                const float* o = dyn + w * 3 * wn;
-                a += o[j];
-                bu += o[wn + j];
-                bv += o[2 * wn + j];
-            }
+        for (int j = lane; j < wn; j += 32) {
+            const float a = ww[j], bu = ww[wn + j], bv = ww[2 * wn + j];
             if (a == 0.0f && bu == 0.0f && bv == 0.0f) continue;
             const int gi = x0 + j % wx, gj = y0 + j / wx;
-            if (gi >= sc.nx || gj >= sc.ny) {
+            if (gi >= nx || gj >= ny) {
                 set_status(B.status, ST_OOB);
                 continue;
             }
-            red_add_v4(&g_cur[sc.g0 + (int64_t)gj * sc.nx + gi], a, bu, bv, 0.0f);
+            red_add_v4(&g_cur[sc.g0 + (int64_t)gj * nx + gi], a, bu, bv, 0.0f);
         }
+        __syncwarp();   // the window is free for the next chunk
     }
     grid_barrier(B.bar, B.status);
+    phase_done(3);
     if (blockIdx.x == 0 && threadIdx.x == 0) B.work[0] = 0;
 
-    // ---- 5. gather, per tile: grid update into shared memory, then advect
-    float2* vw = reinterpret_cast<float2*>(dyn);
+    // ---- 5. gather: each warp takes chunks and gathers one alone: the tile window's node velocities (the grid
+    // update) into its shared memory, then the chunk's particles advected
+    float2* vw = reinterpret_cast<float2*>(ww);
     for (;;) {
-        const int t = next_item(&B.work[1], &item);
-        if (t >= B.nentries) break;
-        const int s = B.tile_scene[t];
-        if (s < 0) continue;
-        const Scene2 sc = B.scene[s];
+        int k = 0;
+        if (lane == 0) k = (int)atomicAdd(&B.work[1], 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= items) break;
+        const int t = B.item_tile[k];
+        const int s = t >= 0 && t < B.nentries ? B.tile_scene[t] : -1;
+        if (s < 0) continue;   // flagged in the scatter
+        const Scene2& sc = B.scene[s];
+        const int q = k - B.scene_chunk_start[s] - B.chunk_start[t];
         const int ts = ts_cur[t], te = ts_cur[t + 1];
-        if (te <= ts || ts < sc.p0 || te > sc.p0 + sc.np) continue;
+        const int p0 = sc.p0, p1 = sc.p0 + sc.np;
+        const int c0 = ts + q * CHUNK, c1 = min(te, c0 + CHUNK);
+        if (q < 0 || c0 >= c1 || ts < p0 || te > p1) continue;
         const int lt = t - sc.t0;
-        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;
-        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
-        for (int j = threadIdx.x; j < wn; j += blockDim.x) {
+        const int tx = sc.tx, ty = sc.ty, nx = sc.nx, ny = sc.ny;
+        const int x0 = (lt % sc.ntx) * tx, y0 = (lt / sc.ntx) * ty;
+        const int wx = tx + 2, wn = wx * (ty + 2);
+        const Params2 prm = sc.prm;
+        for (int j = lane; j < wn; j += 32) {
             const int gi = x0 + j % wx, gj = y0 + j / wx;
             float2 v = make_float2(0.0f, 0.0f);
-            if (gi < sc.nx && gj < sc.ny) {
-                const float4 g = g_cur[sc.g0 + (int64_t)gj * sc.nx + gi];
-                v = grid_velocity2(g.x, g.y, g.z, gi, gj, sc.nx, sc.ny, sc.prm);
+            if (gi < nx && gj < ny) {
+                const float4 gv = g_cur[sc.g0 + (int64_t)gj * nx + gi];
+                v = grid_velocity2(gv.x, gv.y, gv.z, gi, gj, nx, ny, prm);
             }
             vw[j] = v;
         }
-        __syncthreads();
-        for (int b = ts; b < te; b += blockDim.x) {
-            const int slot = b + threadIdx.x;
+        __syncwarp();
+        int src_next = c0 + lane < c1 ? B.perm[c0 + lane] : -1;
+        for (int b = c0; b < c1; b += 32) {
+            const int slot = b + lane;
+            int src = src_next;
+            if (slot + 32 < c1) src_next = B.perm[slot + 32];   // the next round's source
             int nkey = -1, ntile = -1;
-            if (slot < te) {
-                int src = B.perm[slot];
-                if (src < sc.p0 || src >= sc.p0 + sc.np) {
+            if (slot < c1) {
+                if (src < p0 || src >= p1) {
                     set_status(B.status, ST_OOB);
                     src = slot;
                 }
                 const float px = in[PX * st + src], py = in[PY * st + src];
                 const float pj = in[PJ * st + src], pm = in[PM * st + src];
-                const Stencil2 sn = stencil2(px, py, sc.nx, sc.ny);
+                const Stencil2 sn = stencil2(px, py, nx, ny);
                 const int lx = sn.col - x0, ly = sn.row - y0;
                 Advected2 a;
-                if (lx >= 0 && lx < sc.tx && ly >= 0 && ly < sc.ty) {
+                if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
                     const int wb = ly * wx + lx;
-                    a = advect2(sn, px, py, pj, sc.nx, sc.ny, sc.prm,
-                                [&](int k) { return vw[wb + (k / 3) * wx + k % 3]; });
+                    a = advect2(sn, px, py, pj, nx, ny, prm, [&](int o) { return vw[wb + (o / 3) * wx + o % 3]; });
                 } else {
                     set_status(B.status, ST_OOB);
                     a = Advected2{px, py, in[PU * st + src], in[PV * st + src], in[PC00 * st + src],
@@ -379,6 +503,17 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) k_batch2_step(Batch2 B) {
             }
             warp_tally(B.cell_count, nkey, nkey >= 0, B.ncells, B.status);
             warp_tally(B.tile_count, ntile, ntile >= 0, B.nentries, B.status);
+        }
+        __syncwarp();   // the window is free for the next chunk
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(B.done, 1u) == gridDim.x - 1) {   // the last CTA: the launch's end
+            atomicExch(B.done, 0u);
+            const unsigned long long start = *(volatile unsigned long long*)&B.phase_ns[NPHASE + 1];
+            atomicAdd(&B.phase_ns[NPHASE - 1], global_ns() - start);
+            atomicAdd(&B.phase_ns[NPHASE], 1ull);
         }
     }
 }
@@ -441,9 +576,11 @@ struct vf_mpm2_batch {
     int ncells = 0, nentries = 0;
     cudaStream_t stream = nullptr;
     DeviceBuffer scene_d, tile_scene, part[2], key, perm, cell_count, cursor, tile_count, tile_start[2], grid[2];
-    DeviceBuffer ctl;      // step counter, two work counters, the barrier
+    DeviceBuffer chunk_start, scene_chunks, scene_chunk_start, item_tile;
+    DeviceBuffer ctl;      // step counter, two work counters, the done count, the barrier, the phase clock
     DeviceBuffer status;
     int64_t nodes = 0;
+    int wmax = 0;
     int64_t steps = 0, launches = 0;
     bool loaded = false;
     cudaGraphExec_t graph = nullptr;
@@ -469,12 +606,20 @@ Batch2 view(vf_mpm2_batch* h) {
     b.tile_count = h->tile_count.as<int>();
     b.tile_start[0] = h->tile_start[0].as<int>();
     b.tile_start[1] = h->tile_start[1].as<int>();
+    b.chunk_start = h->chunk_start.as<int>();
+    b.scene_chunks = h->scene_chunks.as<int>();
+    b.scene_chunk_start = h->scene_chunk_start.as<int>();
+    b.item_tile = h->item_tile.as<int>();
+    b.item_cap = (int)(h->item_tile.bytes / 4);
     b.grid[0] = h->grid[0].as<float4>();
     b.grid[1] = h->grid[1].as<float4>();
     unsigned* ctl = h->ctl.as<unsigned>();
     b.step = ctl;
     b.work = ctl + 1;
+    b.wmax = h->wmax;
+    b.done = ctl + 3;
     b.bar = reinterpret_cast<GridBarrier*>(ctl + 4);
+    b.phase_ns = reinterpret_cast<unsigned long long*>(ctl + 8);
     b.status = h->status.as<uint32_t>();
     return b;
 }
@@ -623,7 +768,8 @@ int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t 
     h->ncells = (int)cells;
     h->nentries = (int)entries;
     h->nodes = nodes;
-    h->smem = std::max((size_t)(block / 32) * 3 * wmax * sizeof(float), (size_t)wmax * sizeof(float2));
+    h->wmax = wmax;
+    h->smem = (size_t)(block / 32) * warp_smem_floats(wmax) * sizeof(float);
     auto fail = [&](int32_t code) {
         vf_mpm2_batch_destroy(h);
         return code;
@@ -651,7 +797,10 @@ int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t 
         (rc = h->cursor.alloc((size_t)cells * 4)) || (rc = h->tile_count.alloc((size_t)entries * 4)) ||
         (rc = h->tile_start[0].alloc((size_t)entries * 4)) || (rc = h->tile_start[1].alloc((size_t)entries * 4)) ||
         (rc = h->grid[0].alloc((size_t)nodes * 16)) || (rc = h->grid[1].alloc((size_t)nodes * 16)) ||
-        (rc = h->ctl.alloc(64)) || (rc = h->status.alloc(16)))
+        (rc = h->chunk_start.alloc((size_t)entries * 4)) || (rc = h->scene_chunks.alloc((size_t)nscenes * 4)) ||
+        (rc = h->scene_chunk_start.alloc((size_t)(nscenes + 1) * 4)) ||
+        (rc = h->item_tile.alloc((size_t)(np / CHUNK + entries + 1) * 4)) ||
+        (rc = h->ctl.alloc(128)) || (rc = h->status.alloc(16)))
         return fail(rc);
     if (cudaMemcpyAsync(h->scene_d.ptr, sc.data(), sc.size() * sizeof(Scene2), cudaMemcpyHostToDevice, h->stream) !=
             cudaSuccess ||
@@ -755,6 +904,19 @@ int32_t vf_mpm2_batch_config(const vf_mpm2_batch* h, int32_t scene, int32_t* til
     return VF_OK;
 }
 
+int32_t vf_mpm2_batch_phases(vf_mpm2_batch* h, double ms[5], int64_t* launches) {
+    VF_REQUIRE(h && ms, VF_EINVAL, "null argument");
+    unsigned long long ns[NPHASE + 1];
+    unsigned long long* dev = reinterpret_cast<unsigned long long*>(h->ctl.as<unsigned>() + 8);
+    VF_TRY_CUDA(cudaMemcpyAsync(ns, dev, sizeof ns, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < NPHASE; k++) ms[k] = (double)ns[k] / 1e6;
+    if (launches) *launches = (int64_t)ns[NPHASE];
+    VF_TRY_CUDA(cudaMemsetAsync(dev, 0, sizeof ns, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
 int64_t vf_mpm2_batch_particles(const vf_mpm2_batch* h) { return h ? h->np : 0; }
 int64_t vf_mpm2_batch_steps(const vf_mpm2_batch* h) { return h ? h->steps : 0; }
 int64_t vf_mpm2_batch_launches(const vf_mpm2_batch* h) { return h ? h->launches : 0; }
@@ -766,7 +928,8 @@ void vf_mpm2_batch_destroy(vf_mpm2_batch* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
     for (DeviceBuffer* b : {&h->scene_d, &h->tile_scene, &h->part[0], &h->part[1], &h->key, &h->perm, &h->cell_count,
                             &h->cursor, &h->tile_count, &h->tile_start[0], &h->tile_start[1], &h->grid[0], &h->grid[1],
-                            &h->ctl, &h->status})
+                            &h->chunk_start, &h->scene_chunks, &h->scene_chunk_start, &h->item_tile, &h->ctl,
+                            &h->status})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
