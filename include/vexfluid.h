@@ -301,6 +301,59 @@ void* vf_swe_stream(vf_swe* h);
 int32_t vf_swe_on_gpu(const vf_swe* h);
 void vf_swe_destroy(vf_swe* h);
 
+/* The state on the device, for callers that work on it between steps (the learned correction): pointers to
+ * the current h, hu, hv (nx*ny floats each, on the handle's stream), valid until the next dispatch. After changing
+ * it, vf_swe_measure_speed sets the next step's wave speed from the changed state (as load's fastestWave does). */
+int32_t vf_swe_state(vf_swe* h, float** hcell, float** hu, float** hv);
+int32_t vf_swe_measure_speed(vf_swe* h);
+/* The fine handle's current state averaged over 2x2 blocks into the coarse handle's current state (fine nx, ny
+ * = 2 x the coarse's), and the coarse wave speed measured; on the device. */
+int32_t vf_swe_restrict(vf_swe* fine, vf_swe* coarse);
+/* The inverse for a patch: the coarse cells [x0, x0 + nx/2) x [y0, y0 + ny/2) of `coarse`, each copied to its 2x2
+ * fine cells of `fine` (a patch of nx x ny cells), and the fine wave speed measured. */
+int32_t vf_swe_prolong(vf_swe* coarse, int32_t x0, int32_t y0, vf_swe* fine);
+/* The fine patch's interior [m, nx - m) x [m, ny - m) (m even) averaged back into the coarse cells it covers
+ * (patch cell (m, m) lies over coarse cell (x0 + m/2, y0 + m/2)). */
+int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t margin, vf_swe* coarse, int32_t x0, int32_t y0);
+
+/* ------------------------------------------------------------------ the flux-correction network */
+/* A 3-layer 5x5 convolutional network (3 -> 32 -> 32 -> 6 channels, ReLU between; bf16 weights and activations,
+ * fp32 accumulation on the tensor cores) that corrects a coarse shallow-water state by the divergence of six
+ * face fields (the east and north faces' transfer of h, hu, hv; faces on the walls held at zero, so totals are
+ * conserved):  U(i,j) -= s_flux (G_e(i,j) - G_e(i-1,j) + G_n(i,j) - G_n(i,j-1)).
+ * No counterpart in the reference. Trained on samples (S, P, T): a coarse state S, the plain coarse solver's state
+ * P an interval later, and the fine solver's state after that interval restricted to the coarse grid T; the loss
+ * is the mean over cells, components and samples of ((P - s_flux Div G(S) - T) / s_res)^2 / 2, and training is
+ * Adam on fp32 master parameters. The parameters, in order: w1 [32][25][3], b1 [32], w2 [32][25][32], b2 [32],
+ * w3 [6][25][32], b3 [6] (w[cout][ky*5+kx][cin]); the features are (h - 1)*4, hu*4, hv*4. */
+typedef struct vf_cnn vf_cnn;
+
+int64_t vf_cnn_param_count(void);
+/* For an nx x ny coarse grid: up to `batch` samples per training step, a ring of `samples` sample slots. */
+int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, float s_flux, float s_res,
+                      vf_cnn** out);
+/* Reads or writes (write != 0: also resets Adam's moments) the fp32 parameters, vf_cnn_param_count() floats. */
+int32_t vf_cnn_params(vf_cnn* h, float* host, int64_t n, int32_t write);
+/* Sample slot `slot`, part kind (0 = S, 1 = P, 2 = T): three planes copied in from device (from_host = 0) or host. */
+int32_t vf_cnn_put(vf_cnn* h, int32_t slot, int32_t kind, const float* hcell, const float* hu, const float* hv,
+                   int32_t from_host);
+/* The loss over samples, and (loss_plain non-null) the loss with no correction. */
+int32_t vf_cnn_loss(vf_cnn* h, const int32_t* slots, int32_t n, double* loss, double* loss_plain);
+/* The loss's gradient (vf_cnn_param_count() floats) over samples, without an update. */
+int32_t vf_cnn_gradients(vf_cnn* h, const int32_t* slots, int32_t n, float* grads, double* loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss over samples; *loss is the loss before it. */
+int32_t vf_cnn_train(vf_cnn* h, const int32_t* slots, int32_t n, float lr, double* loss);
+/* The correction of a state in place (device planes of the network's grid, e.g. from vf_swe_state). */
+int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv);
+/* The network's output for sample slot's S: nx*ny*8 floats (six used per cell, the east face's h, hu, hv then the
+ * north face's). */
+int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out);
+void* vf_cnn_stream(vf_cnn* h);
+int32_t vf_cnn_profile(vf_cnn* h, int32_t enable);
+int32_t vf_cnn_profile_read(vf_cnn* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches);
+int64_t vf_cnn_launches(const vf_cnn* h);
+void vf_cnn_destroy(vf_cnn* h);
+
 /* ------------------------------------------------------------------ particle diagnostics */
 /* ParticleDiagnostics.of over a device-resident J (ParticleDiagnostics.java:126-148): out = {minDensity,
  * maxDensity, lowDensity, highDensity, mach, courant, nonFinite}. */

@@ -162,6 +162,27 @@ def lib() -> ctypes.CDLL:
         "vf_mpm2_batch_destroy": ([_vp], None),
         "vf_mpm2_autotune": ([ctypes.POINTER(Scene2), ctypes.c_int32, ctypes.c_uint32] + [_f32p] * 5 +
                              [ctypes.c_char_p, _i32p, _i32p], ctypes.c_int32),
+        "vf_swe_state": ([_vp] + [ctypes.POINTER(_vp)] * 3, ctypes.c_int32),
+        "vf_swe_measure_speed": ([_vp], ctypes.c_int32),
+        "vf_swe_restrict": ([_vp, _vp], ctypes.c_int32),
+        "vf_swe_prolong": ([_vp, ctypes.c_int32, ctypes.c_int32, _vp], ctypes.c_int32),
+        "vf_swe_restrict_patch": ([_vp, ctypes.c_int32, _vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
+        "vf_cnn_param_count": ([], ctypes.c_int64),
+        "vf_cnn_create": ([ctypes.c_int32] * 4 + [ctypes.c_float, ctypes.c_float, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_cnn_params": ([_vp, _f32p, ctypes.c_int64, ctypes.c_int32], ctypes.c_int32),
+        "vf_cnn_put": ([_vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_cnn_loss": ([_vp, _i32p, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+                        ctypes.c_int32),
+        "vf_cnn_gradients": ([_vp, _i32p, ctypes.c_int32, _f32p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
+        "vf_cnn_train": ([_vp, _i32p, ctypes.c_int32, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
+        "vf_cnn_correct": ([_vp, _vp, _vp, _vp], ctypes.c_int32),
+        "vf_cnn_fluxes": ([_vp, ctypes.c_int32, _f32p], ctypes.c_int32),
+        "vf_cnn_stream": ([_vp], _vp),
+        "vf_cnn_profile": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_cnn_profile_read": ([_vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
+                                 _i64p], ctypes.c_int32),
+        "vf_cnn_launches": ([_vp], ctypes.c_int64),
+        "vf_cnn_destroy": ([_vp], None),
         "vf_swe_create": ([ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_swe_load": ([_vp] + [_f32p] * 3 + [_i32p, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
@@ -561,6 +582,106 @@ def autotune(scenes: Sequence[Scene], x, y, u, v, m, *, tait: bool = False, stic
     return tuned, int(block[0]), int(trials[0])
 
 
+class FluxNet:
+    """The flux-correction network of the learned coarse shallow-water solver (vf_cnn_*): a 3-layer 5x5 CNN
+    (3 -> 32 -> 32 -> 6) whose output's divergence corrects a coarse state, trained with Adam on samples
+    (S, P, T) held on the device (see vexfluid.h for the loss)."""
+
+    def __init__(self, nx: int, ny: int, *, batch: int = 1, samples: int = 1, s_flux: float = 1e-3,
+                 s_res: float = 1e-3):
+        h = _vp()
+        check(lib().vf_cnn_create(nx, ny, batch, samples, s_flux, s_res, ctypes.byref(h)))
+        self._h = h
+        self.nx, self.ny, self.s_flux, self.s_res = nx, ny, s_flux, s_res
+
+    @staticmethod
+    def count() -> int:
+        return int(lib().vf_cnn_param_count())
+
+    def params(self, values=None) -> np.ndarray | None:
+        n = self.count()
+        if values is None:
+            out = np.empty(n, np.float32)
+            check(lib().vf_cnn_params(self._h, _fp(out), n, 0))
+            return out
+        a = _f32(values, n)
+        check(lib().vf_cnn_params(self._h, _fp(a), n, 1))
+        return None
+
+    def put(self, slot: int, kind: int, h, hu, hv) -> None:
+        """Sample slot's part kind (0 S, 1 P, 2 T) from host arrays."""
+        n = self.nx * self.ny
+        a = [_f32(np.asarray(q).ravel(), n) for q in (h, hu, hv)]
+        check(lib().vf_cnn_put(self._h, slot, kind, *[q.ctypes.data_as(_vp) for q in a], 1))
+
+    def put_state(self, slot: int, kind: int, sim: "PatchSimulation") -> None:
+        """Sample slot's part kind from a PatchSimulation's current device state (same grid)."""
+        ptr = sim.device_state()
+        check(lib().vf_cnn_put(self._h, slot, kind, *ptr, 0))
+
+    def _slots(self, slots):
+        a = np.ascontiguousarray(np.atleast_1d(slots), np.int32)
+        return _ip(a), len(a), a
+
+    def loss(self, slots) -> tuple[float, float]:
+        p, n, keep = self._slots(slots)
+        l, lp = ctypes.c_double(), ctypes.c_double()
+        check(lib().vf_cnn_loss(self._h, p, n, ctypes.byref(l), ctypes.byref(lp)))
+        return l.value, lp.value
+
+    def gradients(self, slots) -> tuple[np.ndarray, float]:
+        p, n, keep = self._slots(slots)
+        g = np.empty(self.count(), np.float32)
+        l = ctypes.c_double()
+        check(lib().vf_cnn_gradients(self._h, p, n, _fp(g), ctypes.byref(l)))
+        return g, l.value
+
+    def train(self, slots, lr: float) -> float:
+        p, n, keep = self._slots(slots)
+        l = ctypes.c_double()
+        check(lib().vf_cnn_train(self._h, p, n, lr, ctypes.byref(l)))
+        return l.value
+
+    def fluxes(self, slot: int = 0) -> np.ndarray:
+        out = np.empty(self.nx * self.ny * 8, np.float32)
+        check(lib().vf_cnn_fluxes(self._h, slot, _fp(out)))
+        return out.reshape(self.ny, self.nx, 8)
+
+    def correct(self, sim: "PatchSimulation") -> None:
+        """The correction of a PatchSimulation's current state in place, and its wave speed measured again."""
+        check(lib().vf_cnn_correct(self._h, *sim.device_state()))
+        check(lib().vf_swe_measure_speed(sim._h))
+
+    def profile(self, on: bool) -> None:
+        check(lib().vf_cnn_profile(self._h, 1 if on else 0))
+
+    def profile_read(self) -> dict:
+        return _profile_read(lib().vf_cnn_profile_read, self._h)
+
+    def launches(self) -> int:
+        return int(lib().vf_cnn_launches(self._h))
+
+    def stream(self):
+        return lib().vf_cnn_stream(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_cnn_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def scatter2(mode: int, nx: int, ny: int, x, y, u, v, m):
     """One bilinear P2G (Scatter.kernel / preReduced / gather / segmented) of host particles."""
     n = len(x)
@@ -800,6 +921,27 @@ class PatchSimulation:
     def params(self, params) -> None:
         w = _words(params)
         check(lib().vf_swe_params(self._h, _ip(w), len(w)))
+
+    def device_state(self):
+        """Device pointers (h, hu, hv) of the current state, valid until the next dispatch."""
+        p = [_vp() for _ in range(3)]
+        check(lib().vf_swe_state(self._h, *[ctypes.byref(q) for q in p]))
+        return p
+
+    def measure_speed(self) -> None:
+        check(lib().vf_swe_measure_speed(self._h))
+
+    def restrict_from(self, fine: "PatchSimulation") -> None:
+        """This (coarse) state = the fine state averaged over 2x2 cells."""
+        check(lib().vf_swe_restrict(fine._h, self._h))
+
+    def prolong_from(self, coarse: "PatchSimulation", x0: int, y0: int) -> None:
+        """This patch's cells copied from coarse cells from (x0, y0) on, each to its 2x2 fine cells."""
+        check(lib().vf_swe_prolong(coarse._h, x0, y0, self._h))
+
+    def restrict_into(self, margin: int, coarse: "PatchSimulation", x0: int, y0: int) -> None:
+        """This patch's interior (margin cells in from each side) averaged back into the coarse cells it covers."""
+        check(lib().vf_swe_restrict_patch(self._h, margin, coarse._h, x0, y0))
 
     def advance(self, ticks_: int, max_steps: int) -> Advance:
         steps = ctypes.c_int32()

@@ -292,6 +292,50 @@ struct DiagPart {
     int non_finite, negative, wet;
 };
 
+// The next step's wave speed from a state the host or another kernel changed: bits of the largest
+// max(|u|, |v|) + sqrt(g h), the same per-cell expression the step's update computes (ShallowWater.java:236-241).
+__global__ void __launch_bounds__(256) k_swe_speed(const float* h, const float* hu, const float* hv, int64_t n,
+                                                   const float* params, int* speed) {
+    const float g = params[0], dry = params[4];
+    int best = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float d = h[i];
+        const float u = velocity(d, hu[i], dry), w = velocity(d, hv[i], dry);
+        best = max(best, __float_as_int(fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * d)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(speed, best);
+}
+
+// Coarse cell (i, j) of the box [x0, x0 + cnx) x [y0, y0 + cny) = the mean of fine cells (2i..2i+1, 2j..2j+1)
+// counted from the fine patch's cell (fx0, fy0).
+__global__ void k_swe_restrict(const float* const* fine, int fnx, int fx0, int fy0, float* const* coarse, int ccnx,
+                               int x0, int y0, int cnx, int cny) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)cnx * cny) return;
+    const int i = (int)(k % cnx), j = (int)(k / cnx);
+    const int64_t f = (int64_t)(fy0 + 2 * j) * fnx + fx0 + 2 * i;
+    const int64_t c = (int64_t)(y0 + j) * ccnx + x0 + i;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const float* a = fine[q];
+        coarse[q][c] = 0.25f * ((a[f] + a[f + 1]) + (a[f + fnx] + a[f + fnx + 1]));
+    }
+}
+
+// Fine patch cell (fi, fj) = coarse cell (x0 + fi/2, y0 + fj/2), the coarse index clamped into its grid.
+__global__ void k_swe_prolong(const float* const* coarse, int ccnx, int ccny, int x0, int y0, float* const* fine, int fnx,
+                              int fny) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)fnx * fny) return;
+    const int fi = (int)(k % fnx), fj = (int)(k / fnx);
+    const int ci = min(max(x0 + fi / 2, 0), ccnx - 1), cj = min(max(y0 + fj / 2, 0), ccny - 1);
+    const int64_t c = (int64_t)cj * ccnx + ci;
+#pragma unroll
+    for (int q = 0; q < 3; q++) fine[q][k] = coarse[q][c];
+}
+
 __global__ void __launch_bounds__(256) k_swe_diag(const float* h, const float* hu, const float* hv, int64_t n,
                                                   double g, double dry, DiagPart* parts) {
     DiagPart p{0.0, INFINITY, 0.0, 0.0, 0.0, 0.0, 0, 0, 0};
@@ -712,6 +756,95 @@ void vf_swe_destroy(vf_swe* h) {
     for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status, &h->diag}) b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
+}
+
+
+// ------------------------------------------------------------------ the state on the device
+
+int32_t vf_swe_state(vf_swe* h, float** hcell, float** hu, float** hv) {
+    VF_REQUIRE(h && hcell && hu && hv, VF_EINVAL, "null argument");
+    const int s = (int)(h->dispatched % 2);
+    *hcell = field(h, s, 0);
+    *hu = field(h, s, 1);
+    *hv = field(h, s, 2);
+    return VF_OK;
+}
+
+int32_t vf_swe_measure_speed(vf_swe* h) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    const int s = (int)(h->dispatched % 2);
+    int* slot = speed_slot(h, (int)(h->dispatched % 3));
+    VF_TRY_CUDA(cudaMemsetAsync(slot, 0, 4, h->stream));
+    VF_LAUNCH(h->prof, "k_swe_speed", h->stream, k_swe_speed, std::max(1, std::min(div_up(h->cells, 256), sm_count() * 8)), 256,
+              0, field(h, s, 0), field(h, s, 1), field(h, s, 2), h->cells, params_ptr(h), slot);
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
+namespace {
+
+// The three current fields of a handle as a device array of pointers (a small upload on the handle's stream).
+struct FieldPtrs {
+    DeviceBuffer buf;
+    int32_t make(vf_swe* h) {
+        const int s = (int)(h->dispatched % 2);
+        float* p[3] = {field(h, s, 0), field(h, s, 1), field(h, s, 2)};
+        int32_t rc = buf.alloc(sizeof p);
+        if (rc) return rc;
+        VF_TRY_CUDA(cudaMemcpyAsync(buf.ptr, p, sizeof p, cudaMemcpyHostToDevice, h->stream));
+        return VF_OK;
+    }
+};
+
+}  // namespace
+
+int32_t vf_swe_restrict(vf_swe* fine, vf_swe* coarse) {
+    VF_REQUIRE(fine && coarse, VF_EINVAL, "null handle");
+    VF_REQUIRE(fine->nx == 2 * coarse->nx && fine->ny == 2 * coarse->ny, VF_EINVAL,
+               "a %d x %d grid restricts to %d x %d, not %d x %d", fine->nx, fine->ny, fine->nx / 2, fine->ny / 2,
+               coarse->nx, coarse->ny);
+    VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
+    FieldPtrs f, c;
+    int32_t rc;
+    if ((rc = f.make(fine)) || (rc = c.make(coarse))) return rc;
+    VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
+    VF_LAUNCH(coarse->prof, "k_swe_restrict", coarse->stream, k_swe_restrict, div_up(coarse->cells, 256), 256, 0,
+              f.buf.as<const float*>(), fine->nx, 0, 0, c.buf.as<float*>(), coarse->nx, 0, 0, coarse->nx, coarse->ny);
+    VF_TRY_CUDA(cudaStreamSynchronize(coarse->stream));
+    return vf_swe_measure_speed(coarse);
+}
+
+int32_t vf_swe_prolong(vf_swe* coarse, int32_t x0, int32_t y0, vf_swe* fine) {
+    VF_REQUIRE(fine && coarse, VF_EINVAL, "null handle");
+    VF_REQUIRE(fine->nx % 2 == 0 && fine->ny % 2 == 0, VF_EINVAL, "a patch of even size, got %d x %d", fine->nx, fine->ny);
+    VF_TRY_CUDA(cudaStreamSynchronize(coarse->stream));
+    FieldPtrs f, c;
+    int32_t rc;
+    if ((rc = f.make(fine)) || (rc = c.make(coarse))) return rc;
+    VF_TRY_CUDA(cudaStreamSynchronize(coarse->stream));
+    VF_LAUNCH(fine->prof, "k_swe_prolong", fine->stream, k_swe_prolong, div_up(fine->cells, 256), 256, 0,
+              c.buf.as<const float*>(), coarse->nx, coarse->ny, x0, y0, f.buf.as<float*>(), fine->nx, fine->ny);
+    VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
+    return vf_swe_measure_speed(fine);
+}
+
+int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t margin, vf_swe* coarse, int32_t x0, int32_t y0) {
+    VF_REQUIRE(fine && coarse, VF_EINVAL, "null handle");
+    VF_REQUIRE(margin >= 0 && margin % 2 == 0 && 2 * margin < fine->nx && 2 * margin < fine->ny, VF_EINVAL,
+               "an even margin inside the patch, got %d", margin);
+    const int cnx = (fine->nx - 2 * margin) / 2, cny = (fine->ny - 2 * margin) / 2;
+    const int cx0 = x0 + margin / 2, cy0 = y0 + margin / 2;
+    VF_REQUIRE(cx0 >= 0 && cy0 >= 0 && cx0 + cnx <= coarse->nx && cy0 + cny <= coarse->ny, VF_EINVAL,
+               "the patch's interior [%d, %d) x [%d, %d) leaves the coarse grid", cx0, cx0 + cnx, cy0, cy0 + cny);
+    VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
+    FieldPtrs f, c;
+    int32_t rc;
+    if ((rc = f.make(fine)) || (rc = c.make(coarse))) return rc;
+    VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
+    VF_LAUNCH(coarse->prof, "k_swe_restrict", coarse->stream, k_swe_restrict, div_up((int64_t)cnx * cny, 256), 256, 0,
+              f.buf.as<const float*>(), fine->nx, margin, margin, c.buf.as<float*>(), coarse->nx, cx0, cy0, cnx, cny);
+    VF_TRY_CUDA(cudaStreamSynchronize(coarse->stream));
+    return VF_OK;
 }
 
 }  // extern "C"
