@@ -312,9 +312,15 @@ int32_t vf_swe_restrict(vf_swe* fine, vf_swe* coarse);
 /* The inverse for a patch: the coarse cells [x0, x0 + nx/2) x [y0, y0 + ny/2) of `coarse`, each copied to its 2x2
  * fine cells of `fine` (a patch of nx x ny cells), and the fine wave speed measured. */
 int32_t vf_swe_prolong(vf_swe* coarse, int32_t x0, int32_t y0, vf_swe* fine);
-/* The fine patch's interior [m, nx - m) x [m, ny - m) (m even) averaged back into the coarse cells it covers
- * (patch cell (m, m) lies over coarse cell (x0 + m/2, y0 + m/2)). */
-int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t margin, vf_swe* coarse, int32_t x0, int32_t y0);
+/* nx x ny coarse cells from (x0, y0) of `coarse` = the means of the fine patch's 2x2 blocks from fine cell
+ * (fx0, fy0). */
+int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t fx0, int32_t fy0, vf_swe* coarse, int32_t x0, int32_t y0,
+                              int32_t nx, int32_t ny);
+/* dst's current state = src's (same grid), on the device; dst's wave speed measured. */
+int32_t vf_swe_copy_state(vf_swe* dst, vf_swe* src);
+/* Per tile of tile x tile cells (row-major, ntiles = ceil(nx/tile) * ceil(ny/tile)): the largest relative depth
+ * jump between neighbouring cells, (|dh east| + |dh north|) / max(h, dry), of the current state. */
+int32_t vf_swe_jump_indicator(vf_swe* h, int32_t tile, float* out, int32_t ntiles);
 
 /* ------------------------------------------------------------------ the flux-correction network */
 /* A 3-layer 5x5 convolutional network (3 -> 32 -> 32 -> 6 channels, ReLU between; bf16 weights and activations,
@@ -343,8 +349,15 @@ int32_t vf_cnn_loss(vf_cnn* h, const int32_t* slots, int32_t n, double* loss, do
 int32_t vf_cnn_gradients(vf_cnn* h, const int32_t* slots, int32_t n, float* grads, double* loss);
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss over samples; *loss is the loss before it. */
 int32_t vf_cnn_train(vf_cnn* h, const int32_t* slots, int32_t n, float lr, double* loss);
-/* The correction of a state in place (device planes of the network's grid, e.g. from vf_swe_state). */
-int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv);
+/* The correction: predict from the state at an interval's start (the network's S), apply to the plain solver's
+ * state at its end (P); both device planes of the network's grid, e.g. from vf_swe_state. `stream` (a
+ * cudaStream_t, e.g. vf_swe_stream) is the stream that produces and consumes the state: the network's work is
+ * ordered after that stream's work so far and that stream's later work after the network's, with no host wait;
+ * NULL waits on the host instead. vf_cnn_apply without a prediction since the last apply is VF_ESTATE.
+ * vf_cnn_correct predicts and applies on one state. */
+int32_t vf_cnn_predict(vf_cnn* h, const float* hcell, const float* hu, const float* hv, void* stream);
+int32_t vf_cnn_apply(vf_cnn* h, float* hcell, float* hu, float* hv, void* stream);
+int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv, void* stream);
 /* The network's output for sample slot's S: nx*ny*8 floats (six used per cell, the east face's h, hu, hv then the
  * north face's). */
 int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out);

@@ -166,7 +166,9 @@ def lib() -> ctypes.CDLL:
         "vf_swe_measure_speed": ([_vp], ctypes.c_int32),
         "vf_swe_restrict": ([_vp, _vp], ctypes.c_int32),
         "vf_swe_prolong": ([_vp, ctypes.c_int32, ctypes.c_int32, _vp], ctypes.c_int32),
-        "vf_swe_restrict_patch": ([_vp, ctypes.c_int32, _vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_restrict_patch": ([_vp, ctypes.c_int32, ctypes.c_int32, _vp] + [ctypes.c_int32] * 4, ctypes.c_int32),
+        "vf_swe_copy_state": ([_vp, _vp], ctypes.c_int32),
+        "vf_swe_jump_indicator": ([_vp, ctypes.c_int32, _f32p, ctypes.c_int32], ctypes.c_int32),
         "vf_cnn_param_count": ([], ctypes.c_int64),
         "vf_cnn_create": ([ctypes.c_int32] * 4 + [ctypes.c_float, ctypes.c_float, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_cnn_params": ([_vp, _f32p, ctypes.c_int64, ctypes.c_int32], ctypes.c_int32),
@@ -175,7 +177,9 @@ def lib() -> ctypes.CDLL:
                         ctypes.c_int32),
         "vf_cnn_gradients": ([_vp, _i32p, ctypes.c_int32, _f32p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
         "vf_cnn_train": ([_vp, _i32p, ctypes.c_int32, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
-        "vf_cnn_correct": ([_vp, _vp, _vp, _vp], ctypes.c_int32),
+        "vf_cnn_correct": ([_vp] * 5, ctypes.c_int32),
+        "vf_cnn_predict": ([_vp] * 5, ctypes.c_int32),
+        "vf_cnn_apply": ([_vp] * 5, ctypes.c_int32),
         "vf_cnn_fluxes": ([_vp, ctypes.c_int32, _f32p], ctypes.c_int32),
         "vf_cnn_stream": ([_vp], _vp),
         "vf_cnn_profile": ([_vp, ctypes.c_int32], ctypes.c_int32),
@@ -593,6 +597,7 @@ class FluxNet:
         check(lib().vf_cnn_create(nx, ny, batch, samples, s_flux, s_res, ctypes.byref(h)))
         self._h = h
         self.nx, self.ny, self.s_flux, self.s_res = nx, ny, s_flux, s_res
+        self.batch, self.samples = batch, samples
 
     @staticmethod
     def count() -> int:
@@ -648,8 +653,18 @@ class FluxNet:
         return out.reshape(self.ny, self.nx, 8)
 
     def correct(self, sim: "PatchSimulation") -> None:
-        """The correction of a PatchSimulation's current state in place, and its wave speed measured again."""
-        check(lib().vf_cnn_correct(self._h, *sim.device_state()))
+        """The correction predicted from a PatchSimulation's current state and applied to it in place, and its
+        wave speed measured again."""
+        check(lib().vf_cnn_correct(self._h, *sim.device_state(), sim.stream()))
+        check(lib().vf_swe_measure_speed(sim._h))
+
+    def predict(self, sim: "PatchSimulation") -> None:
+        """The correction predicted from the current state (an interval's start)."""
+        check(lib().vf_cnn_predict(self._h, *sim.device_state(), sim.stream()))
+
+    def apply(self, sim: "PatchSimulation") -> None:
+        """The last prediction applied to the current state (the interval's end), its wave speed measured again."""
+        check(lib().vf_cnn_apply(self._h, *sim.device_state(), sim.stream()))
         check(lib().vf_swe_measure_speed(sim._h))
 
     def profile(self, on: bool) -> None:
@@ -939,9 +954,19 @@ class PatchSimulation:
         """This patch's cells copied from coarse cells from (x0, y0) on, each to its 2x2 fine cells."""
         check(lib().vf_swe_prolong(coarse._h, x0, y0, self._h))
 
-    def restrict_into(self, margin: int, coarse: "PatchSimulation", x0: int, y0: int) -> None:
-        """This patch's interior (margin cells in from each side) averaged back into the coarse cells it covers."""
-        check(lib().vf_swe_restrict_patch(self._h, margin, coarse._h, x0, y0))
+    def restrict_into(self, fx0: int, fy0: int, coarse: "PatchSimulation", x0: int, y0: int, nx: int, ny: int) -> None:
+        """nx x ny coarse cells from (x0, y0) = this patch's 2x2 means from its cell (fx0, fy0)."""
+        check(lib().vf_swe_restrict_patch(self._h, fx0, fy0, coarse._h, x0, y0, nx, ny))
+
+    def copy_from(self, other: "PatchSimulation") -> None:
+        check(lib().vf_swe_copy_state(self._h, other._h))
+
+    def jump_indicator(self, tile: int) -> np.ndarray:
+        """Per tile (rows of tiles from the south-west): the largest relative depth jump between neighbours."""
+        tx, ty = -(-self._nx // tile), -(-self._ny // tile)
+        out = np.empty(tx * ty, np.float32)
+        check(lib().vf_swe_jump_indicator(self._h, tile, _fp(out), len(out)))
+        return out.reshape(ty, tx)
 
     def advance(self, ticks_: int, max_steps: int) -> Advance:
         steps = ctypes.c_int32()

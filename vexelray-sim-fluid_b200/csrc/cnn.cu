@@ -166,7 +166,10 @@ struct vf_cnn {
     DeviceBuffer w1, w2, w3, t2, t3;
     DeviceBuffer x0, a1, a2, y3, dy3, dy2, dy1, resid, loss;
     DeviceBuffer samples;   // cap x {state, plain, target} x 3 fields x cells floats
+    DeviceBuffer state;     // the state a prediction reads, 3 planes
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t adam_steps = 0;
+    bool predicted = false;   // y3 holds a prediction not yet applied
     int grid_conv[5] = {0}, grid_wgrad[3] = {0};
     Profiler prof;
 };
@@ -302,8 +305,13 @@ int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, fl
         (rc = h->x0.alloc(bc * 8 * 2)) || (rc = h->a1.alloc(bc * 32 * 2)) || (rc = h->a2.alloc(bc * 32 * 2)) ||
         (rc = h->y3.alloc(bc * 8 * 4)) || (rc = h->dy3.alloc(bc * 8 * 2)) || (rc = h->dy2.alloc(bc * 32 * 2)) ||
         (rc = h->dy1.alloc(bc * 32 * 2)) || (rc = h->resid.alloc(bc * 3 * 4)) || (rc = h->loss.alloc(16)) ||
-        (rc = h->samples.alloc((size_t)samples * 9 * h->cells * 4)))
+        (rc = h->samples.alloc((size_t)samples * 9 * h->cells * 4)) || (rc = h->state.alloc((size_t)3 * h->cells * 4)))
         return fail(rc);
+    if (cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+        set_error("cudaEventCreate failed");
+        return fail(VF_ECUDA);
+    }
     const int modes[5][3] = {{8, 32, CONV_RELU}, {32, 32, CONV_RELU}, {32, 8, CONV_LINEAR}, {8, 32, CONV_GRAD_MASK},
                              {32, 32, CONV_GRAD_MASK}};
     const int wg[3][2] = {{8, 32}, {32, 32}, {32, 8}};
@@ -407,19 +415,57 @@ int32_t vf_cnn_train(vf_cnn* h, const int32_t* slots, int32_t n, float lr, doubl
     return VF_OK;
 }
 
-int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv) {
+namespace {
+
+// Orders the network's stream after `stream`'s work so far (no host wait).
+int32_t follow(vf_cnn* h, cudaStream_t stream) {
+    if (!stream) return VF_OK;
+    VF_TRY_CUDA(cudaEventRecord(h->ev_in, stream));
+    VF_TRY_CUDA(cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+    return VF_OK;
+}
+
+// Orders `stream` after the network's work so far; without a stream, waits on the host.
+int32_t handback(vf_cnn* h, cudaStream_t stream) {
+    if (!stream) {
+        VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+        return VF_OK;
+    }
+    VF_TRY_CUDA(cudaEventRecord(h->ev_out, h->stream));
+    VF_TRY_CUDA(cudaStreamWaitEvent(stream, h->ev_out, 0));
+    return VF_OK;
+}
+
+}  // namespace
+
+int32_t vf_cnn_predict(vf_cnn* h, const float* hcell, const float* hu, const float* hv, void* stream) {
     VF_REQUIRE(h && hcell && hu && hv, VF_EINVAL, "null argument");
-    float* s = h->resid.as<float>();   // the state copied into one contiguous 3-plane block for the features
+    int32_t rc = follow(h, (cudaStream_t)stream);
+    if (rc) return rc;
+    float* s = h->state.as<float>();   // the state copied into one contiguous 3-plane block for the features
     for (int f = 0; f < 3; f++)
         VF_TRY_CUDA(cudaMemcpyAsync(s + f * h->cells, f == 0 ? hcell : f == 1 ? hu : hv, (size_t)h->cells * 4,
                                     cudaMemcpyDeviceToDevice, h->stream));
     const float* st[1] = {s};
-    int32_t rc = forward(h, st, 1);
+    if ((rc = forward(h, st, 1))) return rc;
+    h->predicted = true;
+    return handback(h, (cudaStream_t)stream);
+}
+
+int32_t vf_cnn_apply(vf_cnn* h, float* hcell, float* hu, float* hv, void* stream) {
+    VF_REQUIRE(h && hcell && hu && hv, VF_EINVAL, "null argument");
+    VF_REQUIRE(h->predicted, VF_ESTATE, "no prediction to apply");
+    int32_t rc = follow(h, (cudaStream_t)stream);
     if (rc) return rc;
     VF_LAUNCH(h->prof, "k_apply_flux", h->stream, k_apply_flux, div_up(h->cells, EW_THREADS), EW_THREADS, 0, hcell, hu,
               hv, h->y3.as<float>(), h->nx, h->ny, h->s_flux);
-    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
-    return VF_OK;
+    h->predicted = false;
+    return handback(h, (cudaStream_t)stream);
+}
+
+int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv, void* stream) {
+    int32_t rc = vf_cnn_predict(h, hcell, hu, hv, stream);
+    return rc ? rc : vf_cnn_apply(h, hcell, hu, hv, stream);
 }
 
 int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out) {
@@ -454,8 +500,11 @@ void vf_cnn_destroy(vf_cnn* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DeviceBuffer* b : {&h->params, &h->grads, &h->adam_m, &h->adam_v, &h->w1, &h->w2, &h->w3, &h->t2, &h->t3, &h->x0,
-                            &h->a1, &h->a2, &h->y3, &h->dy3, &h->dy2, &h->dy1, &h->resid, &h->loss, &h->samples})
+                            &h->a1, &h->a2, &h->y3, &h->dy3, &h->dy2, &h->dy1, &h->resid, &h->loss, &h->samples,
+                            &h->state})
         b->release();
+    if (h->ev_in) cudaEventDestroy(h->ev_in);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

@@ -336,6 +336,19 @@ __global__ void k_swe_prolong(const float* const* coarse, int ccnx, int ccny, in
     for (int q = 0; q < 3; q++) fine[q][k] = coarse[q][c];
 }
 
+// Per tile of t x t cells: the largest relative depth jump to the east or north neighbour,
+// (|h(i+1,j) - h(i,j)| + |h(i,j+1) - h(i,j)|) / max(h(i,j), dry), as float bits (atomicMax).
+__global__ void k_swe_jump(const float* h, int nx, int ny, int t, int tiles_x, float dry, int* out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)nx * ny) return;
+    const int i = (int)(k % nx), j = (int)(k / nx);
+    const float d = h[k];
+    const float ex = i < nx - 1 ? fabsf(h[k + 1] - d) : 0.0f;
+    const float ny_ = j < ny - 1 ? fabsf(h[k + nx] - d) : 0.0f;
+    const float jump = (ex + ny_) / fmaxf(d, dry);
+    atomicMax(&out[(j / t) * tiles_x + i / t], __float_as_int(jump));
+}
+
 __global__ void __launch_bounds__(256) k_swe_diag(const float* h, const float* hu, const float* hv, int64_t n,
                                                   double g, double dry, DiagPart* parts) {
     DiagPart p{0.0, INFINITY, 0.0, 0.0, 0.0, 0.0, 0, 0, 0};
@@ -777,8 +790,7 @@ int32_t vf_swe_measure_speed(vf_swe* h) {
     VF_TRY_CUDA(cudaMemsetAsync(slot, 0, 4, h->stream));
     VF_LAUNCH(h->prof, "k_swe_speed", h->stream, k_swe_speed, std::max(1, std::min(div_up(h->cells, 256), sm_count() * 8)), 256,
               0, field(h, s, 0), field(h, s, 1), field(h, s, 2), h->cells, params_ptr(h), slot);
-    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
-    return VF_OK;
+    return VF_OK;   // the next dispatch, on the same stream, reads the word
 }
 
 namespace {
@@ -828,22 +840,50 @@ int32_t vf_swe_prolong(vf_swe* coarse, int32_t x0, int32_t y0, vf_swe* fine) {
     return vf_swe_measure_speed(fine);
 }
 
-int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t margin, vf_swe* coarse, int32_t x0, int32_t y0) {
+int32_t vf_swe_restrict_patch(vf_swe* fine, int32_t fx0, int32_t fy0, vf_swe* coarse, int32_t x0, int32_t y0,
+                              int32_t nx, int32_t ny) {
     VF_REQUIRE(fine && coarse, VF_EINVAL, "null handle");
-    VF_REQUIRE(margin >= 0 && margin % 2 == 0 && 2 * margin < fine->nx && 2 * margin < fine->ny, VF_EINVAL,
-               "an even margin inside the patch, got %d", margin);
-    const int cnx = (fine->nx - 2 * margin) / 2, cny = (fine->ny - 2 * margin) / 2;
-    const int cx0 = x0 + margin / 2, cy0 = y0 + margin / 2;
-    VF_REQUIRE(cx0 >= 0 && cy0 >= 0 && cx0 + cnx <= coarse->nx && cy0 + cny <= coarse->ny, VF_EINVAL,
-               "the patch's interior [%d, %d) x [%d, %d) leaves the coarse grid", cx0, cx0 + cnx, cy0, cy0 + cny);
+    VF_REQUIRE(nx >= 1 && ny >= 1 && fx0 >= 0 && fy0 >= 0 && fx0 + 2 * nx <= fine->nx && fy0 + 2 * ny <= fine->ny,
+               VF_EINVAL, "%d x %d coarse cells from fine cell (%d, %d) leave the %d x %d patch", nx, ny, fx0, fy0,
+               fine->nx, fine->ny);
+    VF_REQUIRE(x0 >= 0 && y0 >= 0 && x0 + nx <= coarse->nx && y0 + ny <= coarse->ny, VF_EINVAL,
+               "coarse cells [%d, %d) x [%d, %d) leave the %d x %d grid", x0, x0 + nx, y0, y0 + ny, coarse->nx, coarse->ny);
     VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
     FieldPtrs f, c;
     int32_t rc;
     if ((rc = f.make(fine)) || (rc = c.make(coarse))) return rc;
     VF_TRY_CUDA(cudaStreamSynchronize(fine->stream));
-    VF_LAUNCH(coarse->prof, "k_swe_restrict", coarse->stream, k_swe_restrict, div_up((int64_t)cnx * cny, 256), 256, 0,
-              f.buf.as<const float*>(), fine->nx, margin, margin, c.buf.as<float*>(), coarse->nx, cx0, cy0, cnx, cny);
+    VF_LAUNCH(coarse->prof, "k_swe_restrict", coarse->stream, k_swe_restrict, div_up((int64_t)nx * ny, 256), 256, 0,
+              f.buf.as<const float*>(), fine->nx, fx0, fy0, c.buf.as<float*>(), coarse->nx, x0, y0, nx, ny);
     VF_TRY_CUDA(cudaStreamSynchronize(coarse->stream));
+    return VF_OK;
+}
+
+int32_t vf_swe_copy_state(vf_swe* dst, vf_swe* src) {
+    VF_REQUIRE(dst && src, VF_EINVAL, "null handle");
+    VF_REQUIRE(dst->nx == src->nx && dst->ny == src->ny, VF_EINVAL, "grids differ: %d x %d and %d x %d", dst->nx,
+               dst->ny, src->nx, src->ny);
+    VF_TRY_CUDA(cudaStreamSynchronize(src->stream));
+    const int sd = (int)(dst->dispatched % 2), ss = (int)(src->dispatched % 2);
+    for (int f = 0; f < 3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(field(dst, sd, f), field(src, ss, f), (size_t)src->cells * 4, cudaMemcpyDeviceToDevice,
+                                    dst->stream));
+    return vf_swe_measure_speed(dst);
+}
+
+int32_t vf_swe_jump_indicator(vf_swe* h, int32_t tile, float* out, int32_t ntiles) {
+    VF_REQUIRE(h && out && tile >= 1, VF_EINVAL, "null argument or tile < 1");
+    const int tx = (h->nx + tile - 1) / tile, ty = (h->ny + tile - 1) / tile;
+    VF_REQUIRE(ntiles == tx * ty, VF_EINVAL, "%d tiles of %d cells cover the grid, got %d", tx * ty, tile, ntiles);
+    DeviceBuffer d;
+    int32_t rc = d.alloc((size_t)ntiles * 4);
+    if (rc) return rc;
+    VF_TRY_CUDA(cudaMemsetAsync(d.ptr, 0, (size_t)ntiles * 4, h->stream));
+    const int s = (int)(h->dispatched % 2);
+    VF_LAUNCH(h->prof, "k_swe_jump", h->stream, k_swe_jump, div_up(h->cells, 256), 256, 0, field(h, s, 0), h->nx, h->ny,
+              tile, tx, h->host_params[4], d.as<int>());
+    VF_TRY_CUDA(cudaMemcpyAsync(out, d.ptr, (size_t)ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     return VF_OK;
 }
 
