@@ -215,6 +215,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_tensor_peak():
+    """Dense bf16 TFLOP/s: the burst figure (a kernel timed alone) and its kind."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 def profiled_traffic(kernel: str):
     """dram bytes per launch of a kernel from the committed ncu summary, scaled to this workload, or None."""
     p = ROOT / "profiles" / "traffic.json"
@@ -424,6 +432,7 @@ def run_ours(args, dist: Dist):
                             "kernel": "k_swe_tile", "bytes_per_cell": 24}}
 
     batch = None if args.no_batch else run_batch(args, vf, dist, peak)
+    learned = None if args.no_learned else run_learned(args, vf)
 
     if dist.rank != 0:
         return
@@ -449,9 +458,65 @@ def run_ours(args, dist: Dist):
         "clocks": clocks.summary(),
         "swe": swe,
         "batch": batch,
+        "learned": learned,
         "p2g_variants": variants,
     }
     print(json.dumps(line), flush=True)
+
+
+CNN_FLOPS_PER_CELL = 2 * 25 * (3 * 32 + 32 * 32 + 32 * 6)   # 65.6 kFLOP: the three convolutions, algorithmic
+
+
+def run_learned(args, vf):
+    """The learned coarse shallow-water configuration: the committed network (trained at 2048^2 on held-in seeds)
+    against the plain fine solver and the plain coarse solver on held-out seeds, 2000 fine steps each."""
+    from vexfluid import learned as L
+    net, report = L.trained()
+    seeds = list(range(1, 1 + args.learned_seeds))
+    rows = []
+    try:
+        for seed in seeds:
+            plain = L.evaluate(None, report["fine"], seed, 2000, report["interval_ticks"])
+            lrn = L.evaluate(net, report["fine"], seed, 2000, report["interval_ticks"])
+            rows.append((plain, lrn))
+        # the network's kernels, timed alone over a few corrections of the coarse grid
+        with vf.PatchSimulation(report["coarse"], report["coarse"]) as c:
+            h0 = L.restrict(L.bumps(3, report["fine"]))
+            z = np.zeros_like(h0)
+            c.load(h0.ravel(), z.ravel(), z.ravel(), L.coarse_params())
+            net.correct(c)
+            net.profile(True)
+            for _ in range(10):
+                net.correct(c)
+            prof = net.profile_read()
+            net.profile(False)
+    finally:
+        net.close()
+    conv_ms = sum(prof[k][0] / prof[k][1] for k in ("k_conv1", "k_conv2", "k_conv3"))
+    cells = report["coarse"] ** 2
+    tflops = CNN_FLOPS_PER_CELL * cells / (conv_ms / 1e3) / 1e12
+    tpeak, tkind = measured_tensor_peak()
+    mean = lambda key, k: float(np.mean([r[k][key] for r in rows]))
+    return {
+        "workload": (f"learned coarse shallow water: fine {report['fine']}^2 HLL (16 bumps, the 4096^2 distribution "
+                     f"halved in sigma and centres), coarse {report['coarse']}^2, correction every "
+                     f"{report['interval_coarse_steps']} coarse steps ({report['interval_ticks']} ticks), "
+                     f"held-out seeds {seeds}, 2000 fine steps each"),
+        "fine_cell_updates_per_s": mean("fine_cell_updates_per_s", 1),
+        "learned_equivalent_cell_updates_per_s": mean("equivalent_fine_cell_updates_per_s", 1),
+        "speedup_vs_fine": mean("speedup", 1),
+        "plain_coarse_speedup_vs_fine": mean("speedup", 0),
+        "h_rms_error": {"learned": mean("h_rms_error", 1), "plain_coarse": mean("h_rms_error", 0),
+                        "learned_max": float(max(r[1]["h_rms_error"] for r in rows))},
+        "per_seed": [{"seed": r[0]["seed"], "plain_err": r[0]["h_rms_error"], "learned_err": r[1]["h_rms_error"],
+                      "speedup": r[1]["speedup"]} for r in rows],
+        "network_kernels_us": {k: 1e3 * v[0] / v[1] for k, v in prof.items()},
+        "roofline": {"bound": "tensor", "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
+                     "peak_kind": tkind, "traffic": None, "kernel": "k_conv1 + k_conv2 + k_conv3 (mma.sync bf16)",
+                     "flops_per_cell": CNN_FLOPS_PER_CELL},
+        "training": {"seeds": report["train_seeds"], "pairs_per_seed": report["pairs_per_seed"],
+                     "adam_steps": report["adam_steps"], "train_seconds": report["train_seconds"]},
+    }
 
 
 def cpu_batch_rate(scenes, x, y, m, budget_s=10.0):
@@ -554,6 +619,8 @@ def main():
     ap.add_argument("--no-variants", action="store_true", help="skip the comparison of the three P2G schedules")
     ap.add_argument("--variant-steps", type=int, default=20)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes sub-measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned shallow-water sub-measurement")
+    ap.add_argument("--learned-seeds", type=int, default=4)
     ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
                     help="the batched step's autotune cache (JSON)")
     args = ap.parse_args()

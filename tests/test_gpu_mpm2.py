@@ -178,3 +178,44 @@ def test_fixed_scatter_is_bit_exact_against_the_oracle(jittered64):
                                  ip(e[1]), ip(e[2]))
         for f in range(3):
             assert np.array_equal(g[f], e[f])
+
+
+def c0_dam_break(seed=0):
+    """The 2D configuration: 128^2 nodes (dx = 1/128), 4 particles per cell jittered in every cell whose centre lies
+    in [0.05,0.55] x [0.05,0.30] (2048 cells: 8192 particles), still, m = 1/4 (rho0 = 1 per cell)."""
+    n = 128
+    rng = np.random.default_rng(seed)
+    cx = np.arange(math.ceil(0.05 * n - 0.5), math.ceil(0.55 * n - 0.5), dtype=np.float32)
+    cy = np.arange(math.ceil(0.05 * n - 0.5), math.ceil(0.30 * n - 0.5), dtype=np.float32)
+    gy, gx = np.meshgrid(cy, cx, indexing="ij")
+    cells = np.repeat(np.stack([gx.ravel(), gy.ravel()], 1), 4, axis=0)
+    pos = (cells + rng.random(cells.shape, dtype=np.float32) * np.float32(0.999)).astype(np.float32)
+    return n, np.ascontiguousarray(pos[:, 0]), np.ascontiguousarray(pos[:, 1]), np.full(len(pos), 0.25, np.float32)
+
+
+def test_the_2d_configuration_matches_the_oracle():
+    """Config 0: Tait k = 50 (50 n^2 in node units), rho0 = 1, g = -9.8 (n nodes/s^2), dt = 1e-4, sticky walls 3
+    cells thick; sorted every 10 steps on both sides. One step's grid per node (1e-5), 100 steps' positions (1e-4),
+    masses unchanged."""
+    n, x, y, m = c0_dam_break()
+    assert len(x) == 8192
+    params = vf.flip_params(1e-4, 0, -9.8 * n, 50.0 * n * n, 1.0)
+    o = Flip2State(n, n, x, y, m)
+    with vf.ParticleSimulation(n, n, len(x), tait=True, sticky=3) as s:
+        s.load(x, y, np.zeros_like(x), np.zeros_like(x), m, params)
+        s.advance(1, 10)
+        o.sort()
+        o.step(params.view(F), (1, 3))
+        for key in ("gm", "gmu", "gmv"):
+            e = o.g[key].astype(np.float64)
+            assert np.all(np.abs(s.read(key) - e) <= 1e-5 * np.maximum(1, np.abs(e))), key
+        s.advance(99, 10)
+        for k in range(1, 100):
+            if k % 10 == 0:
+                o.sort()
+            o.step(params.view(F), (1, 3))
+        for key in ("x", "y"):
+            e = o.a[key]
+            got = s.read(key)
+            assert np.all(np.abs(got - e) <= 1e-4 * np.abs(e)), key
+        assert np.array_equal(s.read("m"), o.a["m"])
