@@ -362,6 +362,12 @@ int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv, void* stre
  * north face's). */
 int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out);
 void* vf_cnn_stream(vf_cnn* h);
+/* The forward and input-gradient convolutions' kernels: 0 (the default) mma.sync, 1 tcgen05.mma with operands in
+ * swizzled shared memory and accumulators in tensor memory. Both compute the same network (to fp32 summation
+ * order); at 32 channels the mma.sync kernels measured faster. The weight gradients always run on mma.sync. */
+int32_t vf_cnn_set_path(vf_cnn* h, int32_t path);
+/* Waits for the network's stream and reports a kernel's status bits (VF_ETIMEOUT for a bounded wait that expired). */
+int32_t vf_cnn_status(vf_cnn* h);
 int32_t vf_cnn_profile(vf_cnn* h, int32_t enable);
 int32_t vf_cnn_profile_read(vf_cnn* h, int32_t index, char* name, size_t cap, double* total_ms, int64_t* launches);
 int64_t vf_cnn_launches(const vf_cnn* h);

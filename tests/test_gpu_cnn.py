@@ -52,12 +52,17 @@ def blocks(g):
     return {k: np.asarray(v, np.float64) for k, v in d.items()}
 
 
-@pytest.mark.parametrize("ny,nx", [(21, 45), (40, 64)])
-def test_forward_matches_the_restatement(ny, nx):
+PATHS = [pytest.param(1, id="tcgen05"), pytest.param(0, id="mma_sync")]
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("ny,nx", [(21, 45), (40, 64), (33, 300)])
+def test_forward_matches_the_restatement(ny, nx, path):
     rng = np.random.default_rng(1)
     params = random_params(rng, scale3=1.0)
     S = state(rng, ny, nx)
     with vf.FluxNet(nx, ny) as net:
+        net.set_path(path)
         net.params(params)
         np.testing.assert_array_equal(net.params(), params)
         net.put(0, 0, *S)
@@ -67,7 +72,8 @@ def test_forward_matches_the_restatement(ny, nx):
     assert err <= 1e-2 * np.abs(want).max(), (err, np.abs(want).max())
 
 
-def test_gradients_match_the_restatement():
+@pytest.mark.parametrize("path", PATHS)
+def test_gradients_match_the_restatement(path):
     rng = np.random.default_rng(2)
     ny, nx = 24, 40
     params = random_params(rng)
@@ -79,6 +85,7 @@ def test_gradients_match_the_restatement():
         T = S + np.stack([smooth(rng, ny, nx, 2e-3) for _ in range(3)])
         samples.append((S, P.astype(np.float32), T.astype(np.float32)))
     with vf.FluxNet(nx, ny, batch=2, samples=2, s_flux=s_flux, s_res=s_res) as net:
+        net.set_path(path)
         net.params(params)
         for k, (S, P, T) in enumerate(samples):
             for kind, a in enumerate((S, P, T)):

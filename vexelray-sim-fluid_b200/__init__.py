@@ -182,6 +182,8 @@ def lib() -> ctypes.CDLL:
         "vf_cnn_apply": ([_vp] * 5, ctypes.c_int32),
         "vf_cnn_fluxes": ([_vp, ctypes.c_int32, _f32p], ctypes.c_int32),
         "vf_cnn_stream": ([_vp], _vp),
+        "vf_cnn_set_path": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_cnn_status": ([_vp], ctypes.c_int32),
         "vf_cnn_profile": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_cnn_profile_read": ([_vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
                                  _i64p], ctypes.c_int32),
@@ -666,6 +668,13 @@ class FluxNet:
         """The last prediction applied to the current state (the interval's end), its wave speed measured again."""
         check(lib().vf_cnn_apply(self._h, *sim.device_state(), sim.stream()))
         check(lib().vf_swe_measure_speed(sim._h))
+
+    def set_path(self, path: int) -> None:
+        """The convolutions' kernels: 0 mma.sync (default), 1 tcgen05."""
+        check(lib().vf_cnn_set_path(self._h, path))
+
+    def status(self) -> None:
+        check(lib().vf_cnn_status(self._h))
 
     def profile(self, on: bool) -> None:
         check(lib().vf_cnn_profile(self._h, 1 if on else 0))

@@ -170,7 +170,9 @@ struct vf_cnn {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t adam_steps = 0;
     bool predicted = false;   // y3 holds a prediction not yet applied
-    int grid_conv[5] = {0}, grid_wgrad[3] = {0};
+    int path = 0;             // the convolutions: 0 mma.sync (measured faster at 32 channels), 1 tcgen05
+    int grid_conv[5] = {0}, grid_wgrad[3] = {0}, grid_umma[5] = {0};
+    DeviceBuffer status;
     Profiler prof;
 };
 
@@ -186,13 +188,32 @@ int32_t pack(vf_cnn* h) {
     return VF_OK;
 }
 
+int conv_index(int cin, int cout, int mode) {
+    return mode == CONV_RELU ? (cin == 8 ? 0 : 1) : mode == CONV_LINEAR ? 2 : (cin == 8 ? 3 : 4);
+}
+
 int32_t conv(vf_cnn* h, const char* name, int cin, int cout, int mode, int grid, const bf16* in, const bf16* w,
              const float* bias, int bias_n, bf16* out_b, float* out_f, const bf16* mask, int nb) {
     ConvArgs a{in, w, bias, bias_n, out_b, out_f, mask, h->ny, h->nx, nb};
     h->prof.begin(name, h->stream);
-    cudaError_t e = launch_conv(cin, cout, mode, grid, a, h->stream);
+    cudaError_t e = h->path == 1
+                        ? launch_conv_umma(cin, cout, mode, h->grid_umma[conv_index(cin, cout, mode)], a,
+                                           h->status.as<uint32_t>(), h->stream)
+                        : launch_conv(cin, cout, mode, grid, a, h->stream);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
+    return VF_OK;
+}
+
+int32_t cnn_status(vf_cnn* h) {
+    uint32_t st = 0;
+    VF_TRY_CUDA(cudaMemcpyAsync(&st, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    if (st) {
+        VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+        set_error("a network kernel flagged device status 0x%x", st);
+        return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
+    }
     return VF_OK;
 }
 
@@ -263,7 +284,7 @@ int32_t forward_backward(vf_cnn* h, const int32_t* slots, int nb, double* loss_o
     }
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     if (loss_out) *loss_out = sum / (2.0 * 3.0 * (double)cells * nb);
-    return VF_OK;
+    return cnn_status(h);
 }
 
 }  // namespace
@@ -305,7 +326,8 @@ int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, fl
         (rc = h->x0.alloc(bc * 8 * 2)) || (rc = h->a1.alloc(bc * 32 * 2)) || (rc = h->a2.alloc(bc * 32 * 2)) ||
         (rc = h->y3.alloc(bc * 8 * 4)) || (rc = h->dy3.alloc(bc * 8 * 2)) || (rc = h->dy2.alloc(bc * 32 * 2)) ||
         (rc = h->dy1.alloc(bc * 32 * 2)) || (rc = h->resid.alloc(bc * 3 * 4)) || (rc = h->loss.alloc(16)) ||
-        (rc = h->samples.alloc((size_t)samples * 9 * h->cells * 4)) || (rc = h->state.alloc((size_t)3 * h->cells * 4)))
+        (rc = h->samples.alloc((size_t)samples * 9 * h->cells * 4)) || (rc = h->state.alloc((size_t)3 * h->cells * 4)) ||
+        (rc = h->status.alloc(16)))
         return fail(rc);
     if (cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {
@@ -327,7 +349,18 @@ int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, fl
         }
         (is_conv ? h->grid_conv[k] : h->grid_wgrad[k - 5]) = std::max(per, 1) * sm_count();
     }
-    for (DeviceBuffer* b : {&h->params, &h->grads, &h->adam_m, &h->adam_v, &h->samples})
+    for (int k = 0; k < 5; k++) {
+        const void* fn = conv_umma_kernel(modes[k][0], modes[k][1], modes[k][2]);
+        const size_t smem = conv_umma_smem_for(modes[k][0], modes[k][1]);
+        int per = 0;
+        if (!fn || cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 128, smem) != cudaSuccess) {
+            set_error("cannot give a tensor-core convolution %zu bytes of shared memory", smem);
+            return fail(VF_ECUDA);
+        }
+        h->grid_umma[k] = std::max(per, 1) * sm_count();
+    }
+    for (DeviceBuffer* b : {&h->params, &h->grads, &h->adam_m, &h->adam_v, &h->samples, &h->status})
         if (cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream) != cudaSuccess) return fail(VF_ECUDA);
     if (pack(h) || cudaStreamSynchronize(h->stream) != cudaSuccess) {
         set_error("initialising the network failed");
@@ -476,10 +509,22 @@ int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out) {
     if (rc) return rc;
     VF_TRY_CUDA(cudaMemcpyAsync(out, h->y3.ptr, (size_t)h->cells * 8 * 4, cudaMemcpyDeviceToHost, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
-    return VF_OK;
+    return cnn_status(h);
 }
 
 void* vf_cnn_stream(vf_cnn* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t vf_cnn_set_path(vf_cnn* h, int32_t path) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(path == 0 || path == 1, VF_EINVAL, "path 0 (mma.sync) or 1 (tcgen05), got %d", path);
+    h->path = path;
+    return VF_OK;
+}
+
+int32_t vf_cnn_status(vf_cnn* h) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    return cnn_status(h);
+}
 
 int32_t vf_cnn_profile(vf_cnn* h, int32_t enable) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
@@ -501,7 +546,7 @@ void vf_cnn_destroy(vf_cnn* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DeviceBuffer* b : {&h->params, &h->grads, &h->adam_m, &h->adam_v, &h->w1, &h->w2, &h->w3, &h->t2, &h->t3, &h->x0,
                             &h->a1, &h->a2, &h->y3, &h->dy3, &h->dy2, &h->dy1, &h->resid, &h->loss, &h->samples,
-                            &h->state})
+                            &h->state, &h->status})
         b->release();
     if (h->ev_in) cudaEventDestroy(h->ev_in);
     if (h->ev_out) cudaEventDestroy(h->ev_out);

@@ -69,4 +69,11 @@ cudaError_t launch_wgrad(int cin, int cout, int grid, const WgradArgs& a, cudaSt
 size_t conv_smem(int cin, int cout);
 size_t wgrad_smem(int cin, int cout);
 
+// The same convolutions on tcgen05 (cnn_umma.cu): 128 threads, conv_umma_smem_for bytes of dynamic shared memory,
+// a persistent grid; a bounded wait that expires sets ST_TIMEOUT in *status.
+const void* conv_umma_kernel(int cin, int cout, int mode);
+size_t conv_umma_smem_for(int cin, int cout);
+cudaError_t launch_conv_umma(int cin, int cout, int mode, int grid, const ConvArgs& a, uint32_t* status,
+                             cudaStream_t s);
+
 }  // namespace vf
