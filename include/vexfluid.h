@@ -290,6 +290,11 @@ int32_t vf_swe_dispatch(vf_swe* h, int32_t n);
 int64_t vf_swe_dispatched(const vf_swe* h);
 int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks);
 int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks);
+/* The step kernel's tile width: 64 or 32 cells (16 rows either way); 0 picks by grid size (32 when 64-wide tiles
+ * would give fewer than four per resident CTA slot, e.g. 1024^2). No counterpart in the reference: results are
+ * bit-identical for both widths, only the speed differs. */
+int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width);
+int32_t vf_swe_tile_width(const vf_swe* h);
 /* Diagnostics.of(h, hu, hv, g, dry, dt, dx, dy) over the current state (Diagnostics.java:43-81), reduced on the
  * device. out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
 int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]);
@@ -362,9 +367,10 @@ int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv, void* stre
  * north face's). */
 int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out);
 void* vf_cnn_stream(vf_cnn* h);
-/* The forward and input-gradient convolutions' kernels: 0 (the default) mma.sync, 1 tcgen05.mma with operands in
- * swizzled shared memory and accumulators in tensor memory. Both compute the same network (to fp32 summation
- * order); at 32 channels the mma.sync kernels measured faster. The weight gradients always run on mma.sync. */
+/* The forward and input-gradient convolutions' kernels: 0 (the default) mma.sync with each warp computing several
+ * output rows from every A fragment it loads (32 input channels), 1 tcgen05.mma with operands in swizzled shared
+ * memory and accumulators in tensor memory, 2 mma.sync with one output row per warp. All compute the same network
+ * (to fp32 summation order). The weight gradients always run on mma.sync. */
 int32_t vf_cnn_set_path(vf_cnn* h, int32_t path);
 /* Waits for the network's stream and reports a kernel's status bits (VF_ETIMEOUT for a bounded wait that expired). */
 int32_t vf_cnn_status(vf_cnn* h);

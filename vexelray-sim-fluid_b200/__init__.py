@@ -200,6 +200,8 @@ def lib() -> ctypes.CDLL:
         "vf_swe_steps": ([_vp], ctypes.c_int64),
         "vf_swe_dispatch": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_dispatched": ([_vp], ctypes.c_int64),
+        "vf_swe_set_tile_width": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_tile_width": ([_vp], ctypes.c_int32),
         "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_read_budget": ([_vp, ctypes.c_int32, _i32p], ctypes.c_int32),
         "vf_swe_diagnostics": ([_vp] + [ctypes.c_double] * 5 + [ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
@@ -670,7 +672,8 @@ class FluxNet:
         check(lib().vf_swe_measure_speed(sim._h))
 
     def set_path(self, path: int) -> None:
-        """The convolutions' kernels: 0 mma.sync (default), 1 tcgen05."""
+        """The convolutions' kernels: 0 mma.sync row-blocked (default), 1 tcgen05, 2 mma.sync one output row per
+        warp."""
         check(lib().vf_cnn_set_path(self._h, path))
 
     def status(self) -> None:
@@ -1020,6 +1023,13 @@ class PatchSimulation:
 
     def write_budget(self, slot: int, ticks_: int) -> None:
         check(lib().vf_swe_write_budget(self._h, slot, ticks_))
+
+    def set_tile_width(self, width: int) -> None:
+        """The step kernel's tile width, 32 or 64 cells; 0 chooses by grid size. Results do not depend on it."""
+        check(lib().vf_swe_set_tile_width(self._h, width))
+
+    def tile_width(self) -> int:
+        return int(lib().vf_swe_tile_width(self._h))
 
     def read_budget(self, slot: int) -> int:
         v = ctypes.c_int32()

@@ -170,8 +170,8 @@ struct vf_cnn {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t adam_steps = 0;
     bool predicted = false;   // y3 holds a prediction not yet applied
-    int path = 0;             // the convolutions: 0 mma.sync (measured faster at 32 channels), 1 tcgen05
-    int grid_conv[5] = {0}, grid_wgrad[3] = {0}, grid_umma[5] = {0};
+    int path = 0;             // the convolutions: 0 mma.sync row-blocked, 1 tcgen05, 2 mma.sync one row per warp
+    int grid_conv[2][5] = {{0}}, grid_wgrad[3] = {0}, grid_umma[5] = {0};
     DeviceBuffer status;
     Profiler prof;
 };
@@ -192,14 +192,15 @@ int conv_index(int cin, int cout, int mode) {
     return mode == CONV_RELU ? (cin == 8 ? 0 : 1) : mode == CONV_LINEAR ? 2 : (cin == 8 ? 3 : 4);
 }
 
-int32_t conv(vf_cnn* h, const char* name, int cin, int cout, int mode, int grid, const bf16* in, const bf16* w,
+int32_t conv(vf_cnn* h, const char* name, int cin, int cout, int mode, const bf16* in, const bf16* w,
              const float* bias, int bias_n, bf16* out_b, float* out_f, const bf16* mask, int nb) {
     ConvArgs a{in, w, bias, bias_n, out_b, out_f, mask, h->ny, h->nx, nb};
     h->prof.begin(name, h->stream);
-    cudaError_t e = h->path == 1
-                        ? launch_conv_umma(cin, cout, mode, h->grid_umma[conv_index(cin, cout, mode)], a,
-                                           h->status.as<uint32_t>(), h->stream)
-                        : launch_conv(cin, cout, mode, grid, a, h->stream);
+    const int k = conv_index(cin, cout, mode);
+    cudaError_t e = h->path == 1 ? launch_conv_umma(cin, cout, mode, h->grid_umma[k], a, h->status.as<uint32_t>(),
+                                                    h->stream)
+                    : h->path == 2 ? launch_conv(cin, cout, mode, false, h->grid_conv[1][k], a, h->stream)
+                                   : launch_conv(cin, cout, mode, true, h->grid_conv[0][k], a, h->stream);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
     return VF_OK;
@@ -235,11 +236,11 @@ int32_t forward(vf_cnn* h, const float* const* states, int nb) {
                   h->x0.as<bf16>() + b * cells * 8, cells);
     const float* P = h->params.as<float>();
     int32_t rc;
-    if ((rc = conv(h, "k_conv1", 8, 32, CONV_RELU, h->grid_conv[0], h->x0.as<bf16>(), h->w1.as<bf16>(), P + P_B1,
+    if ((rc = conv(h, "k_conv1", 8, 32, CONV_RELU, h->x0.as<bf16>(), h->w1.as<bf16>(), P + P_B1,
                    CNN_HID, h->a1.as<bf16>(), nullptr, nullptr, nb)) ||
-        (rc = conv(h, "k_conv2", 32, 32, CONV_RELU, h->grid_conv[1], h->a1.as<bf16>(), h->w2.as<bf16>(), P + P_B2,
+        (rc = conv(h, "k_conv2", 32, 32, CONV_RELU, h->a1.as<bf16>(), h->w2.as<bf16>(), P + P_B2,
                    CNN_HID, h->a2.as<bf16>(), nullptr, nullptr, nb)) ||
-        (rc = conv(h, "k_conv3", 32, 8, CONV_LINEAR, h->grid_conv[2], h->a2.as<bf16>(), h->w3.as<bf16>(), P + P_B3,
+        (rc = conv(h, "k_conv3", 32, 8, CONV_LINEAR, h->a2.as<bf16>(), h->w3.as<bf16>(), P + P_B3,
                    CNN_FLUXES, nullptr, h->y3.as<float>(), nullptr, nb)))
         return rc;
     return VF_OK;
@@ -272,11 +273,11 @@ int32_t forward_backward(vf_cnn* h, const int32_t* slots, int nb, double* loss_o
         VF_TRY_CUDA(cudaMemsetAsync(G, 0, h->grads.bytes, h->stream));
         if ((rc = wgrad(h, "k_wgrad3", 32, 8, h->grid_wgrad[2], h->a2.as<bf16>(), h->dy3.as<bf16>(), G + P_W3,
                         G + P_B3, CNN_HID, CNN_FLUXES, nb)) ||
-            (rc = conv(h, "k_dgrad3", 8, 32, CONV_GRAD_MASK, h->grid_conv[3], h->dy3.as<bf16>(), h->t3.as<bf16>(),
+            (rc = conv(h, "k_dgrad3", 8, 32, CONV_GRAD_MASK, h->dy3.as<bf16>(), h->t3.as<bf16>(),
                        nullptr, 0, h->dy2.as<bf16>(), nullptr, h->a2.as<bf16>(), nb)) ||
             (rc = wgrad(h, "k_wgrad2", 32, 32, h->grid_wgrad[1], h->a1.as<bf16>(), h->dy2.as<bf16>(), G + P_W2,
                         G + P_B2, CNN_HID, CNN_HID, nb)) ||
-            (rc = conv(h, "k_dgrad2", 32, 32, CONV_GRAD_MASK, h->grid_conv[4], h->dy2.as<bf16>(), h->t2.as<bf16>(),
+            (rc = conv(h, "k_dgrad2", 32, 32, CONV_GRAD_MASK, h->dy2.as<bf16>(), h->t2.as<bf16>(),
                        nullptr, 0, h->dy1.as<bf16>(), nullptr, h->a1.as<bf16>(), nb)) ||
             (rc = wgrad(h, "k_wgrad1", 8, 32, h->grid_wgrad[0], h->x0.as<bf16>(), h->dy1.as<bf16>(), G + P_W1,
                         G + P_B1, CNN_FEATURES, CNN_HID, nb)))
@@ -337,17 +338,20 @@ int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, fl
     const int modes[5][3] = {{8, 32, CONV_RELU}, {32, 32, CONV_RELU}, {32, 8, CONV_LINEAR}, {8, 32, CONV_GRAD_MASK},
                              {32, 32, CONV_GRAD_MASK}};
     const int wg[3][2] = {{8, 32}, {32, 32}, {32, 8}};
-    for (int k = 0; k < 8; k++) {
-        const bool is_conv = k < 5;
-        const void* fn = is_conv ? conv_kernel(modes[k][0], modes[k][1], modes[k][2]) : wgrad_kernel(wg[k - 5][0], wg[k - 5][1]);
-        const size_t smem = is_conv ? conv_smem(modes[k][0], modes[k][1]) : wgrad_smem(wg[k - 5][0], wg[k - 5][1]);
+    for (int k = 0; k < 13; k++) {
+        const bool is_conv = k < 10;
+        const int c = k % 5;
+        const bool rows = k < 5;
+        const void* fn = is_conv ? conv_kernel(modes[c][0], modes[c][1], modes[c][2], rows)
+                                 : wgrad_kernel(wg[k - 10][0], wg[k - 10][1]);
+        const size_t smem = is_conv ? conv_smem(modes[c][0], modes[c][1], rows) : wgrad_smem(wg[k - 10][0], wg[k - 10][1]);
         int per = 0;
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        if (!fn || cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem) != cudaSuccess) {
             set_error("cannot give a convolution kernel %zu bytes of shared memory", smem);
             return fail(VF_ECUDA);
         }
-        (is_conv ? h->grid_conv[k] : h->grid_wgrad[k - 5]) = std::max(per, 1) * sm_count();
+        (is_conv ? h->grid_conv[rows ? 0 : 1][c] : h->grid_wgrad[k - 10]) = std::max(per, 1) * sm_count();
     }
     for (int k = 0; k < 5; k++) {
         const void* fn = conv_umma_kernel(modes[k][0], modes[k][1], modes[k][2]);
@@ -516,7 +520,8 @@ void* vf_cnn_stream(vf_cnn* h) { return h ? (void*)h->stream : nullptr; }
 
 int32_t vf_cnn_set_path(vf_cnn* h, int32_t path) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
-    VF_REQUIRE(path == 0 || path == 1, VF_EINVAL, "path 0 (mma.sync) or 1 (tcgen05), got %d", path);
+    VF_REQUIRE(path >= 0 && path <= 2, VF_EINVAL,
+               "path 0 (mma.sync, row-blocked), 1 (tcgen05) or 2 (mma.sync, one row per warp), got %d", path);
     h->path = path;
     return VF_OK;
 }

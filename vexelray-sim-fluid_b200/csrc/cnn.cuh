@@ -61,12 +61,13 @@ struct WgradArgs {
 
 // The convolution kernels (cin, cout, mode) = (8, 32, RELU), (32, 32, RELU), (32, 8, LINEAR), (8, 32, GRAD_MASK),
 // (32, 32, GRAD_MASK), and the weight gradients (cin, cout) = (8, 32), (32, 32), (32, 8): 256 threads, the
-// dynamic shared memory below, a persistent grid of any size.
-const void* conv_kernel(int cin, int cout, int mode);
+// dynamic shared memory below, a persistent grid of any size. rows: the row-blocked kernels for 32 input
+// channels (a warp computes several output rows from each loaded A fragment); false: one output row per warp.
+const void* conv_kernel(int cin, int cout, int mode, bool rows);
 const void* wgrad_kernel(int cin, int cout);
-cudaError_t launch_conv(int cin, int cout, int mode, int grid, const ConvArgs& a, cudaStream_t s);
+cudaError_t launch_conv(int cin, int cout, int mode, bool rows, int grid, const ConvArgs& a, cudaStream_t s);
 cudaError_t launch_wgrad(int cin, int cout, int grid, const WgradArgs& a, cudaStream_t s);
-size_t conv_smem(int cin, int cout);
+size_t conv_smem(int cin, int cout, bool rows);
 size_t wgrad_smem(int cin, int cout);
 
 // The same convolutions on tcgen05 (cnn_umma.cu): 128 threads, conv_umma_smem_for bytes of dynamic shared memory,

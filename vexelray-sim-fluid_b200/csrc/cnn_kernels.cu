@@ -9,6 +9,12 @@
 // 25 taps x input channels (a 16-wide k step is 16 channels of one tap, or 8 channels of two taps when
 // the input has 8).
 //
+// The default is the row-blocked kernel (k_conv_rows): a warp computes 16 pixels of four output rows, so
+// each A fragment it loads from shared memory serves every output row that reads that input row (up to
+// five, one per ky) and each B fragment four rows. With 32 input and output channels ldmatrix traffic per
+// pixel falls from 6.25 to 2.8 fragments. With 8 input channels a k step pairs the taps (ky, 2p) and
+// (ky, 2p + 1), p = 0..2, so that the pairs stay within one kernel row; the sixth tap's A rows read zeros.
+//
 // Weight gradient: dW[co][tap][ci] = sum over pixels of dy[p][co] * x[p + tap][ci], a GEMM with M = output
 // channels, N = taps x input channels, K = pixels. Both operands come from shared memory through
 // ldmatrix.trans (pixels are their rows there); warps split the (tap, m tile) units, each accumulating in
@@ -63,6 +69,16 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// 16-byte asynchronous global -> shared copy; src_bytes 0 writes zeros (the source is not read).
+__device__ __forceinline__ void cp16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Stages the 36 x 12 input halo of the tile whose first output pixel is (x0, y0) of sample b, zeros outside.
 template <int C>
 __device__ __forceinline__ void stage_halo(__nv_bfloat16* in_s, const __nv_bfloat16* in, int b, int x0, int y0, int H,
@@ -80,8 +96,18 @@ __device__ __forceinline__ void stage_halo(__nv_bfloat16* in_s, const __nv_bfloa
 
 }  // namespace
 
-size_t conv_smem(int cin, int cout) {
-    return (size_t)cout * (conv_k(cin) + 8) * 2 + (size_t)HH * HW * cin * 2;
+// Rows per warp of the row-blocked convolutions (tile height 4 R).
+#ifndef CONV3_ROWS
+#define CONV3_ROWS 4
+#endif
+#ifndef CONV_ROWS_MINB
+#define CONV_ROWS_MINB 2
+#endif
+constexpr int conv_rows(int cout) { return cout == 8 ? CONV3_ROWS : 4; }
+
+size_t conv_smem(int cin, int cout, bool rows) {
+    const int hh = rows ? 4 * conv_rows(cout) + 4 : HH;
+    return (size_t)cout * (conv_k(cin) + 8) * 2 + (size_t)hh * HW * cin * 2 + (rows ? 16 : 0);
 }
 
 size_t wgrad_smem(int cin, int cout) {
@@ -202,6 +228,145 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(ConvArgs a) {
     }
 }
 
+// Row-blocked convolution for 32 input channels. A CTA owns a 32 x 4R output tile (input halo 36 x (4R+4),
+// staged by cp.async with zero fill); warp w computes pixel columns 16 (w & 1) .. +15 of output rows
+// R (w >> 1) .. +R-1. For each (kx, 16-channel half) the warp loads the A fragments of its R + 4 input rows once
+// and issues, for each ky, the MMAs of the R output rows that read them: an A fragment feeds up to five output
+// rows and a B fragment (one tap's weights) R rows, against one row each in k_conv.
+template <int CIN, int COUT, int MODE, int R>
+__global__ void __launch_bounds__(CONV_THREADS, CONV_ROWS_MINB) k_conv_rows(ConvArgs a) {
+    constexpr int NC = CIN / 8;
+    constexpr int K = conv_k(CIN), KP = K + 8;
+    constexpr int NT = COUT / 8;
+    constexpr int RH = 4 * R, HR = RH + 4;   // tile height, halo rows
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* w_s = reinterpret_cast<__nv_bfloat16*>(smem);   // [COUT][KP]
+    __nv_bfloat16* in_s = w_s + COUT * KP;                          // [HR][HW][CIN]
+    __nv_bfloat16* zrow = in_s + HR * HW * CIN;                      // 8 zeros: the A rows of the missing sixth tap
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < COUT * (K / 8); i += blockDim.x) {
+        const int co = i / (K / 8), c = i % (K / 8);
+        *reinterpret_cast<uint4*>(w_s + co * KP + c * 8) = *reinterpret_cast<const uint4*>(a.w + (int64_t)co * K + c * 8);
+    }
+    if (tid == 0) *reinterpret_cast<uint4*>(zrow) = make_uint4(0, 0, 0, 0);
+    const int H = a.H, W = a.W;
+    const int tx_n = (W + TW - 1) / TW, ty_n = (H + RH - 1) / RH;
+    const int total = a.B * tx_n * ty_n;
+    const int mt = warp & 1, rb = warp >> 1;
+    const int row = lane & 15, khalf = lane >> 4;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+        const int b = tile / (tx_n * ty_n), r0 = tile % (tx_n * ty_n);
+        const int x0 = (r0 % tx_n) * TW, y0 = (r0 / tx_n) * RH;
+        __syncthreads();   // the previous tile's halo is read
+        for (int i = tid; i < HR * HW * NC; i += blockDim.x) {
+            const int c = i % NC, px = (i / NC) % HW, py = i / (NC * HW);
+            const int gx = x0 + px - 2, gy = y0 + py - 2;
+            const bool in = gx >= 0 && gx < W && gy >= 0 && gy < H;
+            cp16(in_s + (py * HW + px) * CIN + swz<NC>(c, px) * 8,
+                 in ? a.in + (((int64_t)b * H + gy) * W + gx) * CIN + c * 8 : a.in, in ? 16u : 0u);
+        }
+        cp_wait_all();
+        __syncthreads();
+        float acc[R][NT][4];
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int n = 0; n < NT; n++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[r][n][q] = 0.0f;
+        // B fragments of the (kk0, kk1) weight columns (k 0-7 from kk0, 8-15 from kk1) into R rows' MMAs
+        auto mma_rows = [&](const uint32_t (&af)[R + 4][4], int ky, int kk0, int kk1) {
+            const int kk = ((lane >> 3) & 1) ? kk1 : kk0;
+            if constexpr (NT == 1) {
+                uint32_t bf[2];
+                ldsm_x2(bf, w_s + (lane & 7) * KP + kk);
+#pragma unroll
+                for (int r = 0; r < R; r++) mma_bf16(acc[r][0], af[r + ky], bf[0], bf[1]);
+            } else {
+#pragma unroll
+                for (int np = 0; np < NT / 2; np++) {
+                    uint32_t bf[4];
+                    ldsm_x4(bf, w_s + (np * 16 + ((lane >> 4) << 3) + (lane & 7)) * KP + kk);
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        mma_bf16(acc[r][2 * np], af[r + ky], bf[0], bf[1]);
+                        mma_bf16(acc[r][2 * np + 1], af[r + ky], bf[2], bf[3]);
+                    }
+                }
+            }
+        };
+        if constexpr (CIN == 8) {
+            // a k step is the taps (ky, 2p) and (ky, 2p + 1), p = 0..2: lanes 0-15 address the first tap's pixels,
+            // lanes 16-31 the second's; the sixth tap (kx = 5) reads the zero row against the zero weight column
+#pragma unroll 1
+            for (int p = 0; p < 3; p++) {
+                const int kx = 2 * p + khalf;
+                uint32_t af[R + 4][4];
+#pragma unroll
+                for (int ir = 0; ir < R + 4; ir++)
+                    ldsm_x4(af[ir], kx <= 4 ? in_s + ((rb * R + ir) * HW + 16 * mt + row + kx) * CIN : zrow);
+#pragma unroll
+                for (int ky = 0; ky < 5; ky++) {
+                    const int kk0 = (ky * 5 + 2 * p) * CIN;
+                    mma_rows(af, ky, kk0, p < 2 ? kk0 + CIN : 25 * CIN);
+                }
+            }
+        } else {
+#pragma unroll 1
+        for (int kx = 0; kx < 5; kx++) {
+#pragma unroll
+            for (int kc = 0; kc < CIN / 16; kc++) {
+                const int c = kc * 2 + khalf, p = 16 * mt + row + kx;
+                const __nv_bfloat16* abase = in_s + (rb * R * HW + p) * CIN + swz<NC>(c, p) * 8;
+                uint32_t af[R + 4][4];
+#pragma unroll
+                for (int ir = 0; ir < R + 4; ir++) ldsm_x4(af[ir], abase + ir * HW * CIN);
+#pragma unroll
+                for (int ky = 0; ky < 5; ky++) {
+                    const int kk = (ky * 5 + kx) * CIN + kc * 16;
+                    mma_rows(af, ky, kk, kk + 8);
+                }
+            }
+        }
+        }
+        // epilogue: fragment element q of (row r, n tile) is pixel 16 mt + lane/4 (+8 for q >= 2), channel
+        // 8 n + 2 (lane%4) + q%2
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int py = y0 + rb * R + r;
+            if (py >= H) continue;
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int px = x0 + 16 * mt + (lane >> 2) + half * 8;
+                if (px >= W) continue;
+                const int64_t pix = ((int64_t)b * H + py) * W + px;
+#pragma unroll
+                for (int n = 0; n < NT; n++) {
+                    const int co = n * 8 + 2 * (lane & 3);
+                    float v0 = acc[r][n][2 * half], v1 = acc[r][n][2 * half + 1];
+                    if constexpr (MODE != CONV_GRAD_MASK) {
+                        if (a.bias) {
+                            if (co < a.bias_n) v0 += a.bias[co];
+                            if (co + 1 < a.bias_n) v1 += a.bias[co + 1];
+                        }
+                    }
+                    if constexpr (MODE == CONV_RELU) {
+                        *reinterpret_cast<__nv_bfloat162*>(a.out_b + pix * COUT + co) =
+                            __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+                    } else if constexpr (MODE == CONV_LINEAR) {
+                        *reinterpret_cast<float2*>(a.out_f + pix * COUT + co) = make_float2(v0, v1);
+                    } else {
+                        const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162*>(a.mask + pix * COUT + co);
+                        if (!(__bfloat162float(mk.x) > 0.0f)) v0 = 0.0f;
+                        if (!(__bfloat162float(mk.y) > 0.0f)) v1 = 0.0f;
+                        *reinterpret_cast<__nv_bfloat162*>(a.out_b + pix * COUT + co) = __floats2bfloat162_rn(v0, v1);
+                    }
+                }
+            }
+        }
+    }
+}
+
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv_wgrad(WgradArgs a) {
     constexpr int NCI = CIN / 8;
@@ -304,7 +469,15 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv_wgrad(WgradArgs a) {
 }
 
 // Launches of the instantiations the network uses (the templates stay in this translation unit).
-const void* conv_kernel(int cin, int cout, int mode) {
+const void* conv_kernel(int cin, int cout, int mode, bool rows) {
+    if (rows) {
+        if (cin == 8 && cout == 32 && mode == CONV_RELU) return (const void*)k_conv_rows<8, 32, CONV_RELU, 4>;
+        if (cin == 32 && cout == 32 && mode == CONV_RELU) return (const void*)k_conv_rows<32, 32, CONV_RELU, 4>;
+        if (cin == 32 && cout == 8 && mode == CONV_LINEAR) return (const void*)k_conv_rows<32, 8, CONV_LINEAR, CONV3_ROWS>;
+        if (cin == 8 && cout == 32 && mode == CONV_GRAD_MASK) return (const void*)k_conv_rows<8, 32, CONV_GRAD_MASK, 4>;
+        if (cin == 32 && cout == 32 && mode == CONV_GRAD_MASK) return (const void*)k_conv_rows<32, 32, CONV_GRAD_MASK, 4>;
+        return nullptr;
+    }
     if (cin == 8 && cout == 32 && mode == CONV_RELU) return (const void*)k_conv<8, 32, CONV_RELU>;
     if (cin == 32 && cout == 32 && mode == CONV_RELU) return (const void*)k_conv<32, 32, CONV_RELU>;
     if (cin == 32 && cout == 8 && mode == CONV_LINEAR) return (const void*)k_conv<32, 8, CONV_LINEAR>;
@@ -320,11 +493,11 @@ const void* wgrad_kernel(int cin, int cout) {
     return nullptr;
 }
 
-cudaError_t launch_conv(int cin, int cout, int mode, int grid, const ConvArgs& a, cudaStream_t s) {
-    const void* k = conv_kernel(cin, cout, mode);
+cudaError_t launch_conv(int cin, int cout, int mode, bool rows, int grid, const ConvArgs& a, cudaStream_t s) {
+    const void* k = conv_kernel(cin, cout, mode, rows);
     if (!k) return cudaErrorInvalidValue;
     void* args[] = {const_cast<ConvArgs*>(&a)};
-    return cudaLaunchKernel(k, dim3(grid), dim3(CONV_THREADS), args, conv_smem(cin, cout), s);
+    return cudaLaunchKernel(k, dim3(grid), dim3(CONV_THREADS), args, conv_smem(cin, cout, rows), s);
 }
 
 cudaError_t launch_wgrad(int cin, int cout, int grid, const WgradArgs& a, cudaStream_t s) {

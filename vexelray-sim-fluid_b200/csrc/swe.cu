@@ -26,12 +26,17 @@ using namespace vf;
 
 namespace {
 
-constexpr int TX = 64, TY = 16;                 // cells per tile
-constexpr int HX = TX + 8;                      // loaded box width: x0-4 .. x0+TX+3
-constexpr int HY = TY + 2;                      // loaded box height: y0-1 .. y0+TY
-constexpr int PX = TX + 2, PY = TY + 2;         // primitive window: x0-1 .. x0+TX
+// A tile is TX x 16 cells, TX = 64, or 32 on grids too small to fill the GPU with 64-wide tiles.
+template <int TX_>
+struct Tile {
+    static constexpr int TX = TX_, TY = 16;
+    static constexpr int HX = TX + 8;                  // loaded box width: x0-4 .. x0+TX+3
+    static constexpr int HY = TY + 2;                  // loaded box height: y0-1 .. y0+TY
+    static constexpr int PX = TX + 2, PY = TY + 2;     // primitive window: x0-1 .. x0+TX
+    static constexpr int BOXF = (HY * HX * 4 + 127) / 128 * 128 / 4;   // floats per staged field, 128-byte padded
+};
 constexpr int SWE_THREADS = 256;
-constexpr int BOXF = (HY * HX * 4 + 127) / 128 * 128 / 4;   // floats per staged field, 128-byte padded
+constexpr int SWE_TY = 16;
 
 struct SweArgs {
     const float* in[3];
@@ -49,11 +54,13 @@ struct SweArgs {
     int use_tma;
 };
 
+template <int TX_>
 struct SweShared {
-    float box[3][BOXF];                         // h, hu, hv, each [HY][HX] (TMA destinations, 128-byte aligned)
-    float pu[PY][PX], pv[PY][PX], pc[PY][PX];   // primitives
-    float fx[3][TY][TX + 1];                    // x-face fluxes (mass, normal=hu, tangent=hv)
-    float fy[3][TY + 1][TX];                    // y-face fluxes (mass, normal=hv, tangent=hu)
+    using T = Tile<TX_>;
+    float box[3][T::BOXF];                                    // h, hu, hv, each [HY][HX] (TMA destinations)
+    float pu[T::PY][T::PX], pv[T::PY][T::PX], pc[T::PY][T::PX];   // primitives
+    float fx[3][T::TY][T::TX + 1];                            // x-face fluxes (mass, normal=hu, tangent=hv)
+    float fy[3][T::TY + 1][T::TX];                            // y-face fluxes (mass, normal=hv, tangent=hu)
     unsigned long long bar;
     int red[SWE_THREADS / 32];
     int clamps;
@@ -115,12 +122,15 @@ __device__ __forceinline__ bool wait_barrier(unsigned long long* bar, int phase,
     return false;
 }
 
+template <int TX_>
 __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
                                                           const __grid_constant__ CUtensorMap tm_hu,
                                                           const __grid_constant__ CUtensorMap tm_hv) {
+    using T = Tile<TX_>;
+    constexpr int TX = T::TX, TY = T::TY, HX = T::HX, HY = T::HY, PX = T::PX, PY = T::PY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t mis = (uint32_t)__cvta_generic_to_shared(smem_raw) & 127u;
-    SweShared& S = *reinterpret_cast<SweShared*>(smem_raw + ((128u - mis) & 127u));
+    SweShared<TX_>& S = *reinterpret_cast<SweShared<TX_>*>(smem_raw + ((128u - mis) & 127u));
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int nx = a.nx, ny = a.ny;
@@ -310,6 +320,9 @@ __global__ void __launch_bounds__(256) k_swe_speed(const float* h, const float* 
 
 // Coarse cell (i, j) of the box [x0, x0 + cnx) x [y0, y0 + cny) = the mean of fine cells (2i..2i+1, 2j..2j+1)
 // counted from the fine patch's cell (fx0, fy0).
+// One device word from a kernel argument: the budget written in stream order, without a host wait.
+__global__ void k_swe_set_word(int* p, int v) { *p = v; }
+
 __global__ void k_swe_restrict(const float* const* fine, int fnx, int fx0, int fy0, float* const* coarse, int ccnx,
                                int x0, int y0, int cnx, int cny) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -412,20 +425,27 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
-// A 2D tensor map over one nx x ny f32 field with an HX x HY box; false if TMA cannot take it
+// A 2D tensor map over one nx x ny f32 field with an hx x hy box; false if TMA cannot take it
 // (row pitch not a multiple of 16 bytes, or an unaligned base).
-bool make_map(CUtensorMap* m, const float* base, int nx, int ny) {
+bool make_map(CUtensorMap* m, const float* base, int nx, int ny, int hx, int hy) {
     EncodeTiled enc = encode_fn();
     if (!enc) return false;
     if (((uintptr_t)base & 15) || ((int64_t)nx * 4) % 16 != 0) return false;
     cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
     cuuint64_t strides[1] = {(cuuint64_t)nx * 4};
-    cuuint32_t box[2] = {(cuuint32_t)HX, (cuuint32_t)HY};
+    cuuint32_t box[2] = {(cuuint32_t)hx, (cuuint32_t)hy};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+// 64-wide tiles unless they would give the GPU fewer than four tiles per resident slot (four CTAs of
+// SweShared<64> fit an SM): the last wave's imbalance then costs more than the narrower tile's halo.
+int auto_tile_width(int nx, int ny) {
+    const int64_t tiles = (int64_t)div_up(nx, 64) * div_up(ny, SWE_TY);
+    return tiles < (int64_t)16 * sm_count() ? 32 : 64;
 }
 
 }  // namespace
@@ -440,8 +460,10 @@ struct vf_swe {
     DeviceBuffer state[2];    // 3 fields each
     DeviceBuffer small;       // speed[3], budget[2], clamped, params[5] (as ints/floats)
     DeviceBuffer status, diag;
-    CUtensorMap maps[2][3];
+    int32_t* host_words = nullptr;   // pinned: the budget and the status word read back together
+    CUtensorMap maps[2][2][3];   // [tile width 64, 32][state][field]
     bool tma = false;
+    int tile_w = 64;             // the tile width the steps use
     // PatchSimulation.java:52-56
     int64_t clock_now = 0;
     int32_t clock_outstanding = 0;
@@ -492,24 +514,41 @@ int32_t dispatch(vf_swe* h) {
     a.ny = h->ny;
     for (int e = 0; e < 4; e++) a.edge[e] = h->edges[e];
     a.use_tma = h->tma ? 1 : 0;
-    dim3 grid(div_up(h->nx, TX), div_up(h->ny, TY));
-    const CUtensorMap* m = h->maps[si];
-    VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile, grid, SWE_THREADS, sizeof(SweShared) + 128, a, m[0], m[1],
-              m[2]);
+    const int wide = h->tile_w == 64;
+    const CUtensorMap* m = h->maps[wide ? 0 : 1][si];
+    dim3 grid(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
+    if (wide)
+        VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile<64>, grid, SWE_THREADS, sizeof(SweShared<64>) + 128, a,
+                  m[0], m[1], m[2]);
+    else
+        VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile<32>, grid, SWE_THREADS, sizeof(SweShared<32>) + 128, a,
+                  m[0], m[1], m[2]);
     h->dispatched++;
     return VF_OK;
 }
 
-int32_t read_budget(vf_swe* h, int slot, int32_t* out) {
-    VF_TRY_CUDA(cudaMemcpyAsync(out, budget_slot(h, slot), 4, cudaMemcpyDeviceToHost, h->stream));
+// The budget left in slot and the device status word, in one host wait.
+int32_t read_budget(vf_swe* h, int slot, int32_t* out, uint32_t* status) {
+    VF_TRY_CUDA(cudaMemcpyAsync(h->host_words, budget_slot(h, slot), 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaMemcpyAsync(h->host_words + 1, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    *out = h->host_words[0];
+    if (status) *status = (uint32_t)h->host_words[1];
     return VF_OK;
 }
 
+// Stream-ordered: the steps dispatched after it read the new budget; no host wait.
 int32_t write_budget(vf_swe* h, int slot, int32_t v) {
-    VF_TRY_CUDA(cudaMemcpyAsync(budget_slot(h, slot), &v, 4, cudaMemcpyHostToDevice, h->stream));
-    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    VF_LAUNCH(h->prof, "k_swe_set_word", h->stream, k_swe_set_word, 1, 1, 0, budget_slot(h, slot), v);
     return VF_OK;
+}
+
+// A nonzero device status (read back with the budget): cleared, and reported as the error it is.
+int32_t status_error(vf_swe* h, uint32_t st) {
+    if (!st) return VF_OK;
+    VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+    set_error("a kernel flagged device status 0x%x", st);
+    return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
 }
 
 int32_t status_swe(vf_swe* h) {
@@ -567,18 +606,29 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
         vf_swe_destroy(h);
         return rc;
     }
-    for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status}) cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream);
-    if (cudaFuncSetAttribute(k_swe_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SweShared) + 128) !=
-        cudaSuccess) {
+    if (cudaMallocHost(&h->host_words, 16) != cudaSuccess) {
+        h->host_words = nullptr;
         vf_swe_destroy(h);
-        set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared));
+        set_error("cudaMallocHost(16) failed");
+        return VF_ENOMEM;
+    }
+    for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status}) cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream);
+    if (cudaFuncSetAttribute(k_swe_tile<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
+        cudaFuncSetAttribute(k_swe_tile<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(SweShared<32>) + 128) != cudaSuccess) {
+        vf_swe_destroy(h);
+        set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared<64>));
         return VF_ECUDA;
     }
     bool tma = true;
     for (int s = 0; s < 2; s++)
-        for (int f = 0; f < 3; f++) tma = tma && make_map(&h->maps[s][f], field(h, s, f), nx, ny);
+        for (int f = 0; f < 3; f++)
+            tma = tma && make_map(&h->maps[0][s][f], field(h, s, f), nx, ny, Tile<64>::HX, Tile<64>::HY) &&
+                  make_map(&h->maps[1][s][f], field(h, s, f), nx, ny, Tile<32>::HX, Tile<32>::HY);
     h->tma = tma;
     if (!tma) memset(h->maps, 0, sizeof h->maps);
+    h->tile_w = auto_tile_width(nx, ny);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("clearing buffers failed");
@@ -636,6 +686,8 @@ int32_t vf_swe_advance(vf_swe* h, int64_t ticks, int32_t max_steps, int32_t* ste
     if (rc) return rc;
     int32_t left = granted;
     int32_t steps = 0;
+    bool read = false;
+    uint32_t st = 0;
     while (left > 0 && steps < max_steps) {
         const int32_t batch =
             h->last_step > 0 ? (int32_t)std::min<int64_t>(max_steps - steps, ((int64_t)left + h->last_step - 1) / h->last_step)
@@ -644,7 +696,8 @@ int32_t vf_swe_advance(vf_swe* h, int64_t ticks, int32_t max_steps, int32_t* ste
             if ((rc = dispatch(h))) return rc;
         steps += batch;
         int32_t now = 0;
-        if ((rc = read_budget(h, (int)(h->dispatched % 2), &now))) return rc;
+        if ((rc = read_budget(h, (int)(h->dispatched % 2), &now, &st))) return rc;
+        read = true;
         if (now > 0 && now < left) h->last_step = (left - now) / batch;
         left = now;
     }
@@ -654,7 +707,7 @@ int32_t vf_swe_advance(vf_swe* h, int64_t ticks, int32_t max_steps, int32_t* ste
     if (steps_out) *steps_out = steps;
     if (spent) *spent = h->clock_now - before;
     if (behind) *behind = left;
-    return status_swe(h);
+    return read ? status_error(h, st) : status_swe(h);
 }
 
 int32_t vf_swe_read(vf_swe* h, float* hcell, float* hu, float* hv) {
@@ -699,6 +752,16 @@ int32_t vf_swe_dispatch(vf_swe* h, int32_t n) {
 
 int64_t vf_swe_dispatched(const vf_swe* h) { return h ? h->dispatched : 0; }
 
+int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(width == 0 || width == 32 || width == 64, VF_EINVAL, "a tile is 32 or 64 cells wide (0: by grid size), got %d",
+               width);
+    h->tile_w = width ? width : auto_tile_width(h->nx, h->ny);
+    return VF_OK;
+}
+
+int32_t vf_swe_tile_width(const vf_swe* h) { return h ? h->tile_w : 0; }
+
 int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks) {
     VF_REQUIRE(h && (slot == 0 || slot == 1), VF_EINVAL, "budget slot is 0 or 1");
     return write_budget(h, slot, ticks);
@@ -706,8 +769,9 @@ int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks) {
 
 int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks) {
     VF_REQUIRE(h && ticks && (slot == 0 || slot == 1), VF_EINVAL, "budget slot is 0 or 1");
-    int32_t rc = read_budget(h, slot, ticks);
-    return rc ? rc : status_swe(h);
+    uint32_t st = 0;
+    int32_t rc = read_budget(h, slot, ticks, &st);
+    return rc ? rc : status_error(h, st);
 }
 
 int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]) {
@@ -767,6 +831,7 @@ void vf_swe_destroy(vf_swe* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status, &h->diag}) b->release();
+    if (h->host_words) cudaFreeHost(h->host_words);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
