@@ -295,6 +295,10 @@ int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks);
  * bit-identical for both widths, only the speed differs. */
 int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width);
 int32_t vf_swe_tile_width(const vf_swe* h);
+/* Each step launched as a programmatic dependent of the previous one (its CTAs may become resident during the
+ * previous step's last wave and wait on the device for its completion): 1 (the default) or 0 (plain stream
+ * order). Bit-identical either way. */
+int32_t vf_swe_set_overlap(vf_swe* h, int32_t on);
 /* Diagnostics.of(h, hu, hv, g, dry, dt, dx, dy) over the current state (Diagnostics.java:43-81), reduced on the
  * device. out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
 int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]);

@@ -202,6 +202,7 @@ def lib() -> ctypes.CDLL:
         "vf_swe_dispatched": ([_vp], ctypes.c_int64),
         "vf_swe_set_tile_width": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_tile_width": ([_vp], ctypes.c_int32),
+        "vf_swe_set_overlap": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_read_budget": ([_vp, ctypes.c_int32, _i32p], ctypes.c_int32),
         "vf_swe_diagnostics": ([_vp] + [ctypes.c_double] * 5 + [ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
@@ -1030,6 +1031,10 @@ class PatchSimulation:
 
     def tile_width(self) -> int:
         return int(lib().vf_swe_tile_width(self._h))
+
+    def set_overlap(self, on: bool) -> None:
+        """Steps launched as programmatic dependents of the previous step (default) or in plain stream order."""
+        check(lib().vf_swe_set_overlap(self._h, 1 if on else 0))
 
     def read_budget(self, slot: int) -> int:
         v = ctypes.c_int32()

@@ -59,10 +59,6 @@ struct Scene2 {
     Params2 prm;
 };
 
-struct GridBarrier {
-    unsigned count, gen;
-};
-
 // The batch's device state, passed by value to the step kernel.
 struct Batch2 {
     const Scene2* scene;
@@ -125,41 +121,6 @@ __device__ __forceinline__ void load_part2(Part2& q, const float* __restrict__ i
     q.c10 = in[PC10 * st + src];
     q.c11 = in[PC11 * st + src];
 }
-constexpr int BAR_SPINS = 1 << 24;   // x ~64 ns of __nanosleep: about a second
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Grid-wide barrier of a cooperative launch (all CTAs co-resident). The last CTA to arrive resets the
-// count and advances the generation; the others wait for the generation to change, at most BAR_SPINS
-// polls, after which they set ST_TIMEOUT and go on (the host reports the status; the kernel ends).
-__device__ void grid_barrier(GridBarrier* b, uint32_t* status) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = ld_acquire(&b->gen);
-        __threadfence();
-        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            int spins = 0;
-            while (ld_acquire(&b->gen) == gen) {
-                if (++spins > BAR_SPINS) {
-                    set_status(status, ST_TIMEOUT);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

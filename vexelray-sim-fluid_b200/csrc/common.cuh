@@ -87,6 +87,46 @@ __device__ __forceinline__ float impulse_factor(float dt, float m, float rho0, f
     return __fmul_rn(__fmul_rn(4.0f, __fmul_rn(dt, __fdiv_rn(m, rho0))), jp);
 }
 
+// ------------------------------------------------------------------ grid-wide barrier (cooperative launches)
+struct GridBarrier {
+    unsigned count, gen;
+};
+
+constexpr int BAR_SPINS = 1 << 24;   // x ~64 ns of __nanosleep: about a second
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs co-resident). The last CTA to arrive resets the
+// count and advances the generation; the others wait for the generation to change, at most BAR_SPINS
+// polls, after which they set ST_TIMEOUT and go on (the host reports the status; the kernel ends).
+__device__ __forceinline__ void grid_barrier(GridBarrier* b, uint32_t* status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&b->gen);
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            int spins = 0;
+            while (ld_acquire(&b->gen) == gen) {
+                if (++spins > BAR_SPINS) {
+                    set_status(status, ST_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 // Params words (int32 bits) to floats, with the reference's validation.

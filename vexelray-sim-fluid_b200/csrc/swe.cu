@@ -122,25 +122,23 @@ __device__ __forceinline__ bool wait_barrier(unsigned long long* bar, int phase,
     return false;
 }
 
+// One tile (tx, ty) of one step. The CTA's mbarrier is initialised; `parity` is the phase its TMA completes.
+// Returns false (status set, nothing written) when the TMA did not land within the bounded wait.
 template <int TX_>
-__global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
-                                                          const __grid_constant__ CUtensorMap tm_hu,
-                                                          const __grid_constant__ CUtensorMap tm_hv) {
+__device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm_h, const CUtensorMap* tm_hu,
+                                         const CUtensorMap* tm_hv, SweShared<TX_>& S, int tx, int ty, int parity) {
     using T = Tile<TX_>;
     constexpr int TX = T::TX, TY = T::TY, HX = T::HX, HY = T::HY, PX = T::PX, PY = T::PY;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const uint32_t mis = (uint32_t)__cvta_generic_to_shared(smem_raw) & 127u;
-    SweShared<TX_>& S = *reinterpret_cast<SweShared<TX_>*>(smem_raw + ((128u - mis) & 127u));
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int x0 = tx * TX, y0 = ty * TY;
     const int nx = a.nx, ny = a.ny;
 
     // ShallowWater.java:184-192: the step from the fastest wave, in whole ticks, within the budget
     const float g = a.params[0], courant = a.params[1], dx = a.params[2], dy = a.params[3], dry = a.params[4];
-    const float fastest = __int_as_float(*a.speed_in);
+    const float fastest = __int_as_float(__ldcg(a.speed_in));
     const float allowed = fminf((courant * fminf(dx, dy)) / fmaxf(fastest, 1e-30f), 2000.0f);
     int ticks = (int)(allowed * 1000000.0f);
-    const int budget = *a.budget_in;
+    const int budget = __ldcg(a.budget_in);
     if (budget < ticks) ticks = budget;
     const float dt = (float)ticks * (float)(1.0 / 1000000.0);
     const float rx = dt / dx;
@@ -148,20 +146,15 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
 
     // 1. stage the tile + halo
     bool loaded = true;
+    if (tid == 0) S.clamps = 0;
     if (a.use_tma) {
         if (tid == 0) {
-            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            // the previous tile's reads of the box (generic proxy) before this tile's TMA writes (async proxy)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            S.clamps = 0;
-        }
-        __syncthreads();
-        if (tid == 0) {
             const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
             const uint32_t bytes = 3u * HY * HX * 4u;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-            const CUtensorMap* maps[3] = {&tm_h, &tm_hu, &tm_hv};
+            const CUtensorMap* maps[3] = {tm_h, tm_hu, tm_hv};
             const int bx = x0 - 4, by = y0 - 1;   // bx is a multiple of 4: 16-byte aligned
             for (int f = 0; f < 3; f++) {
                 const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&S.box[f][0]);
@@ -172,19 +165,18 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
                     : "memory");
             }
         }
-        loaded = wait_barrier(&S.bar, 0, a.status);
+        loaded = wait_barrier(&S.bar, parity, a.status);
     } else {
-        if (tid == 0) S.clamps = 0;
         for (int i = tid; i < HY * HX; i += SWE_THREADS) {
             const int ly = i / HX, lx = i % HX;
             const int gx = x0 - 4 + lx, gy = y0 - 1 + ly;
             const bool in = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
             const int64_t c = (int64_t)gy * nx + gx;
-            for (int f = 0; f < 3; f++) S.box[f][ly * HX + lx] = in ? a.in[f][c] : 0.0f;
+            for (int f = 0; f < 3; f++) S.box[f][ly * HX + lx] = in ? __ldcg(a.in[f] + c) : 0.0f;
         }
     }
-    __syncthreads();
-    if (!loaded) return;   // a TMA that never landed: the status word says so, nothing is written
+    // a TMA that never landed: the status word says so, nothing of the tile is written
+    if (!__syncthreads_and(loaded)) return false;
 
     // 2. primitives of tile + halo (cells x0-1..x0+TX, y0-1..y0+TY that lie in the domain)
     for (int i = tid; i < PY * PX; i += SWE_THREADS) {
@@ -293,6 +285,39 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
         if (m > *(volatile int*)a.speed_out) atomicMax(a.speed_out, m);
         if (S.clamps) atomicAdd(a.clamped, S.clamps);
     }
+    __syncthreads();   // the tile's shared memory is free for the next
+    return true;
+}
+
+template <int TX_>
+__device__ __forceinline__ SweShared<TX_>& swe_shared() {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t mis = (uint32_t)__cvta_generic_to_shared(smem_raw) & 127u;
+    return *reinterpret_cast<SweShared<TX_>*>(smem_raw + ((128u - mis) & 127u));
+}
+
+template <int TX_>
+__device__ __forceinline__ void init_tile_barrier(SweShared<TX_>& S, bool tma) {
+    if (threadIdx.x == 0 && tma) {
+        const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// One step, one CTA per tile (grid = tiles). Launched as a programmatic dependent of the previous step: its CTAs
+// may become resident during that step's last wave, set up their barrier, and wait (griddepcontrol.wait: until
+// the previous grid has completed and its stores are visible) before reading anything the previous step wrote.
+template <int TX_>
+__global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
+                                                          const __grid_constant__ CUtensorMap tm_hu,
+                                                          const __grid_constant__ CUtensorMap tm_hv) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    SweShared<TX_>& S = swe_shared<TX_>();
+    init_tile_barrier(S, a.use_tma);
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    swe_tile<TX_>(a, &tm_h, &tm_hu, &tm_hv, S, blockIdx.x, blockIdx.y, 0);
 }
 
 // ------------------------------------------------------------------ diagnostics (Diagnostics.of)
@@ -464,6 +489,7 @@ struct vf_swe {
     CUtensorMap maps[2][2][3];   // [tile width 64, 32][state][field]
     bool tma = false;
     int tile_w = 64;             // the tile width the steps use
+    bool pdl = true;             // steps launched as programmatic dependents of the previous step
     // PatchSimulation.java:52-56
     int64_t clock_now = 0;
     int32_t clock_outstanding = 0;
@@ -515,14 +541,22 @@ int32_t dispatch(vf_swe* h) {
     for (int e = 0; e < 4; e++) a.edge[e] = h->edges[e];
     a.use_tma = h->tma ? 1 : 0;
     const int wide = h->tile_w == 64;
-    const CUtensorMap* m = h->maps[wide ? 0 : 1][si];
-    dim3 grid(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
-    if (wide)
-        VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile<64>, grid, SWE_THREADS, sizeof(SweShared<64>) + 128, a,
-                  m[0], m[1], m[2]);
-    else
-        VF_LAUNCH(h->prof, "k_swe_tile", h->stream, k_swe_tile<32>, grid, SWE_THREADS, sizeof(SweShared<32>) + 128, a,
-                  m[0], m[1], m[2]);
+    CUtensorMap* m = h->maps[wide ? 0 : 1][si];
+    void* args[] = {&a, &m[0], &m[1], &m[2]};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
+    cfg.blockDim = dim3(SWE_THREADS);
+    cfg.dynamicSmemBytes = wide ? sizeof(SweShared<64>) + 128 : sizeof(SweShared<32>) + 128;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = h->pdl ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    h->prof.begin("k_swe_tile", h->stream);
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, wide ? (const void*)k_swe_tile<64> : (const void*)k_swe_tile<32>, args);
+    h->prof.end(h->stream);
+    VF_TRY_CUDA(e);
     h->dispatched++;
     return VF_OK;
 }
@@ -555,12 +589,7 @@ int32_t status_swe(vf_swe* h) {
     uint32_t st = 0;
     VF_TRY_CUDA(cudaMemcpyAsync(&st, h->status.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
-    if (st) {
-        VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
-        set_error("a kernel flagged device status 0x%x", st);
-        return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
-    }
-    return VF_OK;
+    return status_error(h, st);
 }
 
 // ShallowWater.fastestWave (ShallowWater.java:287-295), on the host.
@@ -761,6 +790,12 @@ int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
 }
 
 int32_t vf_swe_tile_width(const vf_swe* h) { return h ? h->tile_w : 0; }
+
+int32_t vf_swe_set_overlap(vf_swe* h, int32_t on) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->pdl = on != 0;
+    return VF_OK;
+}
 
 int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks) {
     VF_REQUIRE(h && (slot == 0 || slot == 1), VF_EINVAL, "budget slot is 0 or 1");
