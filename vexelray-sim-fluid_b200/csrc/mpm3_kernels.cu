@@ -150,11 +150,12 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 // Each warp takes work units of (non-empty brick, slab of 8 x 4 x 1 cells), sixteen per brick, with no
 // barrier between warps.
 //
-//  1. Lane l owns cell (l % 8, l / 8) of the slab. It first puts its cell's run of the sort's permutation
-//     in ascending order, in place (the stable sort's fix-up, fused here: G2P then reads the stable
-//     permutation), then sums the 27 x 4 deposits of the cell's particles in registers, loading two
-//     particles ahead of the one it sums. A slab's cells are 32 consecutive keys, so their particle
-//     runs form one contiguous range.
+//  1. Lane l owns cell (l % 8, l / 8) of the slab. A slab's cells are 32 consecutive keys, so their
+//     particle runs form one contiguous range of the sort's permutation: the warp stages it in shared
+//     memory, each lane puts its cell's run in ascending order there (the stable sort's fix-up, fused
+//     here: G2P then reads the stable permutation), and the warp writes the range back. The lane then sums
+//     the 27 x 4 deposits of its cell's particles in registers, loading two particles ahead of the one it
+//     sums.
 //  2. The slab's deposits reach a 10 x 6 x 3 node window, private to the warp in shared memory. At one
 //     stencil offset the 32 lanes hit 32 different nodes, so the window takes the cell sums by plain
 //     read-modify-write, a __syncwarp between offsets: no shared-memory atomics.
@@ -169,8 +170,11 @@ constexpr int P2G_THREADS = 128;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
 constexpr int WWX = WIN, WWY = 6, WWZ = 3, WW = WWX * WWY * WWZ;   // a warp's window: 180 nodes
 
+constexpr int RUN_CAP = 768;   // particle slots of one slab staged in shared memory (more: sorted in place)
+
 struct P2GShared {
     float4 wwin[P2G_WARPS][WW];
+    int run[P2G_WARPS][RUN_CAP];   // the slab's run of the permutation, sorted per cell here
 };
 constexpr size_t P2G_SMEM = sizeof(P2GShared);
 // One particle's fields, as the scatter reads them.
@@ -233,18 +237,32 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
         const int s1 = min(max(c < 511 ? s.cell_start[key + 1] : be, s0), be);
         if (!__any_sync(0xffffffffu, s1 > s0)) continue;          // an empty slab (warp-uniform)
 
-        // 1. the stable order of this cell's run, then its particles summed in registers
-        if (s1 - s0 > 1) insertion_sort_run(perm + s0, s1 - s0);
+        // 1. the stable order of this cell's run, then its particles summed in registers. The slab's 32 runs are
+        //    one range [S0, S1): staged in the warp's shared memory, each lane sorts its run there and the warp
+        //    writes the range back, coalesced (in place in global memory when it does not fit).
+        const int S0 = __shfl_sync(0xffffffffu, s0, 0), S1 = __shfl_sync(0xffffffffu, s1, 31);
+        const bool staged = __all_sync(0xffffffffu, s0 >= S0 && s1 <= S1) && S1 - S0 <= RUN_CAP;
+        int* rs = S.run[warp];
+        if (staged) {
+            for (int j = S0 + lane; j < S1; j += 32) rs[j - S0] = perm[j];
+            __syncwarp();
+            if (s1 - s0 > 1) insertion_sort_run(rs + (s0 - S0), s1 - s0);
+            __syncwarp();
+            for (int j = S0 + lane; j < S1; j += 32) perm[j] = rs[j - S0];
+        } else if (s1 - s0 > 1) {
+            insertion_sort_run(perm + s0, s1 - s0);
+        }
+        const int* run = staged ? rs : perm + S0;   // the run, indexed from S0
         float acc[27][4];
 #pragma unroll
         for (int k = 0; k < 27; k++) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
         PIn nxt, nxt2;
-        if (s0 < s1) load_pin(nxt, in, st, checked_src(perm, s0, s.np, s.status));
-        if (s0 + 1 < s1) load_pin(nxt2, in, st, checked_src(perm, s0 + 1, s.np, s.status));
+        if (s0 < s1) load_pin(nxt, in, st, checked_src(run, s0 - S0, s.np, s.status));
+        if (s0 + 1 < s1) load_pin(nxt2, in, st, checked_src(run, s0 + 1 - S0, s.np, s.status));
         for (int i = s0; i < s1; i++) {
             const PIn qq = nxt;
             nxt = nxt2;
-            if (i + 2 < s1) load_pin(nxt2, in, st, checked_src(perm, i + 2, s.np, s.status));
+            if (i + 2 < s1) load_pin(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
             if (!(qq.m > 0.0f)) continue;
             int cell[3];
             float f[3];
