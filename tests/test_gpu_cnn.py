@@ -52,7 +52,7 @@ def blocks(g):
     return {k: np.asarray(v, np.float64) for k, v in d.items()}
 
 
-PATHS = [pytest.param(1, id="tcgen05"), pytest.param(0, id="mma_sync_rows"), pytest.param(2, id="mma_sync_row")]
+PATHS = [pytest.param(0, id="tcgen05"), pytest.param(1, id="mma_sync_rows"), pytest.param(2, id="mma_sync_row")]
 
 
 @pytest.mark.parametrize("path", PATHS)

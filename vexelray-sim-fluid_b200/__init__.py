@@ -673,8 +673,8 @@ class FluxNet:
         check(lib().vf_swe_measure_speed(sim._h))
 
     def set_path(self, path: int) -> None:
-        """The convolutions' kernels: 0 mma.sync row-blocked (default), 1 tcgen05, 2 mma.sync one output row per
-        warp."""
+        """The convolutions' kernels: 0 tcgen05 for the 32-channel inputs (default), 1 mma.sync row-blocked, 2
+        mma.sync one output row per warp."""
         check(lib().vf_cnn_set_path(self._h, path))
 
     def status(self) -> None:

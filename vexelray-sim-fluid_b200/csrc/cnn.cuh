@@ -1,6 +1,7 @@
 // cnn.cuh -- the flux-correction network of the learned coarse shallow-water solver: three 5x5
 // convolutions (3 -> 32 -> 32 -> 6 channels, ReLU between), bf16 weights and activations, fp32
-// accumulation on the tensor cores (mma.sync m16n8k16), trained with Adam on fp32 master weights.
+// accumulation on the tensor cores (tcgen05 for the 32-channel inputs, mma.sync m16n8k16 for the 8-channel ones
+// and as an alternative), trained with Adam on fp32 master weights.
 // No counterpart in the reference; its judge is the plain fine solver (ShallowWater.kernel).
 //
 // Layouts (per sample, row-major cells, channels innermost):
@@ -70,11 +71,11 @@ cudaError_t launch_wgrad(int cin, int cout, int grid, const WgradArgs& a, cudaSt
 size_t conv_smem(int cin, int cout, bool rows);
 size_t wgrad_smem(int cin, int cout);
 
-// The same convolutions on tcgen05 (cnn_umma.cu): 128 threads, conv_umma_smem_for bytes of dynamic shared memory,
-// a persistent grid; a bounded wait that expires sets ST_TIMEOUT in *status.
-const void* conv_umma_kernel(int cin, int cout, int mode);
-size_t conv_umma_smem_for(int cin, int cout);
-cudaError_t launch_conv_umma(int cin, int cout, int mode, int grid, const ConvArgs& a, uint32_t* status,
-                             cudaStream_t s);
+// The 32-input-channel convolutions (cout, mode) = (32, RELU), (8, LINEAR), (32, GRAD_MASK) on tcgen05 with
+// warp-specialised roles (cnn_tc.cu): TMA into a ring of input rows, one MMA-issuing thread, four epilogue warps;
+// 192 threads, one CTA per SM (conv_tc_smem bytes); the launch builds the input's tensor map.
+const void* conv_tc_kernel(int cout, int mode);
+size_t conv_tc_smem(int cout);
+cudaError_t launch_conv_tc(int cout, int mode, const ConvArgs& a, uint32_t* status, cudaStream_t s);
 
 }  // namespace vf

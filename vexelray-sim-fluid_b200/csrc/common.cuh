@@ -1,6 +1,7 @@
 // common.cuh -- status handling, device helpers and shared constants of libvexfluid.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -40,6 +41,13 @@ const char* last_error();
 int32_t require_device();
 // Number of SMs on the current device (148 on B200); cached.
 int sm_count();
+
+// cuTensorMapEncodeTiled from the driver (through the runtime's entry-point query, so the library needs no
+// -lcuda); null when the driver does not offer it.
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled tensor_map_encoder();
 
 // Device status word bits, set by kernels' own bounds checks (never a trap).
 enum : uint32_t {

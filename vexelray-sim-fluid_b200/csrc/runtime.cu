@@ -53,6 +53,21 @@ int sm_count() {
     return cached;
 }
 
+EncodeTiled tensor_map_encoder() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)p;
+        cudaGetLastError();
+    }
+    return fn;
+}
+
 // ------------------------------------------------------------------ profiler
 
 Profiler::~Profiler() {

@@ -431,29 +431,11 @@ __global__ void __launch_bounds__(256) k_swe_diag(const float* h, const float* h
     if (threadIdx.x == 0) parts[blockIdx.x] = sp[0];
 }
 
-typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled encode_fn() {
-    static EncodeTiled fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiled)p;
-        cudaGetLastError();
-    }
-    return fn;
-}
 
 // A 2D tensor map over one nx x ny f32 field with an hx x hy box; false if TMA cannot take it
 // (row pitch not a multiple of 16 bytes, or an unaligned base).
 bool make_map(CUtensorMap* m, const float* base, int nx, int ny, int hx, int hy) {
-    EncodeTiled enc = encode_fn();
+    EncodeTiled enc = tensor_map_encoder();
     if (!enc) return false;
     if (((uintptr_t)base & 15) || ((int64_t)nx * 4) % 16 != 0) return false;
     cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
