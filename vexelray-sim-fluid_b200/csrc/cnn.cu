@@ -170,8 +170,7 @@ struct vf_cnn {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t adam_steps = 0;
     bool predicted = false;   // y3 holds a prediction not yet applied
-    int path = 0;             // the convolutions: 0 tcgen05 (32 input channels; 8: as 1), 1 mma.sync row-blocked,
-                              // 2 mma.sync one row per warp
+    int path = 0;             // the convolutions: 0 tcgen05, 1 mma.sync row-blocked, 2 mma.sync one row per warp
     int grid_conv[2][5] = {{0}}, grid_wgrad[3] = {0};
     DeviceBuffer status;
     Profiler prof;
@@ -198,7 +197,7 @@ int32_t conv(vf_cnn* h, const char* name, int cin, int cout, int mode, const bf1
     ConvArgs a{in, w, bias, bias_n, out_b, out_f, mask, h->ny, h->nx, nb};
     h->prof.begin(name, h->stream);
     const int k = conv_index(cin, cout, mode);
-    cudaError_t e = h->path == 0 && cin == 32 ? launch_conv_tc(cout, mode, a, h->status.as<uint32_t>(), h->stream)
+    cudaError_t e = h->path == 0   ? launch_conv_tc(cin, cout, mode, a, h->status.as<uint32_t>(), h->stream)
                     : h->path == 2            ? launch_conv(cin, cout, mode, false, h->grid_conv[1][k], a, h->stream)
                                               : launch_conv(cin, cout, mode, true, h->grid_conv[0][k], a, h->stream);
     h->prof.end(h->stream);
@@ -354,12 +353,10 @@ int32_t vf_cnn_create(int32_t nx, int32_t ny, int32_t batch, int32_t samples, fl
         (is_conv ? h->grid_conv[rows ? 0 : 1][c] : h->grid_wgrad[k - 10]) = std::max(per, 1) * sm_count();
     }
     for (int k = 0; k < 5; k++) {
-        if (modes[k][0] != 32) continue;
-        const void* fn = conv_tc_kernel(modes[k][1], modes[k][2]);
-        if (!fn || cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_tc_smem(modes[k][1])) !=
-                       cudaSuccess) {
-            set_error("cannot give a tensor-core convolution %zu bytes of shared memory",
-                      conv_tc_smem(modes[k][1]));
+        const void* fn = conv_tc_kernel(modes[k][0], modes[k][1], modes[k][2]);
+        const size_t smem = conv_tc_smem(modes[k][0], modes[k][1]);
+        if (!fn || cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            set_error("cannot give a tensor-core convolution %zu bytes of shared memory", smem);
             return fail(VF_ECUDA);
         }
     }

@@ -71,11 +71,11 @@ cudaError_t launch_wgrad(int cin, int cout, int grid, const WgradArgs& a, cudaSt
 size_t conv_smem(int cin, int cout, bool rows);
 size_t wgrad_smem(int cin, int cout);
 
-// The 32-input-channel convolutions (cout, mode) = (32, RELU), (8, LINEAR), (32, GRAD_MASK) on tcgen05 with
-// warp-specialised roles (cnn_tc.cu): TMA into a ring of input rows, one MMA-issuing thread, four epilogue warps;
-// 192 threads, one CTA per SM (conv_tc_smem bytes); the launch builds the input's tensor map.
-const void* conv_tc_kernel(int cout, int mode);
-size_t conv_tc_smem(int cout);
-cudaError_t launch_conv_tc(int cout, int mode, const ConvArgs& a, uint32_t* status, cudaStream_t s);
+// The convolutions on tcgen05 with warp-specialised roles (cnn_tc.cu): TMA into a ring of input rows, one
+// MMA-issuing thread, eight epilogue warps; (cin, cout, mode) as conv_kernel's; 320 threads, one CTA per SM
+// (conv_tc_smem bytes); the launch builds the input's tensor map.
+const void* conv_tc_kernel(int cin, int cout, int mode);
+size_t conv_tc_smem(int cin, int cout);
+cudaError_t launch_conv_tc(int cin, int cout, int mode, const ConvArgs& a, uint32_t* status, cudaStream_t s);
 
 }  // namespace vf
