@@ -147,20 +147,19 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 
 // ------------------------------------------------------------------ P2G: sorted brick tile
 
-// Each warp takes work units of (non-empty brick, slab of 8 x 4 x 1 cells), sixteen per brick, with no
-// barrier between warps.
+// Each warp takes work units of (non-empty brick, 8 x 8 x 2 cells), four per brick, with no barrier between warps.
 //
-//  1. Lane l owns cell (l % 8, l / 8) of the slab. A slab's cells are 32 consecutive keys, so their
-//     particle runs form one contiguous range of the sort's permutation: the warp stages it in shared
-//     memory, each lane puts its cell's run in ascending order there (the stable sort's fix-up, fused
-//     here: G2P then reads the stable permutation), and the warp writes the range back. The lane then sums
-//     the 27 x 4 deposits of its cell's particles in registers, loading two particles ahead of the one it
-//     sums.
-//  2. The slab's deposits reach a 10 x 6 x 3 node window, private to the warp in shared memory. At one
-//     stencil offset the 32 lanes hit 32 different nodes, so the window takes the cell sums by plain
-//     read-modify-write, a __syncwarp between offsets: no shared-memory atomics.
+//  1. A unit's 128 cells are consecutive keys, so their particle runs form one contiguous range of the sort's
+//     permutation. The warp stages it in shared memory, puts each cell's run in ascending order there (the stable
+//     sort's fix-up, fused here: G2P then reads the stable permutation), and writes the range back.
+//  2. Cells are dealt to lanes from a queue ordered by particle count, largest first: a lane sums one whole cell's
+//     27 x 4 deposits in registers (loading two particles ahead), adds them into the warp's 10 x 10 x 4 node
+//     window in shared memory when the cell is done, and takes the next cell. A cell's count varies (about
+//     8 +- 2.6 at 8 per cell), so one fixed cell per lane left half the lanes idle behind each warp's fullest cell;
+//     the queue keeps them busy. Lanes that finish together add at the same stencil offset into distinct cells'
+//     distinct nodes, so the window takes plain read-modify-writes, a warp sync between offsets.
 //  3. The warp reduces every touched node of its window into the grid with one 16-byte vector
-//     reduction (red.global.add.v4.f32); neighbouring slabs' windows overlap, and the reductions add.
+//     reduction (red.global.add.v4.f32); neighbouring units' windows overlap, and the reductions add.
 //
 // The per-particle arithmetic is Flip3.scatter's regrouped so a node costs a weight, one mass FMA and
 // three momentum FMAs:  momentum_a(node o) = w(o) (A_a + sum_e B_ae o_e),
@@ -168,13 +167,20 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 // which is (w m)(v_a + C_a . d) + w s d_a with d = o - f (Flip3.java:225-243).
 constexpr int P2G_THREADS = 128;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
-constexpr int WWX = WIN, WWY = 6, WWZ = 3, WW = WWX * WWY * WWZ;   // a warp's window: 180 nodes
-
-constexpr int RUN_CAP = 768;   // particle slots of one slab staged in shared memory (more: sorted in place)
+constexpr int UZ = 2;                                      // brick z-layers per work unit
+constexpr int UCELLS = BRICK * BRICK * UZ;                 // 128 cells
+constexpr int UPB = BRICK / UZ;                            // units per brick
+constexpr int WWX = WIN, WWY = WIN, WWZ = UZ + 2, WW = WWX * WWY * WWZ;   // a warp's window: 400 nodes
+constexpr int RUN_CAP = 2048;   // particle slots of one unit staged in shared memory (more: sorted in place)
+constexpr int NBUCKET = 32;     // count buckets of the cell queue (counts of 31 and more share the last)
 
 struct P2GShared {
     float4 wwin[P2G_WARPS][WW];
-    int run[P2G_WARPS][RUN_CAP];   // the slab's run of the permutation, sorted per cell here
+    int run[P2G_WARPS][RUN_CAP];         // the unit's range of the permutation, sorted per cell here
+    int start[P2G_WARPS][UCELLS + 1];    // cell c's particles: [start[c], start[c + 1])
+    unsigned char order[P2G_WARPS][UCELLS];   // non-empty cells by descending count
+    int bucket[P2G_WARPS][NBUCKET];
+    int next[P2G_WARPS];                 // the queue's head
 };
 constexpr size_t P2G_SMEM = sizeof(P2GShared);
 // One particle's fields, as the scatter reads them.
@@ -215,135 +221,207 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
     const int64_t st = s.stride;
     const float* __restrict__ in = s.in;
     int* __restrict__ perm = s.perm;
+    const unsigned ALL = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int lx = lane & 7, lyl = lane >> 3;
     float4* ww = S.wwin[warp];
-    const int units = *s.n_active * 16;
+    int* cstart = S.start[warp];
+    unsigned char* order = S.order[warp];
+    int* bucket = S.bucket[warp];
+    const int units = *s.n_active * UPB;
     const int total_warps = gridDim.x * P2G_WARPS;
     for (int u = blockIdx.x * P2G_WARPS + warp; u < units; u += total_warps) {
-        const int b = s.active[u >> 4], q = u & 15;
+        const int b = s.active[u / UPB], lz0 = (u % UPB) * UZ;
         const int bx = b % dm.nbx, by = (b / dm.nbx) % dm.nby, bz = b / (dm.nbx * dm.nby);
-        const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK;
+        const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK + lz0;
         int bs = s.brick_start[b], be = s.brick_start[b + 1];
         if (bs < 0 || be > s.np || be < bs) {
             set_status(s.status, ST_OOB);
             bs = max(bs, 0);
             be = min(max(be, bs), s.np);
         }
-        const int lz = q >> 1, ly0 = (q & 1) * 4, ly = ly0 + lyl;
-        const int c = (lz * 8 + ly) * 8 + lx;
-        const int64_t key = (int64_t)b * 512 + c;
-        const int s0 = min(max(s.cell_start[key], bs), be);
-        const int s1 = min(max(c < 511 ? s.cell_start[key + 1] : be, s0), be);
-        if (!__any_sync(0xffffffffu, s1 > s0)) continue;          // an empty slab (warp-uniform)
+        // the unit's cell starts (clamped into the brick and made non-decreasing)
+        const int64_t key0 = (int64_t)b * 512 + lz0 * 64;
+        for (int c = lane; c <= UCELLS; c += 32) {
+            int v = (c < UCELLS || lz0 + UZ < BRICK) ? s.cell_start[key0 + c] : be;
+            if (v < bs || v > be) {
+                set_status(s.status, ST_OOB);
+                v = min(max(v, bs), be);
+            }
+            cstart[c] = v;
+        }
+        __syncwarp();
+        // a prefix maximum keeps the runs ordered even if the starts were not
+        int carry = bs;
+        for (int c0 = 0; c0 <= UCELLS; c0 += 32) {
+            const int c = c0 + lane;
+            int v = c <= UCELLS ? cstart[c] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(ALL, v, o);
+                if (lane >= o) v = max(v, y);
+            }
+            v = max(v, carry);
+            if (c <= UCELLS) cstart[c] = v;
+            carry = __shfl_sync(ALL, v, 31);
+        }
+        __syncwarp();
+        const int S0 = cstart[0], S1 = cstart[UCELLS];
+        if (S1 == S0) continue;   // an empty unit (warp-uniform)
 
-        // 1. the stable order of this cell's run, then its particles summed in registers. The slab's 32 runs are
-        //    one range [S0, S1): staged in the warp's shared memory, each lane sorts its run there and the warp
-        //    writes the range back, coalesced (in place in global memory when it does not fit).
-        const int S0 = __shfl_sync(0xffffffffu, s0, 0), S1 = __shfl_sync(0xffffffffu, s1, 31);
-        const bool staged = __all_sync(0xffffffffu, s0 >= S0 && s1 <= S1) && S1 - S0 <= RUN_CAP;
+        // 1. the unit's range staged, each cell's run sorted there, written back
+        const bool staged = S1 - S0 <= RUN_CAP;
         int* rs = S.run[warp];
         if (staged) {
             for (int j = S0 + lane; j < S1; j += 32) rs[j - S0] = perm[j];
             __syncwarp();
-            if (s1 - s0 > 1) insertion_sort_run(rs + (s0 - S0), s1 - s0);
+            for (int c = lane; c < UCELLS; c += 32)
+                if (cstart[c + 1] - cstart[c] > 1) insertion_sort_run(rs + (cstart[c] - S0), cstart[c + 1] - cstart[c]);
             __syncwarp();
             for (int j = S0 + lane; j < S1; j += 32) perm[j] = rs[j - S0];
-        } else if (s1 - s0 > 1) {
-            insertion_sort_run(perm + s0, s1 - s0);
+        } else {
+            for (int c = lane; c < UCELLS; c += 32)
+                if (cstart[c + 1] - cstart[c] > 1) insertion_sort_run(perm + cstart[c], cstart[c + 1] - cstart[c]);
         }
-        const int* run = staged ? rs : perm + S0;   // the run, indexed from S0
+        const int* run = staged ? rs : perm + S0;   // the range, indexed from S0
+
+        // the queue: non-empty cells bucketed by count, largest first
+        bucket[lane] = 0;
+        for (int j = lane; j < WW; j += 32) ww[j] = make_float4(0, 0, 0, 0);
+        __syncwarp();
+        for (int c = lane; c < UCELLS; c += 32) {
+            const int n = cstart[c + 1] - cstart[c];
+            if (n > 0) atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1);
+        }
+        __syncwarp();
+        {
+            int v = bucket[lane], x = v;   // exclusive scan over the buckets (largest counts first)
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(ALL, x, o);
+                if (lane >= o) x += y;
+            }
+            bucket[lane] = x - v;
+            if (lane == 31) S.next[warp] = x;   // the number of non-empty cells, for now
+        }
+        __syncwarp();
+        const int ncells = S.next[warp];
+        for (int c = lane; c < UCELLS; c += 32) {
+            const int n = cstart[c + 1] - cstart[c];
+            if (n > 0) order[atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1)] = (unsigned char)c;
+        }
+        __syncwarp();
+        if (lane == 0) S.next[warp] = 32;
+        __syncwarp();
+
+        // 2. cells from the queue, summed in registers, added into the window when done
         float acc[27][4];
 #pragma unroll
         for (int k = 0; k < 27; k++) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+        int cell = lane < ncells ? order[lane] : -1;
+        int i = 0, end = 0;
         PIn nxt, nxt2;
-        if (s0 < s1) load_pin(nxt, in, st, checked_src(run, s0 - S0, s.np, s.status));
-        if (s0 + 1 < s1) load_pin(nxt2, in, st, checked_src(run, s0 + 1 - S0, s.np, s.status));
-        for (int i = s0; i < s1; i++) {
-            const PIn qq = nxt;
-            nxt = nxt2;
-            if (i + 2 < s1) load_pin(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
-            if (!(qq.m > 0.0f)) continue;
-            int cell[3];
-            float f[3];
-            stencil_axis(qq.x, dm.nx, cell[0], f[0]);
-            stencil_axis(qq.y, dm.ny, cell[1], f[1]);
-            stencil_axis(qq.z, dm.nz, cell[2], f[2]);
-            if (cell[0] != cx0 + lx || cell[1] != cy0 + ly || cell[2] != cz0 + lz) {
-                set_status(s.status, ST_OOB);
-                continue;
-            }
-            float wx[3], wy[3], wz[3];
+        auto open = [&]() {   // the lane's new cell: its range and the first two particles in flight
+            i = cstart[cell];
+            end = cstart[cell + 1];
+            load_pin(nxt, in, st, checked_src(run, i - S0, s.np, s.status));
+            if (i + 1 < end) load_pin(nxt2, in, st, checked_src(run, i + 1 - S0, s.np, s.status));
+        };
+        if (cell >= 0) open();
+        while (__any_sync(ALL, cell >= 0)) {
+            if (cell >= 0 && i < end) {
+                const PIn qq = nxt;
+                nxt = nxt2;
+                if (i + 2 < end) load_pin(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
+                i++;
+                int cl[3];
+                float f[3];
+                stencil_axis(qq.x, dm.nx, cl[0], f[0]);
+                stencil_axis(qq.y, dm.ny, cl[1], f[1]);
+                stencil_axis(qq.z, dm.nz, cl[2], f[2]);
+                const bool mine = cl[0] == cx0 + (cell & 7) && cl[1] == cy0 + ((cell >> 3) & 7) && cl[2] == cz0 + (cell >> 6);
+                if (!mine) set_status(s.status, ST_OOB);
+                if (mine && qq.m > 0.0f) {
+                    float wx[3], wy[3], wz[3];
 #pragma unroll
-            for (int e = 0; e < 3; e++) {
-                float* we = e == 0 ? wx : e == 1 ? wy : wz;
-                const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
-                we[0] = 0.5f * (ta * ta);
-                we[1] = 0.75f - tc * tc;
-                we[2] = 0.5f * (te * te);
-            }
-            float jp;
-            if (p.tait) {
-                const float r = __frcp_rn(qq.j), r2 = r * r;
-                jp = p.bulk * ((r2 * r2) * r2 - qq.j);
-            } else {
-                jp = p.bulk * (1.0f - qq.j);
-            }
-            const float sp = (k4dt * (qq.m * vol)) * jp;
-            const float vel[3] = {qq.u, qq.v, qq.w};
-            float A[3], B[3][3];
+                    for (int e = 0; e < 3; e++) {
+                        float* we = e == 0 ? wx : e == 1 ? wy : wz;
+                        const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
+                        we[0] = 0.5f * (ta * ta);
+                        we[1] = 0.75f - tc * tc;
+                        we[2] = 0.5f * (te * te);
+                    }
+                    float jp;
+                    if (p.tait) {
+                        const float r = __frcp_rn(qq.j), r2 = r * r;
+                        jp = p.bulk * ((r2 * r2) * r2 - qq.j);
+                    } else {
+                        jp = p.bulk * (1.0f - qq.j);
+                    }
+                    const float sp = (k4dt * (qq.m * vol)) * jp;
+                    const float vel[3] = {qq.u, qq.v, qq.w};
+                    float A[3], B[3][3];
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-                const float c0 = qq.c[3 * r], c1 = qq.c[3 * r + 1], c2 = qq.c[3 * r + 2];
-                A[r] = qq.m * (vel[r] - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[r];
-                B[r][0] = qq.m * c0;
-                B[r][1] = qq.m * c1;
-                B[r][2] = qq.m * c2;
-                B[r][r] += sp;
-            }
+                    for (int r = 0; r < 3; r++) {
+                        const float c0 = qq.c[3 * r], c1 = qq.c[3 * r + 1], c2 = qq.c[3 * r + 2];
+                        A[r] = qq.m * (vel[r] - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[r];
+                        B[r][0] = qq.m * c0;
+                        B[r][1] = qq.m * c1;
+                        B[r][2] = qq.m * c2;
+                        B[r][r] += sp;
+                    }
 #pragma unroll
-            for (int oz = 0; oz < 3; oz++) {
+                    for (int oz = 0; oz < 3; oz++) {
 #pragma unroll
-                for (int oy = 0; oy < 3; oy++) {
-                    const float wyz = wy[oy] * wz[oz];
-                    const float mw = qq.m * wyz;
-                    float T[3];
+                        for (int oy = 0; oy < 3; oy++) {
+                            const float wyz = wy[oy] * wz[oz];
+                            const float mw = qq.m * wyz;
+                            float T[3];
 #pragma unroll
-                    for (int r = 0; r < 3; r++) T[r] = A[r] + (float)oy * B[r][1] + (float)oz * B[r][2];
+                            for (int r = 0; r < 3; r++) T[r] = A[r] + (float)oy * B[r][1] + (float)oz * B[r][2];
 #pragma unroll
-                    for (int ox = 0; ox < 3; ox++) {
-                        const int k = (oz * 3 + oy) * 3 + ox;
-                        const float w = wx[ox] * wyz;
-                        acc[k][0] += wx[ox] * mw;
+                            for (int ox = 0; ox < 3; ox++) {
+                                const int k = (oz * 3 + oy) * 3 + ox;
+                                const float w = wx[ox] * wyz;
+                                acc[k][0] += wx[ox] * mw;
 #pragma unroll
-                        for (int r = 0; r < 3; r++) acc[k][1 + r] += w * (T[r] + (float)ox * B[r][0]);
+                                for (int r = 0; r < 3; r++) acc[k][1 + r] += w * (T[r] + (float)ox * B[r][0]);
+                            }
+                        }
                     }
                 }
             }
-        }
-
-        // 2. into the warp's window (__syncwarp orders each offset's writes before the next's reads)
-        __syncwarp();
-        for (int j = lane; j < WW; j += 32) ww[j] = make_float4(0, 0, 0, 0);
-        __syncwarp();
+            const bool done = cell >= 0 && i >= end;
+            const unsigned fm = __ballot_sync(ALL, done);
+            if (done) {
+                // into the window: lanes flushing together hold distinct cells, so at one stencil offset they
+                // write distinct nodes
+                const int wb = ((cell >> 6) * WWY + ((cell >> 3) & 7)) * WWX + (cell & 7);
 #pragma unroll
-        for (int k = 0; k < 27; k++) {
-            const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
-            const int wi = (oz * WWY + lyl + oy) * WWX + lx + ox;
-            float4 v = ww[wi];
-            v.x += acc[k][0];
-            v.y += acc[k][1];
-            v.z += acc[k][2];
-            v.w += acc[k][3];
-            ww[wi] = v;
-            __syncwarp();
+                for (int k = 0; k < 27; k++) {
+                    const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
+                    const int wi = wb + (oz * WWY + oy) * WWX + ox;
+                    float4 v = ww[wi];
+                    v.x += acc[k][0];
+                    v.y += acc[k][1];
+                    v.z += acc[k][2];
+                    v.w += acc[k][3];
+                    ww[wi] = v;
+                    acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+                    __syncwarp(fm);
+                }
+                const int pos = atomicAdd(&S.next[warp], 1);
+                cell = pos < ncells ? order[pos] : -1;
+                if (cell >= 0) open();
+            }
+            __syncwarp();   // this iteration's window writes before the next iteration's reads
         }
+        __syncwarp();
 
         // 3. the window's touched nodes into the grid
         for (int j = lane; j < WW; j += 32) {
             const float4 t = ww[j];
             if (t.x == 0.0f && t.y == 0.0f && t.z == 0.0f && t.w == 0.0f) continue;
-            const int gx = cx0 + j % WWX, gy = cy0 + ly0 + (j / WWX) % WWY, gz = cz0 + lz + j / (WWX * WWY);
+            const int gx = cx0 + j % WWX, gy = cy0 + (j / WWX) % WWY, gz = cz0 + j / (WWX * WWY);
             if (gx >= dm.nx || gy >= dm.ny || gz >= dm.nz) {
                 set_status(s.status, ST_OOB);
                 continue;
