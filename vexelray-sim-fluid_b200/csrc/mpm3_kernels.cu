@@ -314,9 +314,9 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
         __syncwarp();
 
         // 2. cells from the queue, summed in registers, added into the window when done
-        float acc[27][4];
+        float2 acc01[27], acc23[27];   // per node (mass, x-momentum) and (y-, z-momentum)
 #pragma unroll
-        for (int k = 0; k < 27; k++) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+        for (int k = 0; k < 27; k++) acc01[k] = acc23[k] = make_float2(0.0f, 0.0f);
         int cell = lane < ncells ? order[lane] : -1;
         int i = 0, end = 0;
         PIn nxt, nxt2;
@@ -369,22 +369,47 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
                         B[r][2] = qq.m * c2;
                         B[r][r] += sp;
                     }
+                    // paired fp32 (FFMA2): a node's (mass, x-momentum) += wx (m wyz, wyz M_x) and (y-, z-momentum)
+                    // += wx (wyz M_y, wyz M_z), M_a = T_a + ox B_a0, T_a = A_a + oy B_a1 + oz B_a2; the mass lane
+                    // rides along with zero coefficients
+                    const float2 c01 = make_float2(qq.m, A[0]), c23 = make_float2(A[1], A[2]);
+                    const float2 b0_01 = make_float2(0.0f, B[0][0]), b0_23 = make_float2(B[1][0], B[2][0]);
+                    const float2 b1_01 = make_float2(0.0f, B[0][1]), b1_23 = make_float2(B[1][1], B[2][1]);
+                    const float2 b2_01 = make_float2(0.0f, B[0][2]), b2_23 = make_float2(B[1][2], B[2][2]);
 #pragma unroll
                     for (int oz = 0; oz < 3; oz++) {
 #pragma unroll
                         for (int oy = 0; oy < 3; oy++) {
                             const float wyz = wy[oy] * wz[oz];
-                            const float mw = qq.m * wyz;
-                            float T[3];
-#pragma unroll
-                            for (int r = 0; r < 3; r++) T[r] = A[r] + (float)oy * B[r][1] + (float)oz * B[r][2];
+                            const float2 w2 = make_float2(wyz, wyz);
+                            float2 t01 = c01, t23 = c23;
+                            if (oy) {
+                                const float2 f2 = make_float2((float)oy, (float)oy);
+                                t01 = __ffma2_rn(f2, b1_01, t01);
+                                t23 = __ffma2_rn(f2, b1_23, t23);
+                            }
+                            if (oz) {
+                                const float2 f2 = make_float2((float)oz, (float)oz);
+                                t01 = __ffma2_rn(f2, b2_01, t01);
+                                t23 = __ffma2_rn(f2, b2_23, t23);
+                            }
+                            const float2 g01 = __fmul2_rn(w2, t01), g23 = __fmul2_rn(w2, t23);
+                            const float2 h01 = __fmul2_rn(w2, b0_01), h23 = __fmul2_rn(w2, b0_23);
 #pragma unroll
                             for (int ox = 0; ox < 3; ox++) {
-                                const int k = (oz * 3 + oy) * 3 + ox;
-                                const float w = wx[ox] * wyz;
-                                acc[k][0] += wx[ox] * mw;
-#pragma unroll
-                                for (int r = 0; r < 3; r++) acc[k][1 + r] += w * (T[r] + (float)ox * B[r][0]);
+                                const int kk = (oz * 3 + oy) * 3 + ox;
+                                float2 q01 = g01, q23 = g23;
+                                if (ox == 1) {
+                                    q01 = __fadd2_rn(q01, h01);
+                                    q23 = __fadd2_rn(q23, h23);
+                                } else if (ox == 2) {
+                                    const float2 two = make_float2(2.0f, 2.0f);
+                                    q01 = __ffma2_rn(two, h01, q01);
+                                    q23 = __ffma2_rn(two, h23, q23);
+                                }
+                                const float2 x2 = make_float2(wx[ox], wx[ox]);
+                                acc01[kk] = __ffma2_rn(x2, q01, acc01[kk]);
+                                acc23[kk] = __ffma2_rn(x2, q23, acc23[kk]);
                             }
                         }
                     }
@@ -401,12 +426,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
                     const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
                     const int wi = wb + (oz * WWY + oy) * WWX + ox;
                     float4 v = ww[wi];
-                    v.x += acc[k][0];
-                    v.y += acc[k][1];
-                    v.z += acc[k][2];
-                    v.w += acc[k][3];
+                    v.x += acc01[k].x;
+                    v.y += acc01[k].y;
+                    v.z += acc23[k].x;
+                    v.w += acc23[k].y;
                     ww[wi] = v;
-                    acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+                    acc01[k] = acc23[k] = make_float2(0.0f, 0.0f);
                     __syncwarp(fm);
                 }
                 const int pos = atomicAdd(&S.next[warp], 1);
