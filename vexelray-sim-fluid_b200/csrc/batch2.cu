@@ -97,8 +97,13 @@ constexpr int BATCH_MAX_THREADS = 512;
 constexpr int NPHASE = 5;         // tile scan, cell scan, permute, scatter, gather
 constexpr int CHUNK = 1024;       // particles of a work item of the scatter and gather: a tile's run in chunks
 // Shared memory of one warp of the step: its node window (m, mu, mv arrays of the largest tile's window; the
-// gather reuses it for float2 velocities).
-__host__ __device__ constexpr int warp_smem_floats(int wmax) { return 3 * wmax; }
+// gather reuses it for float2 velocities), then the scatter's cell queue: per cell of a tile (at most QCELLS) its
+// particles' range within the chunk, the non-empty cells by descending count, count buckets, the queue's head.
+constexpr int QCELLS = 512;                // cells of the largest tile (32 x 16)
+constexpr int QBUCKETS = 32;               // count buckets (31 particles and more share the last)
+constexpr int QWORDS = 2 * QCELLS + QCELLS / 2 + QBUCKETS + 4;   // a multiple of 4 words
+__host__ __device__ constexpr int window_words(int wmax) { return (3 * wmax + 3) & ~3; }   // 16-byte aligned
+__host__ __device__ constexpr int warp_smem_floats(int wmax) { return window_words(wmax) + QWORDS; }
 
 // One particle's fields as the scatter reads them (source slot < 0: none, zeros).
 struct Part2 {
@@ -324,15 +329,55 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             continue;
         }
         const int lt = t - sc.t0;
-        const int tx = sc.tx, ty = sc.ty, nx = sc.nx, ny = sc.ny;
+        const int tx = sc.tx, ty = sc.ty, nx = sc.nx, ny = sc.ny, tc = sc.tc;
         const int x0 = (lt % sc.ntx) * tx, y0 = (lt / sc.ntx) * ty;   // the tile's first cell = first node
         const int wx = tx + 2, wn = wx * (ty + 2);
         const Params2 prm = sc.prm;
+        int2* crange = reinterpret_cast<int2*>(ww + window_words(B.wmax));   // per cell: its particles in the chunk
+        unsigned short* order = reinterpret_cast<unsigned short*>(crange + QCELLS);
+        int* bucket = reinterpret_cast<int*>(order + QCELLS);
+        int* head = bucket + QBUCKETS;
         for (int j = lane; j < 3 * wn; j += 32) ww[j] = 0.0f;
+        bucket[lane] = 0;
         __syncwarp();
-        // software pipeline: the next batch's fields and the one after's source slots in flight
+        // the tile's cells (keys cb + j, j = ly * tx + lx; after the permute cursor[key] is the run's end) clipped
+        // to the chunk, and counted into the buckets
+        const int cb = sc.c0 + lt * tc;
+        if (tc > QCELLS) {
+            if (lane == 0) set_status(B.status, ST_OOB);
+            continue;
+        }
+        for (int j = lane; j < tc; j += 32) {
+            const int e = B.cursor[cb + j], b0 = j == 0 ? ts : B.cursor[cb + j - 1];
+            const int lo = max(b0, c0), hi = min(e, c1);
+            crange[j] = make_int2(lo, hi);
+            if (hi > lo) atomicAdd(&bucket[QBUCKETS - 1 - min(hi - lo, QBUCKETS - 1)], 1);
+        }
+        __syncwarp();
+        {
+            const int v = bucket[lane];
+            int x = v;   // exclusive scan over the buckets, largest counts first
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            bucket[lane] = x - v;
+            if (lane == 31) *head = x;
+        }
+        __syncwarp();
+        const int ncq = *head;   // non-empty cells
+        for (int j = lane; j < tc; j += 32) {
+            const int2 r = crange[j];
+            if (r.y > r.x) order[atomicAdd(&bucket[QBUCKETS - 1 - min(r.y - r.x, QBUCKETS - 1)], 1)] = (unsigned short)j;
+        }
+        __syncwarp();
+        if (lane == 0) *head = 32;
+        __syncwarp();
+        // cells dealt to lanes from the queue; a lane sums its cell's 27 amounts (Flip.scatter, Flip.java:269-303)
+        // over the cell's particles in registers and adds them into the window when the cell is done. Lanes that
+        // finish together hold distinct cells, so at one stencil offset they write distinct nodes.
         auto source = [&](int slot) {
-            if (slot >= c1) return -1;
             const int src = B.perm[slot];
             if (src < p0 || src >= p1) {
                 set_status(B.status, ST_OOB);
@@ -340,43 +385,53 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             }
             return src;
         };
-        Part2 cur, nxt;
-        int s_cur = source(c0 + lane);
-        load_part2(cur, in, st, s_cur);
-        int s_nxt = source(c0 + 32 + lane);
-        for (int b = c0; b < c1; b += 32) {
-            load_part2(nxt, in, st, s_nxt);
-            const int s_after = source(b + 64 + lane);
-            float amt[27];
+        float acc[27];
 #pragma unroll
-            for (int a = 0; a < 27; a++) amt[a] = 0.0f;
-            int key = -1;
-            if (s_cur >= 0) {
-                const Stencil2 sn = stencil2(cur.x, cur.y, nx, ny);
-                const int lx = sn.col - x0, ly = sn.row - y0;
-                if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
-                    const float sp = impulse_factor(prm.dt, cur.m, prm.rho0, prm.bulk, cur.j, prm.tait);
-                    scatter_amounts2(sn, cur.m, cur.u, cur.v, cur.c00, cur.c01, cur.c10, cur.c11, sp, amt);
-                    key = ly * wx + lx;   // the window index of the stencil's lower-left node
-                } else {
-                    set_status(B.status, ST_OOB);
+        for (int a = 0; a < 27; a++) acc[a] = 0.0f;
+        int cell = lane < ncq ? order[lane] : -1, i = 0, end = 0;
+        Part2 nxt;   // the lane's next particle in flight
+        auto open = [&]() {
+            const int2 r = crange[cell];
+            i = r.x;
+            end = r.y;
+            load_part2(nxt, in, st, source(i));
+        };
+        if (cell >= 0) open();
+        while (__any_sync(0xffffffffu, cell >= 0)) {
+            if (cell >= 0 && i < end) {
+                const Part2 cur = nxt;
+                if (i + 1 < end) load_part2(nxt, in, st, source(i + 1));
+                i++;
+                if (cur.m > 0.0f) {
+                    const Stencil2 sn = stencil2(cur.x, cur.y, nx, ny);
+                    if (sn.col == x0 + cell % tx && sn.row == y0 + cell / tx) {
+                        const float sp = impulse_factor(prm.dt, cur.m, prm.rho0, prm.bulk, cur.j, prm.tait);
+                        scatter_accumulate2(sn, cur.m, cur.u, cur.v, cur.c00, cur.c01, cur.c10, cur.c11, sp, acc);
+                    } else {
+                        set_status(B.status, ST_OOB);
+                    }
                 }
             }
-            const bool tail = segmented_sum<27>(amt, key) && key >= 0;
+            const bool done = cell >= 0 && i >= end;
+            const unsigned fm = __ballot_sync(0xffffffffu, done);
+            if (done) {
+                const int wb = (cell / tx) * wx + cell % tx;
 #pragma unroll
-            for (int o = 0; o < 9; o++) {
-                if (tail) {
-                    const int wi = key + (o / 3) * wx + o % 3;
-                    ww[wi] += amt[3 * o];
-                    ww[wn + wi] += amt[3 * o + 1];
-                    ww[2 * wn + wi] += amt[3 * o + 2];
+                for (int o = 0; o < 9; o++) {
+                    const int wi = wb + (o / 3) * wx + o % 3;
+                    ww[wi] += acc[3 * o];
+                    ww[wn + wi] += acc[3 * o + 1];
+                    ww[2 * wn + wi] += acc[3 * o + 2];
+                    acc[3 * o] = acc[3 * o + 1] = acc[3 * o + 2] = 0.0f;
+                    __syncwarp(fm);
                 }
-                __syncwarp();
+                const int pos = atomicAdd(head, 1);
+                cell = pos < ncq ? order[pos] : -1;
+                if (cell >= 0) open();
             }
-            cur = nxt;
-            s_cur = s_nxt;
-            s_nxt = s_after;
+            __syncwarp();   // this iteration's window writes before the next iteration's reads
         }
+        __syncwarp();
         for (int j = lane; j < wn; j += 32) {
             const float a = ww[j], bu = ww[wn + j], bv = ww[2 * wn + j];
             if (a == 0.0f && bu == 0.0f && bv == 0.0f) continue;

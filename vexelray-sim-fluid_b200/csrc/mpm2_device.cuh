@@ -76,6 +76,23 @@ __device__ __forceinline__ bool segmented_sum(float (&amt)[N], int key) {
     return lane == 31 || above != key;
 }
 
+// Flip.scatter's 27 amounts of one particle (Flip.java:269-303) added to acc (the same arithmetic as
+// scatter_amounts2, each amount formed and then added).
+__device__ __forceinline__ void scatter_accumulate2(const Stencil2& s, float m, float u, float w, float c00, float c01,
+                                                    float c10, float c11, float sp, float (&acc)[27]) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const float wgt = s.wx[k % 3] * s.wy[k / 3];
+        const float wm = wgt * m;
+        const float dx = (float)(k % 3) - s.fx, dy = (float)(k / 3) - s.fy;
+        const float velU = u + (c00 * dx + c01 * dy);
+        const float velV = w + (c10 * dx + c11 * dy);
+        acc[3 * k] += wm;
+        acc[3 * k + 1] += wm * velU + wgt * (sp * dx);
+        acc[3 * k + 2] += wm * velV + wgt * (sp * dy);
+    }
+}
+
 // Flip.scatter's 27 amounts of one particle (Flip.java:269-303): for stencil node k (k % 3 across,
 // k / 3 up), mass w m and the momentum w m (v + C d) + w s d, d = node - f.
 __device__ __forceinline__ void scatter_amounts2(const Stencil2& s, float m, float u, float w, float c00, float c01,
