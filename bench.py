@@ -37,6 +37,7 @@ PKG = ROOT / "vexelray-sim-fluid_b200"
 N3 = 256                    # grid nodes per axis, dx = 1/256
 PPC3 = 8                    # particles per cell
 BOX3 = ((0.05, 0.45), (0.05, 0.4325), (0.05, 0.45))   # 8.16M particles at 8 ppc (the config's "~8.2M")
+BOX3_LITERAL = ((0.05, 0.45), (0.05, 0.65), (0.05, 0.45))   # the literal box: 12,734,496 particles
 DT3 = 5e-5
 G_SI = 9.8
 SEED3 = 1
@@ -59,13 +60,13 @@ def package():
     return mod
 
 
-def dam3():
+def dam3(box=BOX3):
     """Seeded particles of the 3D config: every cell whose centre lies in the box, PPC3 jittered particles
     each (cell + U*0.999 per axis, as the reference's tests fill cells), z-major order."""
     n = N3
     rng = np.random.default_rng(SEED3)
     ranges = []
-    for lo, hi in BOX3:
+    for lo, hi in box:
         a, b = lo * n, hi * n
         c0 = math.ceil(a - 0.5)
         c1 = math.ceil(b - 0.5)
@@ -274,6 +275,105 @@ class Dist:
 
 # ---------------------------------------------------------------------------------------------- CPU side
 
+def c0_dam_break(seed=0):
+    """The 2D configuration: 128^2 nodes (dx = 1/128), 4 particles per cell jittered in every cell whose centre lies
+    in [0.05,0.55] x [0.05,0.30] (2048 cells: 8192 particles), still, m = 1/4; Tait k = 50 (50 n^2 in node
+    units), rho0 = 1, g = -9.8 m/s^2 (n nodes/s^2), dt = 1e-4, sticky walls 3 cells thick."""
+    n = 128
+    rng = np.random.default_rng(seed)
+    cx = np.arange(math.ceil(0.05 * n - 0.5), math.ceil(0.55 * n - 0.5), dtype=np.float32)
+    cy = np.arange(math.ceil(0.05 * n - 0.5), math.ceil(0.30 * n - 0.5), dtype=np.float32)
+    gy, gx = np.meshgrid(cy, cx, indexing="ij")
+    cells = np.repeat(np.stack([gx.ravel(), gy.ravel()], 1), 4, axis=0)
+    pos = (cells + rng.random(cells.shape, dtype=np.float32) * np.float32(0.999)).astype(np.float32)
+    x, y = np.ascontiguousarray(pos[:, 0]), np.ascontiguousarray(pos[:, 1])
+    return n, x, y, np.full(len(x), 0.25, np.float32), (1e-4, 0.0, -G_SI * n, K_TAIT * n * n, 1.0)
+
+
+def run_c0(args, vf, dist):
+    """The 2D configuration on the GPU (sorted every 10 steps, one scene per launch sequence) and the oracle's
+    step on one host core over the same scene."""
+    n, x, y, m, p = c0_dam_break()
+    params = vf.flip_params(*p)
+    steps = 1000
+    zeros = np.zeros_like(x)
+    with vf.ParticleSimulation(n, n, len(x), tait=True, sticky=WALL_BATCH) as s:
+        s.load(x, y, zeros, zeros, m, params)
+        s.advance(10, 10)
+        s.read("m")   # a blocking read: the device is idle
+        t0 = time.perf_counter()
+        s.advance(steps, 10)
+        s.read("m")
+        ms = 1e3 * (time.perf_counter() - t0)   # host clock: launches and the final read included
+    cpu = None
+    if not args.no_cpu and dist.rank == 0:
+        sys.path.insert(0, str(ROOT / "tests"))
+        from _oracle import Flip2State
+        o = Flip2State(n, n, x, y, m)
+        pw = np.array(params, np.float32)
+        t0, done = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 2.0:
+            if done % 10 == 0:
+                o.sort()
+            o.step(pw, (1, WALL_BATCH))
+            done += 1
+        el = time.perf_counter() - t0
+        cpu = {"value": len(x) * done / el, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+               "sample": f"{done} steps of the same scene, oracle C port of FlipStep.step, 1 thread, {el:.1f} s"}
+    return {"workload": "2D dam break 128^2 (config 0): 8192 particles, Tait k=50, sticky walls 3, dt 1e-4, sorted "
+                        "every 10 steps; host-clock time of 1000 steps (launch-bound at this size)",
+            "particles": len(x), "steps": steps, "ms_per_step": ms / steps,
+            "particle_steps_per_s": len(x) * steps / (ms / 1e3), "cpu_baseline": cpu}
+
+
+def cpu_swe_rate(h, budget_s=10.0):
+    """The oracle's shallow-water step (plain C, one thread) on the 4096^2 state: cell-updates/s."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _oracle import OracleSweBackend, Stepper, swe_params
+    n = N_SWE
+    z = np.zeros_like(h)
+    st = Stepper(OracleSweBackend(n, n, (0, 0, 0, 0)), n, n)
+    st.set(h, z, z, swe_params(9.81, 0.45, 1.0, 1.0, 1e-6), 1e9)
+    t0, done = time.perf_counter(), 0
+    while done < 1 or time.perf_counter() - t0 < budget_s:
+        st.step(1)
+        done += 1
+        if done >= 20:
+            break
+    el = time.perf_counter() - t0
+    return {"value": n * n * done / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{done} steps of the same 4096^2 state, oracle C port of ShallowWater.kernel, 1 thread, "
+                      f"{el:.1f} s"}
+
+
+def run_literal(args, vf):
+    """The 3D configuration's literal box, [0.05,0.65] in y: 12.9M particles, the same step, K device-timed steps."""
+    x, y, z, m, params = dam3(BOX3_LITERAL)
+    np3 = len(x)
+    zeros = np.zeros(np3, np.float32)
+    steps = min(args.steps, 50)
+    with vf.ParticleSimulation3(N3, N3, N3, np3) as sim:
+        sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params))
+        sim.advance(3)
+        sim.finish()
+        e0, e1 = vf.Event(), vf.Event()
+        e0.record(sim.stream())
+        sim.advance(steps)
+        e1.record(sim.stream())
+        ms = e0.elapsed_ms(e1)
+        sim.profile(True)
+        sim.advance(steps)
+        sim.finish()
+        prof = sim.profile_read()
+        sim.profile(False)
+        touched = sim.touched_nodes()
+    pg = sum(prof.get(k, (0.0, 1))[0] for k in ("k_p2g3_tile", "k_g2p3_tile")) / steps
+    return {"workload": "3D dam break, the config's literal box [0.05,0.45]x[0.05,0.65]x[0.05,0.45] at 8 per cell",
+            "particles": np3, "steps": steps, "ms_per_step": ms / steps,
+            "particle_steps_per_s": np3 * steps / (ms / 1e3), "p2g_g2p_ms_per_step": pg,
+            "p2g_g2p_hbm_frac": (152.0 * np3 + 28.0 * touched) / (pg / 1e3) / 1e9 / measured_peaks()[0]}
+
+
 def cpu_step_rate(x, y, z, m, params, budget_s=20.0, max_steps=3):
     """The oracle's threaded 3D step on the host cores over the full workload: particle-steps/s."""
     sys.path.insert(0, str(ROOT / "tests"))
@@ -401,6 +501,8 @@ def run_ours(args, dist: Dist):
            "h2d_bytes_per_step": 7 * np3 * 4 / args.steps, "d2h_bytes_per_step": 3 * np3 * 4 / args.steps,
            "job": f"load (7 fields) + {args.steps} steps + read x,y,z, one job per rank"}
     sim.close()
+    literal = None if args.no_literal else run_literal(args, vf)
+    c0 = None if args.no_c0 else run_c0(args, vf, dist)
 
     # shallow water, 4096^2 HLL, a sub-measurement (cells/s and its own roofline)
     swe = None
@@ -429,7 +531,8 @@ def run_ours(args, dist: Dist):
                "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
                "roofline": {"bound": "hbm", "achieved": 24.0 * cells / (k_ms / 1e3) / 1e9, "peak": peak,
                             "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
-                            "kernel": "k_swe_tile", "bytes_per_cell": 24}}
+                            "kernel": "k_swe_tile", "bytes_per_cell": 24},
+               "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
 
     batch = None if args.no_batch else run_batch(args, vf, dist, peak)
     learned = None if args.no_learned else run_learned(args, vf)
@@ -457,6 +560,8 @@ def run_ours(args, dist: Dist):
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "swe": swe,
+        "c0_2d": c0,
+        "literal_box": literal,
         "batch": batch,
         "learned": learned,
         "p2g_variants": variants,
@@ -476,9 +581,7 @@ def run_learned(args, vf):
     rows = []
     try:
         for seed in seeds:
-            plain = L.evaluate(None, report["fine"], seed, 2000, report["interval_ticks"])
-            lrn = L.evaluate(net, report["fine"], seed, 2000, report["interval_ticks"])
-            rows.append((plain, lrn))
+            rows.append(L.evaluate_pair(net, report["fine"], seed, 2000, report["interval_ticks"]))
         # the network's kernels, timed alone over a few corrections of the coarse grid
         with vf.PatchSimulation(report["coarse"], report["coarse"]) as c:
             h0 = L.restrict(L.bumps(3, report["fine"]))
@@ -501,10 +604,11 @@ def run_learned(args, vf):
         "workload": (f"learned coarse shallow water: fine {report['fine']}^2 HLL (16 bumps, the 4096^2 distribution "
                      f"halved in sigma and centres), coarse {report['coarse']}^2, correction every "
                      f"{report['interval_coarse_steps']} coarse steps ({report['interval_ticks']} ticks), "
-                     f"held-out seeds {seeds}, 2000 fine steps each"),
+                     f"held-out seeds {seeds[0]}..{seeds[-1]}, 2000 fine steps each"),
         "fine_cell_updates_per_s": mean("fine_cell_updates_per_s", 1),
         "learned_equivalent_cell_updates_per_s": mean("equivalent_fine_cell_updates_per_s", 1),
         "speedup_vs_fine": mean("speedup", 1),
+        "speedup_min_max": [float(min(r[1]["speedup"] for r in rows)), float(max(r[1]["speedup"] for r in rows))],
         "plain_coarse_speedup_vs_fine": mean("speedup", 0),
         "h_rms_error": {"learned": mean("h_rms_error", 1), "plain_coarse": mean("h_rms_error", 0),
                         "learned_max": float(max(r[1]["h_rms_error"] for r in rows))},
@@ -619,8 +723,10 @@ def main():
     ap.add_argument("--no-variants", action="store_true", help="skip the comparison of the three P2G schedules")
     ap.add_argument("--variant-steps", type=int, default=20)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes sub-measurement")
+    ap.add_argument("--no-literal", action="store_true", help="skip the 12.7M-particle literal-box sub-measurement")
+    ap.add_argument("--no-c0", action="store_true", help="skip the 2D configuration's sub-measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned shallow-water sub-measurement")
-    ap.add_argument("--learned-seeds", type=int, default=4)
+    ap.add_argument("--learned-seeds", type=int, default=64, help="held-out seeds of the learned evaluation")
     ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
                     help="the batched step's autotune cache (JSON)")
     args = ap.parse_args()

@@ -203,13 +203,9 @@ def generate_and_train(net: FluxNet, n_fine: int, seeds, *, pairs: int, spacing:
     return {"losses": losses, "seconds": time.perf_counter() - t0}
 
 
-def evaluate(net: FluxNet | None, n_fine: int, seed: int, fine_steps: int, interval: int, *,
-             threshold: float | None = None, tile: int = 64) -> dict:
-    """One held-out run: the fine solver for `fine_steps` steps, then the coarse solver (with the network, or plain
-    when net is None) over the same ticks from the restricted start; h's RMS error against the fine end state
-    restricted, and both runs' times (device work and host synchronisation, from the first dispatch to the end
-    state on the device)."""
-    nc = n_fine // 2
+def _fine_run(n_fine: int, seed: int, fine_steps: int):
+    """The fine solver for `fine_steps` steps from the seed's bumps: (start h, ticks spent, steps, seconds, the end
+    state's h restricted)."""
     h0 = bumps(seed, n_fine)
     z = np.zeros_like(h0)
     with PatchSimulation(n_fine, n_fine) as fine:
@@ -219,9 +215,14 @@ def evaluate(net: FluxNet | None, n_fine: int, seed: int, fine_steps: int, inter
         t0 = time.perf_counter()
         a = fine.advance(NEVER, fine_steps)
         t_fine = time.perf_counter() - t0
-        span = a.spent_ticks
         ref = restrict(fine.read()[0].reshape(n_fine, n_fine))
-    solver = LearnedShallowWater(nc, nc, net, interval, threshold=threshold, tile=tile)
+    return h0, a.spent_ticks, a.steps, t_fine, ref
+
+
+def _coarse_run(net: FluxNet | None, n_fine: int, seed: int, fine, interval: int, threshold, tile) -> dict:
+    h0, span, fine_steps, t_fine, ref = fine
+    z = np.zeros_like(h0)
+    solver = LearnedShallowWater(n_fine // 2, n_fine // 2, net, interval, threshold=threshold, tile=tile)
     try:
         solver.load_fine(h0, z, z)
         t0 = time.perf_counter()
@@ -231,8 +232,25 @@ def evaluate(net: FluxNet | None, n_fine: int, seed: int, fine_steps: int, inter
     finally:
         solver.close()
     err = float(np.sqrt(np.mean((h.astype(np.float64) - ref) ** 2)))
-    return {"seed": seed, "ticks": int(span), "fine_steps": int(a.steps), "coarse_steps": solver.steps,
+    return {"seed": seed, "ticks": int(span), "fine_steps": int(fine_steps), "coarse_steps": solver.steps,
             "corrections": solver.corrections, "fallback_tiles": solver.fallback_tiles, "h_rms_error": err,
             "fine_s": t_fine, "coarse_s": t_coarse, "speedup": t_fine / t_coarse,
-            "fine_cell_updates_per_s": n_fine * n_fine * a.steps / t_fine,
-            "equivalent_fine_cell_updates_per_s": n_fine * n_fine * a.steps / t_coarse}
+            "fine_cell_updates_per_s": n_fine * n_fine * fine_steps / t_fine,
+            "equivalent_fine_cell_updates_per_s": n_fine * n_fine * fine_steps / t_coarse}
+
+
+def evaluate(net: FluxNet | None, n_fine: int, seed: int, fine_steps: int, interval: int, *,
+             threshold: float | None = None, tile: int = 64) -> dict:
+    """One held-out run: the fine solver for `fine_steps` steps, then the coarse solver (with the network, or plain
+    when net is None) over the same ticks from the restricted start; h's RMS error against the fine end state
+    restricted, and both runs' times (device work and host synchronisation, from the first dispatch to the end
+    state on the device)."""
+    return _coarse_run(net, n_fine, seed, _fine_run(n_fine, seed, fine_steps), interval, threshold, tile)
+
+
+def evaluate_pair(net: FluxNet, n_fine: int, seed: int, fine_steps: int, interval: int, *,
+                  threshold: float | None = None, tile: int = 64) -> tuple[dict, dict]:
+    """evaluate(None, ...) and evaluate(net, ...) against one fine run: (plain, learned)."""
+    fine = _fine_run(n_fine, seed, fine_steps)
+    return (_coarse_run(None, n_fine, seed, fine, interval, threshold, tile),
+            _coarse_run(net, n_fine, seed, fine, interval, threshold, tile))
