@@ -42,7 +42,8 @@ DT3 = 5e-5
 G_SI = 9.8
 SEED3 = 1
 WORKLOAD3 = ("3D MLS-MPM APIC dam break, 256^3 nodes, dx=1/256, 8 particles/cell jittered from seed 1 in "
-             "[0.05,0.45]x[0.05,0.4325]x[0.05,0.45] (8,156,736 particles; the [0.05,0.65] y-extent gives 12.9M), "
+             "[0.05,0.45]x[0.05,0.4325]x[0.05,0.45] (8,156,736 particles; the literal [0.05,0.65] y-extent gives "
+             "12,734,496: literal_box), "
              "dt=5e-5, gravity -9.8 m/s^2, p=B(1/J-1) with B=(5 sqrt(2gH))^2, counting sort by stencil cell "
              "every step, sorted shared-memory-tile P2G")
 
@@ -347,7 +348,7 @@ def cpu_swe_rate(h, budget_s=10.0):
 
 
 def run_literal(args, vf):
-    """The 3D configuration's literal box, [0.05,0.65] in y: 12.9M particles, the same step, K device-timed steps."""
+    """The 3D configuration's literal box, [0.05,0.65] in y: 12,734,496 particles, the same step, K device-timed steps."""
     x, y, z, m, params = dam3(BOX3_LITERAL)
     np3 = len(x)
     zeros = np.zeros(np3, np.float32)
