@@ -466,8 +466,9 @@ def run_ours(args, dist: Dist):
     # the three P2G schedules the 3D config compares, each for K profiled steps from the same state
     variants = {}
     if not args.no_variants:
-        names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile"}
-        for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_TILE):
+        names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile",
+                 vf.VF_P2G_FIXED: "exact_fixed_point"}
+        for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_FIXED, vf.VF_P2G_TILE):
             sim.set_schedule(sched)
             sim.advance(2)
             sim.finish()
@@ -478,7 +479,7 @@ def run_ours(args, dist: Dist):
             v_ms = ev0.elapsed_ms(ev1)
             vp = sim.profile_read()
             sim.profile(False)
-            p2g = [k for k in vp if k.startswith("k_p2g3")]
+            p2g = [k for k in vp if k.startswith("k_p2g3") or k == "k_fixed_to_grid3"]
             variants[names[sched]] = {
                 "ms_per_step": v_ms / args.variant_steps,
                 "p2g_ms_per_step": sum(vp[k][0] for k in p2g) / args.variant_steps,

@@ -78,8 +78,11 @@ enum {
 enum {
     VF_P2G_TILE = 0,    /* sorted particles, one CTA per 8^3-cell brick, shared-memory window, vector red to HBM */
     VF_P2G_ATOMIC = 1,  /* one thread per particle, 27 vector atomics (Flip3.java:225-243's direct scatter) */
-    VF_P2G_WARP = 2     /* one thread per particle, runs of one cell summed across the warp first
+    VF_P2G_WARP = 2,    /* one thread per particle, runs of one cell summed across the warp first
                            (Scatter.segmentedDeposit, Scatter.java:385-439, over 27 nodes x 4 fields) */
+    VF_P2G_FIXED = 3    /* exact: every node amount quantized to 2^-40 and added with 64-bit integer atomics, so the
+                           grid is the same to the bit in any order and its total mass is the particles' quantized
+                           masses' sum exactly (the 3D form of FixedScatter.java:24-60, with 64-bit sums) */
 };
 
 /* ------------------------------------------------------------------ 2D particles (ParticleSimulation) */
@@ -250,6 +253,9 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
 void* vf_mpm3_stream(vf_mpm3* h);
 /* Change the scatter schedule (VF_P2G_*) between steps. */
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
+/* The last scatter's exact grid when it ran VF_P2G_FIXED (VF_ESTATE otherwise): field 0..3 = m, mu, mv, mw as
+ * int64 with 40 fractional bits, n = nx*ny*nz values. No counterpart in the reference. */
+int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n);
 /* Nodes with mass after the last scatter (N_t in the roofline's byte count). Blocking. */
 int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out);
 int64_t vf_mpm3_steps(const vf_mpm3* h);

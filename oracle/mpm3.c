@@ -103,6 +103,49 @@ void or_flip3_scatter(or_flip3* s, const float* params, or_physics ph) {   /* Fl
     }
 }
 
+/* The exact 3D scatter: the amounts of or_flip3_scatter (same operand order, no fused multiply-add), each
+ * quantized to 2^-40 (round to nearest even) and summed as int64, so the result does not depend on the order of
+ * the particles. The centre node (1,1,1) takes what the other 26 mass shares leave of the particle's quantized
+ * mass. The 3D form of FixedScatter (FixedScatter.java:24-60; 64-bit sums instead of its 32-bit ones). q holds
+ * four planes of nx*ny*nz values: m, mu, mv, mw; it is zeroed first. */
+static inline int64_t fixed3(float v) { return (int64_t)llrintf(v * 0x1p40f); }
+
+void or_fixed_scatter3(or_flip3* s, const float* params, or_physics ph, int64_t* q) {
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const size_t nodes = (size_t)nx * ny * nz;
+    const float dt = params[P_DT], bulk = params[P_BULK], rho0 = params[P_RHO0];
+    memset(q, 0, 4 * nodes * sizeof(int64_t));
+    for (int p = 0; p < s->np; p++) {
+        if (!(s->m[p] > 0.0f)) continue;
+        stencil3 st = stencil_of(s->x[p], s->y[p], s->z[p], nx, ny, nz);
+        float m = s->m[p];
+        float vel[3] = {s->u[p], s->v[p], s->w[p]};
+        float c[9];
+        for (int a = 0; a < 9; a++) c[a] = s->c[a][p];
+        float sp = impulse(dt, m, rho0, bulk, s->j[p], ph.eos);
+        int64_t rest = fixed3(m);
+        for (int k = 0; k < 27; k++) {
+            float wgt = weight_k(&st, k);
+            float d[3] = {(float)(k % 3) - st.off[0], (float)((k / 3) % 3) - st.off[1], (float)(k / 9) - st.off[2]};
+            float wm = wgt * m;
+            size_t node = (size_t)(st.base + offset_k(k, nx, ny));
+            if (k != 13) {
+                int64_t share = fixed3(wm);
+                rest -= share;
+                q[node] = (int64_t)((uint64_t)q[node] + (uint64_t)share);
+            }
+            for (int a = 0; a < 3; a++) {
+                float at3 = vel[a] + (c[3 * a] * d[0] + (c[3 * a + 1] * d[1] + c[3 * a + 2] * d[2]));
+                float push = sp * d[a];
+                float mom = wm * at3 + wgt * push;
+                q[(1 + a) * nodes + node] = (int64_t)((uint64_t)q[(1 + a) * nodes + node] + (uint64_t)fixed3(mom));
+            }
+        }
+        size_t centre = (size_t)(st.base + offset_k(13, nx, ny));
+        q[centre] = (int64_t)((uint64_t)q[centre] + (uint64_t)rest);
+    }
+}
+
 void or_flip3_grid(or_flip3* s, const float* params, or_physics ph) {      /* Flip3.java:267-311 */
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     const int size[3] = {nx, ny, nz};

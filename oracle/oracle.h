@@ -102,6 +102,7 @@ typedef struct {
 
 void or_flip3_clear(or_flip3* s);                                            /* Flip3.java:163-172 */
 void or_flip3_scatter(or_flip3* s, const float* params, or_physics ph);      /* Flip3.java:193-246 */
+void or_fixed_scatter3(or_flip3* s, const float* params, or_physics ph, int64_t* q /* 4 * nodes */);
 void or_flip3_grid(or_flip3* s, const float* params, or_physics ph);         /* Flip3.java:267-311 */
 void or_flip3_advect(or_flip3* s, const float* params);                      /* Flip3.java:329-383, 644-655 */
 void or_flip3_step(or_flip3* s, const float* params, or_physics ph);

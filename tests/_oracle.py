@@ -87,6 +87,7 @@ def lib():
                                                                                   ctypes.c_int] + [i32p] * 3
         for n in ("or_flip3_step", "or_flip3_scatter", "or_flip3_grid"):
             getattr(L, n).argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics]
+        L.or_fixed_scatter3.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, i64p]
         L.or_flip3_clear.argtypes = [ctypes.POINTER(OrFlip3)]
         L.or_flip3_advect.argtypes = [ctypes.POINTER(OrFlip3), f32p]
         L.or_flip3_sort.argtypes = [ctypes.POINTER(OrFlip3), i32p, i32p, i32p, f32p]
@@ -452,6 +453,14 @@ class Flip3State:
     def clear_scatter(self, params, physics=(0, 0)):
         lib().or_flip3_clear(ctypes.byref(self.s))
         lib().or_flip3_scatter(ctypes.byref(self.s), fp(np.ascontiguousarray(params, F)), OrPhysics(*physics))
+
+    def fixed_scatter(self, params, physics=(0, 0)) -> list:
+        """The exact scatter (or_fixed_scatter3): m, mu, mv, mw as int64 with 40 fractional bits."""
+        nodes = self.nx * self.ny * self.nz
+        q = np.zeros(4 * nodes, np.int64)
+        lib().or_fixed_scatter3(ctypes.byref(self.s), fp(np.ascontiguousarray(params, F)), OrPhysics(*physics),
+                                q.ctypes.data_as(i64p))
+        return [q[f * nodes:(f + 1) * nodes] for f in range(4)]
 
     def sort(self):
         nk = lib().or_key3_count(self.nx, self.ny, self.nz)

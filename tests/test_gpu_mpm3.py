@@ -18,7 +18,7 @@ from _oracle import F, Flip3State, JavaRandom, flip3_params, slab3, stable_step
 pytestmark = pytest.mark.gpu
 
 SCHEDULES = [("tile", vf.VF_P2G_TILE, True), ("atomic", vf.VF_P2G_ATOMIC, True), ("warp", vf.VF_P2G_WARP, True),
-             ("atomic-unsorted", vf.VF_P2G_ATOMIC, False)]
+             ("atomic-unsorted", vf.VF_P2G_ATOMIC, False), ("fixed", vf.VF_P2G_FIXED, True)]
 
 
 def sim3(n, count, schedule, sort, **kw):
@@ -45,7 +45,7 @@ def conservation_inputs(n=14, count=150):
     return conservation_particles3(n, count)
 
 
-@pytest.mark.parametrize("name,schedule,sort", SCHEDULES[:3])
+@pytest.mark.parametrize("name,schedule,sort", SCHEDULES[:3] + SCHEDULES[4:])
 def test_scatter_matches_the_oracle_per_node(name, schedule, sort):
     """Flip3Test.theScatterConservesMassAndMomentum (Flip3Test.java:57-118) plus a per-node comparison: the
     device's scatter (sort, clear, scatter) against the oracle's particle-order sum."""
@@ -216,3 +216,26 @@ def test_device_pointers_name_the_grid_and_positions():
         assert ptr and stride == 1
         with pytest.raises(vf.IllegalArgumentException):
             s.device_ptr("nope")
+
+
+def test_the_exact_scatter_is_bit_exact_against_the_oracle_in_any_order():
+    """VF_P2G_FIXED: the device's 64-bit fixed-point grid equals the oracle's to the bit, for the particles in two
+    orders (Flip3Test's conservation particles, seed 3), and its mass is the quantized masses' sum exactly."""
+    n = 14
+    x, y, z, m, j, vel, c = conservation_inputs(n)
+    fields = {"u": vel[0], "v": vel[1], "w": vel[2], "j": j}
+    fields.update({f"c{a // 3}{a % 3}": c[a] for a in range(9)})
+    params = flip3_params(0.01, 0, -10, 0, 1e4, 1)
+    want = Flip3State(n, n, n, x, y, z, m, **fields).fixed_scatter(params)
+    for order in (np.arange(len(x)), np.random.default_rng(4).permutation(len(x))):
+        with vf.ParticleSimulation3(n, n, n, len(x), schedule=vf.VF_P2G_FIXED) as s:
+            s.load([x[order], y[order], z[order]], [vel[0][order], vel[1][order], vel[2][order]], m[order],
+                   vf.flip3_params(0.01, 0, -10, 0, 1e4, 1))
+            s.write("j", j[order])
+            for a in range(9):
+                s.write(f"c{a // 3}{a % 3}", c[a][order])
+            s.run(vf.VF3_PASS_SORT | vf.VF3_PASS_CLEAR | vf.VF3_PASS_SCATTER)
+            got = s.fixed_grid()
+        for f in range(4):
+            assert np.array_equal(got[f], want[f]), f
+    assert int(want[0].sum()) == int(np.rint(m.astype(np.float64) * 2.0 ** 40).astype(np.int64).sum())

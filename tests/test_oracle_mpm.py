@@ -345,3 +345,30 @@ def test_fixed_scatter_conserves_mass_exactly_in_any_order(jittered64):
         assert int(g[0].astype(np.int64).sum()) == int(quanta.sum())
     for f in range(3):
         assert np.array_equal(outs[0][f], outs[1][f])
+
+
+def test_exact_3d_scatter_is_order_free_and_keeps_the_quantized_mass():
+    """The exact 3D scatter (the 3D form of FixedScatter, 64-bit sums): the same grid for the particles in another
+    order, a grid mass that is the particles' quantized masses' sum exactly, and per node within one quantum per
+    particle of the float scatter's grid (Flip3Test's conservation particles, seed 3)."""
+    n = 14
+    x, y, z, m, j, vel, c = conservation_particles3(n)
+    fields = {"u": vel[0], "v": vel[1], "w": vel[2], "j": j}
+    fields.update({f"c{a // 3}{a % 3}": c[a] for a in range(9)})
+    params = flip3_params(0.01, 0, -10, 0, 1e4, 1)
+    s = Flip3State(n, n, n, x, y, z, m, **fields)
+    q = s.fixed_scatter(params)
+    order = np.random.default_rng(4).permutation(len(x))
+    shuffled = {k: v[order] for k, v in fields.items()}
+    t = Flip3State(n, n, n, x[order], y[order], z[order], m[order], **shuffled)
+    q2 = t.fixed_scatter(params)
+    for f in range(4):
+        assert np.array_equal(q[f], q2[f]), f
+    quanta = np.rint(m.astype(np.float64) * 2.0 ** 40).astype(np.int64)
+    assert int(q[0].sum()) == int(quanta.sum())
+    s.clear_scatter(params)
+    scale = 2.0 ** -40
+    for f, key in enumerate(("gm", "gmu", "gmv", "gmw")):
+        e = s.g[key].astype(np.float64)
+        got = q[f].astype(np.float64) * scale
+        assert np.all(np.abs(got - e) <= 1e-5 * np.maximum(1, np.abs(e))), key

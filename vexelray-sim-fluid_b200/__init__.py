@@ -33,7 +33,7 @@ VF_EOS_TAIT = 1
 VF_WALL_STICKY_SHIFT = 8
 VF_P2G_SHIFT = 16
 VF_NO_SORT = 1 << 20
-VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP = 0, 1, 2
+VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED = 0, 1, 2, 3
 VF_SCATTER_GRID, VF_SCATTER_PRE_REDUCED, VF_SCATTER_GATHER, VF_SCATTER_SEGMENTED = 0, 1, 2, 3
 VF3_PASS_SORT, VF3_PASS_CLEAR, VF3_PASS_SCATTER, VF3_PASS_GRID, VF3_PASS_ADVECT = 1, 2, 4, 8, 16
 EDGE_WALL, EDGE_OPEN = 0, 1
@@ -141,6 +141,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_device_ptr": ([_vp, ctypes.c_char_p, ctypes.POINTER(_vp), _i32p], ctypes.c_int32),
         "vf_mpm3_stream": ([_vp], _vp),
         "vf_mpm3_set_p2g": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_read_fixed": ([_vp, ctypes.c_int32, _i64p, ctypes.c_int64], ctypes.c_int32),
         "vf_mpm3_touched_nodes": ([_vp, _i64p], ctypes.c_int32),
         "vf_mpm3_steps": ([_vp], ctypes.c_int64),
         "vf_mpm3_on_gpu": ([_vp], ctypes.c_int32),
@@ -757,7 +758,8 @@ class Prepared:
 class ParticleSimulation3:
     """ParticleSimulation3 (ParticleSimulation3.java): a 3D particle fluid in one walled box on the GPU.
 
-    ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC or VF_P2G_WARP.
+    ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC, VF_P2G_WARP or VF_P2G_FIXED
+    (exact: 64-bit fixed-point sums, the same grid in any order).
     ``sort=False`` keeps the particles in load order, as the reference's Flip3Step does.
     """
 
@@ -865,6 +867,16 @@ class ParticleSimulation3:
 
     def set_schedule(self, schedule: int) -> None:
         check(lib().vf_mpm3_set_p2g(self._h, schedule))
+
+    def fixed_grid(self) -> list:
+        """The last scatter's exact grid (VF_P2G_FIXED): m, mu, mv, mw as int64 with 40 fractional bits."""
+        n = self._nx * self._ny * self._nz
+        out = []
+        for f in range(4):
+            a = np.empty(n, np.int64)
+            check(lib().vf_mpm3_read_fixed(self._h, f, a.ctypes.data_as(_i64p), n))
+            out.append(a)
+        return out
 
     def touched_nodes(self) -> int:
         out = ctypes.c_int64()

@@ -39,6 +39,8 @@ struct vf_mpm3 {
     DeviceBuffer params;
     DeviceBuffer status;
     DeviceBuffer scratch;     // readouts
+    DeviceBuffer fixed;       // the exact schedule's grid: int64 [4][nodes], FIXED3_BITS fractional bits
+    bool fixed_valid = false; // `fixed` holds the last scatter's sums
     Params3 hparams{};
     int64_t steps = 0;
     int64_t passes_run = 0;   // steps run through vf_mpm3_run / advance, for grid parity
@@ -185,12 +187,23 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
             VF_LAUNCH(h->prof, "k_p2g3_tile", h->stream, k_p2g3_tile, persistent_blocks(2), 128, p2g_tile_smem(), s);
         } else if (h->p2g == VF_P2G_WARP) {
             VF_LAUNCH(h->prof, "k_p2g3_warp", h->stream, k_p2g3_warp, div_up(h->np, 256), 256, 0, s);
+        } else if (h->p2g == VF_P2G_FIXED) {
+            if (!h->fixed.ptr) {
+                int32_t rc = h->fixed.alloc((size_t)4 * h->nodes * sizeof(long long));
+                if (rc) return rc;
+            }
+            VF_TRY_CUDA(cudaMemsetAsync(h->fixed.ptr, 0, h->fixed.bytes, h->stream));
+            VF_LAUNCH(h->prof, "k_p2g3_fixed", h->stream, k_p2g3_fixed, div_up(h->np, 256), 256, 0, s,
+                      h->fixed.as<unsigned long long>());
+            VF_LAUNCH(h->prof, "k_fixed_to_grid3", h->stream, k_fixed_to_grid3, div_up(h->nodes, 256), 256, 0,
+                      h->fixed.as<long long>(), s.grid, h->nodes);
         } else {
             VF_LAUNCH(h->prof, "k_p2g3_atomic", h->stream, k_p2g3_atomic, div_up(h->np, 256), 256, 0, s);
         }
         VF_CHECK_LAUNCH();
         h->grid_dirty[g] = tile ? 1 : 2;
         h->grid_last = g;
+        h->fixed_valid = h->p2g == VF_P2G_FIXED;
     }
     if (mask & VF3_PASS_ADVECT) {
         s.count_next = count_next ? 1 : 0;
@@ -249,7 +262,7 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
     VF_REQUIRE(nx >= 3 && ny >= 3 && nz >= 3, VF_EINVAL, "a 3D grid needs at least three nodes each way, got %d x %d x %d",
                nx, ny, nz);
     int p2g = (int)((flags & VF_P2G_MASK) >> VF_P2G_SHIFT);
-    VF_REQUIRE(p2g <= VF_P2G_WARP, VF_EINVAL, "no scatter schedule %d", p2g);
+    VF_REQUIRE(p2g <= VF_P2G_FIXED, VF_EINVAL, "no scatter schedule %d", p2g);
     int32_t rc = require_device();
     if (rc) return rc;
     vf_mpm3* h = new vf_mpm3();
@@ -478,9 +491,20 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
 
 void* vf_mpm3_stream(vf_mpm3* h) { return h ? (void*)h->stream : nullptr; }
 
+int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    VF_REQUIRE(field >= 0 && field < 4, VF_EINVAL, "the exact grid has fields 0..3 (m, mu, mv, mw), got %d", field);
+    VF_REQUIRE(n == h->nodes, VF_EINVAL, "the exact grid has %lld nodes, got %lld", (long long)h->nodes, (long long)n);
+    VF_REQUIRE(h->fixed_valid, VF_ESTATE, "the last scatter did not run the exact schedule (VF_P2G_FIXED)");
+    VF_TRY_CUDA(cudaMemcpyAsync(out, h->fixed.as<long long>() + (int64_t)field * h->nodes, (size_t)n * 8,
+                                cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
-    VF_REQUIRE(schedule >= VF_P2G_TILE && schedule <= VF_P2G_WARP, VF_EINVAL, "no scatter schedule %d", schedule);
+    VF_REQUIRE(schedule >= VF_P2G_TILE && schedule <= VF_P2G_FIXED, VF_EINVAL, "no scatter schedule %d", schedule);
     if (schedule == VF_P2G_TILE && h->p2g != VF_P2G_TILE) {
         // the dense pipeline leaves both grids dense-dirty
         for (int g = 0; g < 2; g++)

@@ -62,6 +62,74 @@ __global__ void __launch_bounds__(256) k_p2g3_atomic(Step3 s) {
     }
 }
 
+// ------------------------------------------------------------------ P2G: exact fixed point
+
+__device__ __forceinline__ long long fixed3(float v) {
+    return __float2ll_rn(__fmul_rn(v, (float)(1ull << FIXED3_BITS)));
+}
+
+// One thread per particle; Flip3.scatter's amounts (Flip3.java:193-246) with every operation rounded on its own
+// (__f*_rn: the compiler may not contract them), as the oracle computes them.
+__global__ void __launch_bounds__(256) k_p2g3_fixed(Step3 s, unsigned long long* q) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= s.np) return;
+    const int src = s.perm ? s.perm[d] : d;
+    const float* in = s.in;
+    const int64_t st = s.stride;
+    const float m = in[M * st + src];
+    if (!(m > 0.0f)) return;
+    const Params3 p = *s.params;
+    int cell[3];
+    float off[3], w[3][3];
+    stencil_axis(in[X * st + src], s.d.nx, cell[0], off[0]);
+    stencil_axis(in[Y * st + src], s.d.ny, cell[1], off[1]);
+    stencil_axis(in[Z * st + src], s.d.nz, cell[2], off[2]);
+#pragma unroll
+    for (int a = 0; a < 3; a++) bspline_weights(off[a], w[a]);
+    const float vel[3] = {in[U * st + src], in[V * st + src], in[W * st + src]};
+    float c[9];
+#pragma unroll
+    for (int a = 0; a < 9; a++) c[a] = in[(C00 + a) * st + src];
+    const float sp = impulse_factor(p.dt, m, p.rho0, p.bulk, in[J * st + src], p.tait);
+    const int nx = s.d.nx, ny = s.d.ny;
+    const int64_t nodes = (int64_t)nx * ny * s.d.nz;
+    const int64_t base = ((int64_t)cell[2] * ny + cell[1]) * nx + cell[0];
+    const long long mass = fixed3(m);
+    long long rest = mass;
+#pragma unroll
+    for (int k = 0; k < 27; k++) {
+        const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
+        const float wgt = __fmul_rn(w[0][ox], __fmul_rn(w[1][oy], w[2][oz]));
+        const float dd[3] = {__fsub_rn((float)ox, off[0]), __fsub_rn((float)oy, off[1]), __fsub_rn((float)oz, off[2])};
+        const float wm = __fmul_rn(wgt, m);
+        const int64_t node = base + (int64_t)oz * nx * ny + oy * nx + ox;
+        if (k != 13) {   // the centre node (1, 1, 1) takes the rest below
+            const long long share = fixed3(wm);
+            rest -= share;
+            atomicAdd(q + node, (unsigned long long)share);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float at3 = __fadd_rn(vel[a], __fadd_rn(__fmul_rn(c[3 * a], dd[0]),
+                                                          __fadd_rn(__fmul_rn(c[3 * a + 1], dd[1]),
+                                                                    __fmul_rn(c[3 * a + 2], dd[2]))));
+            const float push = __fmul_rn(sp, dd[a]);
+            const float mom = __fadd_rn(__fmul_rn(wm, at3), __fmul_rn(wgt, push));
+            atomicAdd(q + (int64_t)(1 + a) * nodes + node, (unsigned long long)fixed3(mom));
+        }
+    }
+    atomicAdd(q + base + (int64_t)nx * ny + nx + 1, (unsigned long long)rest);
+}
+
+__global__ void k_fixed_to_grid3(const long long* q, float4* grid, int64_t nodes) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const double inv = 1.0 / (double)(1ull << FIXED3_BITS);
+    grid[i] = make_float4(__double2float_rn(__ll2double_rn(q[i]) * inv), __double2float_rn(__ll2double_rn(q[nodes + i]) * inv),
+                          __double2float_rn(__ll2double_rn(q[2 * nodes + i]) * inv),
+                          __double2float_rn(__ll2double_rn(q[3 * nodes + i]) * inv));
+}
+
 // ------------------------------------------------------------------ P2G: warp-segmented
 
 // One thread per particle; each run of lanes in one stencil cell is summed across the warp first

@@ -126,6 +126,16 @@ struct Step3 {
     int count_next;         // G2P also counts keys for the next step's sort
 };
 
+// The exact (fixed-point) scatter: each node amount of Flip3.scatter in the reference's operand order without
+// FMA contraction, quantized to FIXED3_BITS fractional bits (round to nearest even) and added with 64-bit
+// integer atomics into q[4][nodes] (m, mu, mv, mw), so the sums do not depend on the order of the additions.
+// A particle's 27 mass shares are quantized and the centre node takes the rest of its quantized mass, so the
+// grid's total mass is the particles' quantized masses' sum exactly.
+constexpr int FIXED3_BITS = 40;
+__global__ void k_p2g3_fixed(Step3 s, unsigned long long* q);
+// q (FIXED3_BITS fractional bits) -> the float grid: float(double(q) * 2^-FIXED3_BITS) per component.
+__global__ void k_fixed_to_grid3(const long long* q, float4* grid, int64_t nodes);
+
 __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
 __global__ void k_p2g3_warp(Step3 s);
