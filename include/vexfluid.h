@@ -260,6 +260,16 @@ int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n);
 int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out);
 int64_t vf_mpm3_steps(const vf_mpm3* h);
 int32_t vf_mpm3_on_gpu(const vf_mpm3* h);
+/* A versioned binary snapshot of the simulation, for resume and replay; no counterpart in the reference. The
+ * blob: a 64-byte header (magic "VFSNAP", version, kind 3, nx, ny, nz, the physics flags, particles, steps, payload
+ * length, FNV-1a 64 of the payload), then 8 param words (7 Flip3.params words and a zero), the 17 particle fields
+ * of the current order (x y z u v w m j c00..c22, np floats each) and the last scatter's grid (nodes x float4
+ * {m, mu, mv, mw}). buf = null: *size gets the length only. Blocking. restore: the same grid sizes, particle count
+ * and physics flags (the scatter schedule and the sort switch may differ), VF_EINVAL on any mismatch or a bad
+ * checksum; it sets the step count and leaves the sort to recount. Under VF_P2G_FIXED a restored run continues
+ * bit for bit as the original does. */
+int32_t vf_mpm3_snapshot(vf_mpm3* h, void* buf, int64_t cap, int64_t* size);
+int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size);
 /* Kernel accounting: with profiling on, every launch of the handle is bracketed by CUDA events and its
  * device time summed per kernel; profile_read returns entry `index` (VF_EINVAL past the last). launches is
  * the count of kernels the handle has launched since it was made, profiling on or off. */
@@ -305,6 +315,12 @@ int32_t vf_swe_tile_width(const vf_swe* h);
  * previous step's last wave and wait on the device for its completion): 1 (the default) or 0 (plain stream
  * order). Bit-identical either way. */
 int32_t vf_swe_set_overlap(vf_swe* h, int32_t on);
+/* A versioned binary snapshot of the patch (kind 2, the same 64-byte header with the edges in flags, 8 bits each):
+ * the 16-word device block (speed words in their rotation, budget words, clamp count, params), clock, dispatch
+ * count, steps and the last step's ticks (int64 each), then h, hu, hv. Resumes bit for bit, clock included.
+ * buf = null: *size gets the length only. restore: VF_EINVAL on another size, edges or a bad checksum. */
+int32_t vf_swe_snapshot(vf_swe* h, void* buf, int64_t cap, int64_t* size);
+int32_t vf_swe_restore(vf_swe* h, const void* buf, int64_t size);
 /* Diagnostics.of(h, hu, hv, g, dry, dt, dx, dy) over the current state (Diagnostics.java:43-81), reduced on the
  * device. out = {volume, minDepth, maxDepth, maxSpeed, maxFroude, maxCourant, nonFinite, negative, wet}. */
 int32_t vf_swe_diagnostics(vf_swe* h, double g, double dry, double dt, double dx, double dy, double out[9]);

@@ -142,6 +142,8 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_stream": ([_vp], _vp),
         "vf_mpm3_set_p2g": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm3_read_fixed": ([_vp, ctypes.c_int32, _i64p, ctypes.c_int64], ctypes.c_int32),
+        "vf_mpm3_snapshot": ([_vp, _vp, ctypes.c_int64, _i64p], ctypes.c_int32),
+        "vf_mpm3_restore": ([_vp, _vp, ctypes.c_int64], ctypes.c_int32),
         "vf_mpm3_touched_nodes": ([_vp, _i64p], ctypes.c_int32),
         "vf_mpm3_steps": ([_vp], ctypes.c_int64),
         "vf_mpm3_on_gpu": ([_vp], ctypes.c_int32),
@@ -204,6 +206,8 @@ def lib() -> ctypes.CDLL:
         "vf_swe_set_tile_width": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_tile_width": ([_vp], ctypes.c_int32),
         "vf_swe_set_overlap": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_snapshot": ([_vp, _vp, ctypes.c_int64, _i64p], ctypes.c_int32),
+        "vf_swe_restore": ([_vp, _vp, ctypes.c_int64], ctypes.c_int32),
         "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_read_budget": ([_vp, ctypes.c_int32, _i32p], ctypes.c_int32),
         "vf_swe_diagnostics": ([_vp] + [ctypes.c_double] * 5 + [ctypes.POINTER(ctypes.c_double)], ctypes.c_int32),
@@ -234,6 +238,14 @@ def check(code: int) -> None:
     if code == VF_ESTATE:
         raise IllegalStateException(code, msg)
     raise VfError(code, msg)
+
+
+def _snapshot(fn, h) -> bytes:
+    size = ctypes.c_int64()
+    check(fn(h, None, 0, ctypes.byref(size)))
+    buf = ctypes.create_string_buffer(size.value)
+    check(fn(h, buf, size.value, ctypes.byref(size)))
+    return buf.raw[: size.value]
 
 
 def _f32(a, n=None) -> np.ndarray:
@@ -878,6 +890,15 @@ class ParticleSimulation3:
             out.append(a)
         return out
 
+    def snapshot(self) -> bytes:
+        """The simulation's state as a versioned, checksummed blob (particles in their current order, params,
+        the last grid, the step count)."""
+        return _snapshot(lib().vf_mpm3_snapshot, self._h)
+
+    def restore(self, blob: bytes) -> None:
+        """Resume from snapshot(); the grid, particle count and physics flags must match (ValueError otherwise)."""
+        check(lib().vf_mpm3_restore(self._h, blob, len(blob)))
+
     def touched_nodes(self) -> int:
         out = ctypes.c_int64()
         check(lib().vf_mpm3_touched_nodes(self._h, ctypes.byref(out)))
@@ -1047,6 +1068,14 @@ class PatchSimulation:
     def set_overlap(self, on: bool) -> None:
         """Steps launched as programmatic dependents of the previous step (default) or in plain stream order."""
         check(lib().vf_swe_set_overlap(self._h, 1 if on else 0))
+
+    def snapshot(self) -> bytes:
+        """The patch's state as a versioned, checksummed blob (cells, speed and budget words, clock, steps)."""
+        return _snapshot(lib().vf_swe_snapshot, self._h)
+
+    def restore(self, blob: bytes) -> None:
+        """Resume from snapshot(); the patch's size and edges must match (ValueError otherwise)."""
+        check(lib().vf_swe_restore(self._h, blob, len(blob)))
 
     def read_budget(self, slot: int) -> int:
         v = ctypes.c_int32()

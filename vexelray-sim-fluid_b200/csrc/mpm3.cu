@@ -15,8 +15,14 @@
 
 #include "mpm3_kernels.cuh"
 #include "profiler.cuh"
+#include "snapshot.cuh"
 
 using namespace vf;
+
+// A snapshot's param block (seven Flip3.params words and a zero pad) and the flags it must agree on: the physics
+// flags, not the scatter schedule or the sort switch, so a run can resume under another schedule.
+constexpr int SNAP3_WORDS = 8;
+constexpr uint32_t SNAP3_FLAGS = ~(uint32_t)(VF_P2G_MASK | VF_NO_SORT);
 
 struct vf_mpm3 {
     int nx, ny, nz, np;
@@ -573,6 +579,66 @@ int32_t vf_mpm3_profile_read(vf_mpm3* h, int32_t index, char* name, size_t cap, 
 int64_t vf_mpm3_launches(const vf_mpm3* h) { return h ? h->prof.launches : 0; }
 
 int32_t vf_mpm3_on_gpu(const vf_mpm3* h) { return h ? 1 : 0; }
+
+int32_t vf_mpm3_snapshot(vf_mpm3* h, void* buf, int64_t cap, int64_t* size) {
+    VF_REQUIRE(h && size, VF_EINVAL, "null argument");
+    const size_t fields = (size_t)NF3 * h->np * 4, grid = (size_t)h->nodes * 16;
+    const uint64_t payload = SNAP3_WORDS * 4 + fields + grid;
+    *size = (int64_t)(sizeof(SnapHeader) + payload);
+    if (!buf) return VF_OK;
+    VF_REQUIRE(cap >= *size, VF_EINVAL, "a snapshot of this simulation takes %lld bytes, the buffer has %lld",
+               (long long)*size, (long long)cap);
+    VF_REQUIRE(h->loaded, VF_ESTATE, "nothing loaded");
+    char* body = static_cast<char*>(buf) + sizeof(SnapHeader);
+    int32_t words[SNAP3_WORDS] = {0};
+    const Params3& p = h->hparams;
+    const float w[7] = {p.dt, p.gx, p.gy, p.gz, p.bulk, p.rho0, p.sigma};
+    memcpy(words, w, sizeof w);
+    memcpy(body, words, sizeof words);
+    const float* base = h->part[h->cur].as<float>();
+    char* dst = body + sizeof words;
+    for (int f = 0; f < NF3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(dst + (size_t)f * h->np * 4, base + f * h->stride, (size_t)h->np * 4,
+                                    cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaMemcpyAsync(dst + fields, h->grid[h->grid_last].ptr, grid, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    int32_t rc = check_status(h);
+    if (rc) return rc;
+    SnapHeader hd = snap_header(SNAP_MPM3, h->nx, h->ny, h->nz, (int32_t)(h->flags & SNAP3_FLAGS), h->np, h->steps,
+                                payload);
+    hd.checksum = fnv1a(body, payload);
+    memcpy(buf, &hd, sizeof hd);
+    return VF_OK;
+}
+
+int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    const size_t fields = (size_t)NF3 * h->np * 4, grid = (size_t)h->nodes * 16;
+    SnapHeader want = snap_header(SNAP_MPM3, h->nx, h->ny, h->nz, (int32_t)(h->flags & SNAP3_FLAGS), h->np, 0,
+                                  SNAP3_WORDS * 4 + fields + grid);
+    SnapHeader got;
+    int32_t rc = snap_check(buf, size, want, &got);
+    if (rc) return rc;
+    const char* body = static_cast<const char*>(buf) + sizeof(SnapHeader);
+    int32_t words[SNAP3_WORDS];
+    memcpy(words, body, sizeof words);
+    if ((rc = upload_params(h, words, 7))) return rc;
+    float* base = h->part[h->cur].as<float>();
+    const char* src = body + sizeof words;
+    for (int f = 0; f < NF3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src + (size_t)f * h->np * 4, (size_t)h->np * 4,
+                                    cudaMemcpyHostToDevice, h->stream));
+    // the last grid goes back where readouts look for it; both buffers are cleared densely before their next scatter
+    VF_TRY_CUDA(cudaMemcpyAsync(h->grid[h->grid_last].ptr, src + fields, grid, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = reset_counts(h))) return rc;
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    h->grid_dirty[0] = h->grid_dirty[1] = 2;
+    h->sorted_valid = false;
+    h->fixed_valid = false;
+    h->steps = got.steps;
+    h->loaded = true;
+    return VF_OK;
+}
 
 void vf_mpm3_destroy(vf_mpm3* h) {
     if (!h) return;

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "profiler.cuh"
+#include "snapshot.cuh"
 #include "sort.cuh"
 
 using namespace vf;
@@ -762,6 +763,65 @@ int32_t vf_swe_dispatch(vf_swe* h, int32_t n) {
 }
 
 int64_t vf_swe_dispatched(const vf_swe* h) { return h ? h->dispatched : 0; }
+
+// The snapshot's body: the 16-word device block (speed words in their rotation, budget words, clamp count, params),
+// the host clock, dispatch count, step total and last step's ticks, then h, hu, hv of the current state.
+int32_t vf_swe_snapshot(vf_swe* h, void* buf, int64_t cap, int64_t* size) {
+    VF_REQUIRE(h && size, VF_EINVAL, "null argument");
+    const size_t fields = (size_t)3 * h->cells * 4;
+    const uint64_t payload = 64 + 4 * 8 + fields;
+    *size = (int64_t)(sizeof(SnapHeader) + payload);
+    if (!buf) return VF_OK;
+    VF_REQUIRE(cap >= *size, VF_EINVAL, "a snapshot of this patch takes %lld bytes, the buffer has %lld",
+               (long long)*size, (long long)cap);
+    VF_REQUIRE(h->clock_outstanding == 0, VF_ESTATE, "a grant is outstanding");
+    char* body = static_cast<char*>(buf) + sizeof(SnapHeader);
+    VF_TRY_CUDA(cudaMemcpyAsync(body, h->small.ptr, 64, cudaMemcpyDeviceToHost, h->stream));
+    const int64_t clock[4] = {h->clock_now, h->dispatched, h->total_steps, h->last_step};
+    memcpy(body + 64, clock, sizeof clock);
+    const int s = (int)(h->dispatched % 2);
+    for (int f = 0; f < 3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(body + 96 + (size_t)f * h->cells * 4, field(h, s, f), (size_t)h->cells * 4,
+                                    cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    int32_t rc = status_swe(h);
+    if (rc) return rc;
+    const int32_t edges = h->edges[0] | h->edges[1] << 8 | h->edges[2] << 16 | h->edges[3] << 24;
+    SnapHeader hd = snap_header(SNAP_SWE, h->nx, h->ny, 1, edges, h->cells, h->total_steps, payload);
+    hd.checksum = fnv1a(body, payload);
+    memcpy(buf, &hd, sizeof hd);
+    return VF_OK;
+}
+
+int32_t vf_swe_restore(vf_swe* h, const void* buf, int64_t size) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    const int32_t edges = h->edges[0] | h->edges[1] << 8 | h->edges[2] << 16 | h->edges[3] << 24;
+    SnapHeader want = snap_header(SNAP_SWE, h->nx, h->ny, 1, edges, h->cells, 0, 64 + 4 * 8 + (size_t)3 * h->cells * 4);
+    SnapHeader got;
+    int32_t rc = snap_check(buf, size, want, &got);
+    if (rc) return rc;
+    const char* body = static_cast<const char*>(buf) + sizeof(SnapHeader);
+    int32_t small[16];
+    memcpy(small, body, sizeof small);
+    float p[5];
+    if ((rc = swe_params_check(small + 8, 5, p))) return rc;
+    int64_t clock[4];
+    memcpy(clock, body + 64, sizeof clock);
+    VF_REQUIRE(clock[1] >= 0 && clock[2] >= 0 && clock[3] >= 0, VF_EINVAL, "a snapshot with negative counts");
+    const int s = (int)(clock[1] % 2);
+    for (int f = 0; f < 3; f++)
+        VF_TRY_CUDA(cudaMemcpyAsync(field(h, s, f), body + 96 + (size_t)f * h->cells * 4, (size_t)h->cells * 4,
+                                    cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaMemcpyAsync(h->small.ptr, small, sizeof small, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    memcpy(h->host_params, p, sizeof p);
+    h->clock_now = clock[0];
+    h->dispatched = clock[1];
+    h->total_steps = clock[2];
+    h->last_step = clock[3];
+    h->clock_outstanding = 0;
+    return VF_OK;
+}
 
 int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
