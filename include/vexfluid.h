@@ -70,7 +70,9 @@ enum {
     VF_WALL_STICKY_MASK = 0xffu << 8,
     VF_P2G_SHIFT = 16,              /* bits 16..19: the 3D scatter schedule, VF_P2G_* */
     VF_P2G_MASK = 0xfu << 16,
-    VF_NO_SORT = 1u << 20           /* 3D: keep the particles in load order (Flip3Step's behaviour) */
+    VF_NO_SORT = 1u << 20,          /* 3D: keep the particles in load order (Flip3Step's behaviour) */
+    VF_TENSION = 1u << 21           /* 3D: surface tension's passes between the scatter and the grid (Flip3Step with
+                                       tension, Flip3Step.java:88-109); its strength is sigma, the params' word 6 */
 };
 #define VF_WALL_STICKY(t) ((uint32_t)(t) << VF_WALL_STICKY_SHIFT)
 
@@ -216,7 +218,8 @@ enum {   /* fields (Flip3.PARTICLE, Flip3.java:112-115; grid names Flip3Step.jav
 
 /* ParticleSimulation3.prepare (ParticleSimulation3.java:110-139): every buffer allocated and every kernel
  * loaded, nothing submitted; may run on any thread. nx, ny, nz >= 3; particles >= 1 (Flip3Step.java:54-56).
- * flags: VF_EOS_TAIT, VF_WALL_STICKY(t), P2G schedule << VF_P2G_SHIFT, VF_NO_SORT. */
+ * flags: VF_EOS_TAIT, VF_WALL_STICKY(t), P2G schedule << VF_P2G_SHIFT, VF_NO_SORT, VF_TENSION (prepare(..., tension)).
+ * With VF_TENSION the grid readouts VF3_GU..GW include the tension's force. */
 int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
                         vf_mpm3_prepared** out);
 /* Prepared.close (ParticleSimulation3.java:94-102): frees a preparation never finished. Idempotent. */

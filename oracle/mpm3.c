@@ -146,13 +146,14 @@ void or_fixed_scatter3(or_flip3* s, const float* params, or_physics ph, int64_t*
     }
 }
 
-void or_flip3_grid(or_flip3* s, const float* params, or_physics ph) {      /* Flip3.java:267-311 */
+static void grid3(or_flip3* s, const float* params, or_physics ph, const float* colour, const float* stress) {
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     const int size[3] = {nx, ny, nz};
     const float g[3] = {params[P_GX], params[P_GY], params[P_GZ]};
     const float* mom[3] = {s->gmu, s->gmv, s->gmw};
     float* out[3] = {s->gu, s->gv, s->gw};
     int64_t nodes = (int64_t)nx * ny * nz;
+#pragma omp parallel for schedule(static)   /* each node alone: the split changes no bit */
     for (int64_t node = 0; node < nodes; node++) {
         int at[3] = {(int)(node % nx), (int)((node / nx) % ny), (int)(node / ((int64_t)nx * ny))};
         float mass = s->gm[node];
@@ -160,6 +161,12 @@ void or_flip3_grid(or_flip3* s, const float* params, or_physics ph) {      /* Fl
         if (mass > EMPTY) {
             float dt = params[P_DT];
             for (int a = 0; a < 3; a++) vel[a] = mom[a][node] / mass + dt * g[a];
+            if (colour) {                                                  /* Flip3.java:291-299 */
+                float force[3];
+                or_tension3_force(nx, ny, nz, colour, stress, at, force);
+                float push = (dt * params[6]) / fmaxf(mass, OR_MASS_FLOOR * params[P_RHO0]);
+                for (int a = 0; a < 3; a++) vel[a] = vel[a] + push * force[a];
+            }
         }
         int stuck = 0;
         if (ph.sticky > 0) {
@@ -175,6 +182,15 @@ void or_flip3_grid(or_flip3* s, const float* params, or_physics ph) {      /* Fl
             out[a][node] = vel[a];
         }
     }
+}
+
+void or_flip3_grid(or_flip3* s, const float* params, or_physics ph) {      /* Flip3.java:267-311 */
+    grid3(s, params, ph, NULL, NULL);
+}
+
+void or_flip3_grid_tension(or_flip3* s, const float* params, or_physics ph, const float* colour,
+                           const float* stress) {                        /* Flip3.java:258-310 */
+    grid3(s, params, ph, colour, stress);
 }
 
 static inline void keep_inside(float* at, float* vel, int size) {   /* Flip3.java:644-655 */
@@ -224,6 +240,16 @@ void or_flip3_step(or_flip3* s, const float* params, or_physics ph) {   /* Flip3
     or_flip3_clear(s);
     or_flip3_scatter(s, params, ph);
     or_flip3_grid(s, params, ph);
+    or_flip3_advect(s, params);
+}
+
+void or_flip3_step_tension(or_flip3* s, const float* params, or_physics ph, float* scratch) {
+    const int64_t nodes = (int64_t)s->nx * s->ny * s->nz;
+    or_flip3_clear(s);
+    or_flip3_scatter(s, params, ph);
+    const float* colour = or_tension3_colour(s->nx, s->ny, s->nz, s->gm, params, scratch, scratch + nodes);
+    or_tension3_stress(s->nx, s->ny, s->nz, colour, scratch + 2 * nodes);
+    or_flip3_grid_tension(s, params, ph, colour, scratch + 2 * nodes);
     or_flip3_advect(s, params);
 }
 

@@ -107,6 +107,25 @@ void or_flip3_grid(or_flip3* s, const float* params, or_physics ph);         /* 
 void or_flip3_advect(or_flip3* s, const float* params);                      /* Flip3.java:329-383, 644-655 */
 void or_flip3_step(or_flip3* s, const float* params, or_physics ph);
 
+/* Surface tension (particle/Tension3.java), the passes Flip3Step runs between the scatter and the grid when it
+ * has tension (Flip3Step.java:88-109). Nodes (k*ny + j)*nx + i; every neighbour read held to [1, n-2]. */
+#define OR_TENSION_BLURS 6          /* Flip.java:100 */
+#define OR_MIN_COLOUR 0.3f          /* Tension.java:74 */
+#define OR_MASS_FLOOR 0.3f          /* Tension.java:77 */
+void or_tension3_blur(int nx, int ny, int nz, const float* src, float* dst, const float* params,
+                      int scaled);                                           /* Tension3.java:73-107 */
+/* The mass to a colour and OR_TENSION_BLURS blurs, ping-ponging c0 (first) and c1; returns the last written. */
+const float* or_tension3_colour(int nx, int ny, int nz, const float* gm, const float* params, float* c0, float* c1);
+void or_tension3_stress(int nx, int ny, int nz, const float* colour, float* stress /* 6 * nodes:
+                        txx tyy tzz txy txz tyz */);                        /* Tension3.java:128-154 */
+void or_tension3_force(int nx, int ny, int nz, const float* colour, const float* stress, const int at[3],
+                       float force[3]);                                      /* Tension3.java:162-200 */
+void or_flip3_grid_tension(or_flip3* s, const float* params, or_physics ph, const float* colour,
+                           const float* stress);                             /* Flip3.java:258-310 */
+/* Flip3Step with tension: clear, scatter, colour and blurs, stress, grid with tension, advect.
+ * scratch: 8 * nodes floats. */
+void or_flip3_step_tension(or_flip3* s, const float* params, or_physics ph, float* scratch);
+
 /* The 3D sort key: the stencil base cell of Flip3.Stencil3 (Flip3.java:664-678), base
  * cells 0..n-3 per axis, linearised brick-major in 8x8x8 bricks (the reference has no
  * 3D sort; the key is defined here). */

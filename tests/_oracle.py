@@ -88,6 +88,12 @@ def lib():
         for n in ("or_flip3_step", "or_flip3_scatter", "or_flip3_grid"):
             getattr(L, n).argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics]
         L.or_fixed_scatter3.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, i64p]
+        L.or_tension3_blur.argtypes = [ctypes.c_int] * 3 + [f32p, f32p, f32p, ctypes.c_int]
+        L.or_tension3_colour.argtypes = [ctypes.c_int] * 3 + [f32p] * 4
+        L.or_tension3_colour.restype = f32p
+        L.or_tension3_stress.argtypes = [ctypes.c_int] * 3 + [f32p, f32p]
+        L.or_flip3_grid_tension.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, f32p, f32p]
+        L.or_flip3_step_tension.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, f32p]
         L.or_flip3_clear.argtypes = [ctypes.POINTER(OrFlip3)]
         L.or_flip3_advect.argtypes = [ctypes.POINTER(OrFlip3), f32p]
         L.or_flip3_sort.argtypes = [ctypes.POINTER(OrFlip3), i32p, i32p, i32p, f32p]
@@ -284,6 +290,73 @@ def slab3(seed: int, n=24, width=6, height=12, ppc=8, rho0=1.0):
     return x, y, z, m
 
 
+def drop3(n=40, radius=8.0, seed=5, ppc=8):
+    """Tension3Test's drop (Tension3Test.java:30-62): ppc particles, uniform in each cell whose centre lies within
+    ``radius`` of the box's centre, mass 1/ppc. Returns x, y, z, m and the number of cells."""
+    centre = n / 2.0
+    cells = [(col, row, layer) for layer in range(n) for row in range(n) for col in range(n)
+             if math.sqrt((col + 0.5 - centre) ** 2 + (row + 0.5 - centre) ** 2 + (layer + 0.5 - centre) ** 2)
+             <= radius]
+    count = len(cells) * ppc
+    r = JavaRandom(seed)
+    at = np.empty((3, count), F)
+    k = 0
+    for col, row, layer in cells:
+        for _ in range(ppc):
+            at[0, k] = F(col) + r.next_float() * F(0.999)
+            at[1, k] = F(row) + r.next_float() * F(0.999)
+            at[2, k] = F(layer) + r.next_float() * F(0.999)
+            k += 1
+    return at[0], at[1], at[2], np.full(count, F(1.0 / ppc), F), len(cells)
+
+
+def drop_pressure(make, n=40, radius=8.0, sigma=0.0, sound=200.0):
+    """Tension3Test.pressure (Tension3Test.java:30-124) over any 3D step: a drop at rest, no gravity, run for
+    0.4 s. ``make(x, y, z, m, params)`` returns an object with ``step()`` and ``read(name)``. Returns the mean
+    pressure B(1/J - 1) of the particles in the drop's inner half, averaged over the later steps; 2 sigma / R; R;
+    the largest speed of the centre of mass; the fastest particle."""
+    bulk = sound * sound
+    dt = stable_step(bulk, 1, 20, 0.3)
+    steps = math.ceil(0.4 / dt)
+    centre = n / 2.0
+    x, y, z, m, cells = drop3(n, radius)
+    effective = (3 * cells / (4 * math.pi)) ** (1 / 3)
+    sim = make(x, y, z, m, (dt, 0.0, 0.0, 0.0, bulk, 1.0, sigma))
+    total, samples, fastest, drift = 0.0, 0, 0.0, 0.0
+    for s in range(steps):
+        sim.step()
+        if s >= steps // 3 and s % 5 == 0:
+            pos = np.stack([sim.read(a).astype(np.float64) for a in ("x", "y", "z")])
+            vel = np.stack([sim.read(a).astype(np.float64) for a in ("u", "v", "w")])
+            j = sim.read("j").astype(np.float64)
+            fastest = max(fastest, float(np.sqrt((vel ** 2).sum(0)).max()))
+            inner = np.sqrt(((pos - centre) ** 2).sum(0)) < 0.5 * effective
+            total += float((bulk * (1 / j[inner] - 1)).sum()) / int(inner.sum())
+            drift = max(drift, float(np.sqrt((vel.sum(1) ** 2).sum())) / len(x))
+            samples += 1
+    return total / samples, 2 * sigma / effective, effective, drift, fastest
+
+
+def check_laplace(pressure):
+    """Tension3Test.aDropsPressureIsTwiceSigmaOverItsRadius's bounds (Tension3Test.java:127-150); ``pressure(radius,
+    sigma)`` is drop_pressure over one step implementation."""
+    radius = 8.0
+    sigma = 0.01 * 200.0 * 200.0 * radius
+    none = pressure(radius, 0.0)
+    one = pressure(radius, sigma)
+    two = pressure(radius, 2 * sigma)
+    wide = pressure(1.5 * radius, sigma)
+    assert abs(none[0]) < 0.15 * one[1], f"a drop with no tension has pressure {none[0]}"
+    ratio = (one[0] - none[0]) / one[1]
+    assert 0.3 < ratio < 1.1, f"the pressure is {ratio} of 2 sigma/R"
+    doubled = (two[0] - none[0]) / (one[0] - none[0])
+    assert 1.6 < doubled < 2.4, f"twice the tension gives {doubled} times the pressure"
+    wider = (wide[0] - none[0]) / (one[0] - none[0])
+    assert 0.45 < wider < 0.9, f"a drop of 1.5 times the radius has {wider} of the pressure, against 2/3"
+    assert one[3] < 0.5, f"the drop's centre of mass moves at {one[3]}"
+    return ratio, doubled, wider, one[3]
+
+
 @dataclass
 class Particles:
     """ScatterTest.Particles (ScatterTest.java:453-518): SoA particles in node units."""
@@ -447,8 +520,28 @@ class Flip3State:
         self.s = OrFlip3(nx, ny, nz, self.np, *[fp(self.a[f]) for f in ("x", "y", "z", "u", "v", "w", "m", "j")],
                          cs, *[fp(self.g[f]) for f in ("gm", "gmu", "gmv", "gmw", "gu", "gv", "gw")])
 
-    def step(self, params, physics=(0, 0)):
-        lib().or_flip3_step(ctypes.byref(self.s), fp(np.ascontiguousarray(params, F)), OrPhysics(*physics))
+    def step(self, params, physics=(0, 0), tension=False):
+        """One Flip3Step step; with ``tension``, the step built with surface tension."""
+        p = fp(np.ascontiguousarray(params, F))
+        if tension:
+            if getattr(self, "_scratch", None) is None:
+                self._scratch = np.zeros(8 * self.nx * self.ny * self.nz, F)
+            lib().or_flip3_step_tension(ctypes.byref(self.s), p, OrPhysics(*physics), fp(self._scratch))
+        else:
+            lib().or_flip3_step(ctypes.byref(self.s), p, OrPhysics(*physics))
+
+    def tension_grid(self, params, physics=(0, 0)):
+        """The tension's passes and the grid with tension over the grid as it stands (gm..gmw): fills gu, gv, gw
+        and returns the last colour and the six stress planes."""
+        nodes = self.nx * self.ny * self.nz
+        c0, c1 = np.zeros(nodes, F), np.zeros(nodes, F)
+        stress = np.zeros(6 * nodes, F)
+        pp = np.ascontiguousarray(params, F)
+        last = lib().or_tension3_colour(self.nx, self.ny, self.nz, fp(self.g["gm"]), fp(pp), fp(c0), fp(c1))
+        colour = c0 if ctypes.addressof(last.contents) == c0.ctypes.data else c1
+        lib().or_tension3_stress(self.nx, self.ny, self.nz, fp(colour), fp(stress))
+        lib().or_flip3_grid_tension(ctypes.byref(self.s), fp(pp), OrPhysics(*physics), fp(colour), fp(stress))
+        return colour, stress.reshape(6, nodes)
 
     def clear_scatter(self, params, physics=(0, 0)):
         lib().or_flip3_clear(ctypes.byref(self.s))

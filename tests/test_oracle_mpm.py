@@ -1,18 +1,20 @@
 """The oracle pinned by the reference's own particle tests.
 
 Each test restates one reference test (FlipTest, Flip3Test, ScatterTest, SortTest,
-FixedScatterTest, under vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/)
+FixedScatterTest, Tension3Test, under vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/)
 with its seeded inputs regenerated by the java.util.Random restatement, and applies the
 reference's assertions to the oracle. A test here failing means the restatement is wrong,
 not the kernels.
 """
+import ctypes
 import math
 
 import numpy as np
 import pytest
 
-from _oracle import (F, WALL, Flip2State, Flip3State, JavaRandom, Particles, cells2, flip3_params, flip_column,
-                     flip_params, fp, ip, key3, lib, slab3, stable_step)
+from _oracle import (F, WALL, Flip2State, Flip3State, JavaRandom, OrPhysics, Particles, cells2, check_laplace,
+                     drop3, drop_pressure, flip3_params, flip_column, flip_params, fp, ip, key3, lib, slab3,
+                     stable_step)
 
 
 # ---------------------------------------------------------------------------------- FlipTest
@@ -372,3 +374,47 @@ def test_exact_3d_scatter_is_order_free_and_keeps_the_quantized_mass():
         e = s.g[key].astype(np.float64)
         got = q[f].astype(np.float64) * scale
         assert np.all(np.abs(got - e) <= 1e-5 * np.maximum(1, np.abs(e))), key
+
+
+class OracleDrop:
+    """A 40^3 box stepped by the oracle's Flip3Step with tension, for drop_pressure."""
+
+    def __init__(self, x, y, z, m, p):
+        self.o = Flip3State(40, 40, 40, x, y, z, m)
+        self.p = flip3_params(*p)
+
+    def step(self):
+        self.o.step(self.p, tension=True)
+
+    def read(self, name):
+        return self.o.a[name]
+
+
+def test_oracle_tension_gives_a_drop_laplaces_pressure():
+    """Pins the tension restatement on Tension3Test.aDropsPressureIsTwiceSigmaOverItsRadius (Tension3Test.java:
+    127-150), the reference's own known-answer test, with its bounds: a drop of radius 8 has 0.3-1.1 of 2 sigma/R
+    above the no-tension pressure, twice the tension 1.6-2.4 times as much, a drop 1.5 times as wide 0.45-0.9 of
+    it, and its centre of mass moves at under 0.5."""
+    check_laplace(lambda radius, sigma: drop_pressure(OracleDrop, radius=radius, sigma=sigma))
+
+
+def test_oracle_tension_without_sigma_is_the_plain_grid():
+    """gridWithTension adds dt sigma F / max(m, MASS_FLOOR rho0) (Flip3.java:291-299): with sigma = 0 every velocity
+    is the plain grid's to the bit, and with sigma > 0 the drop's surface nodes move and the far field does not."""
+    n = 24
+    x, y, z, m, _ = drop3(n, radius=5.0)
+    params0 = flip3_params(1e-3, 0, 0, 0, 400.0, 1.0)
+    o = Flip3State(n, n, n, x, y, z, m)
+    o.clear_scatter(params0)
+    o.tension_grid(params0)
+    plain = Flip3State(n, n, n, x, y, z, m)
+    plain.clear_scatter(params0)
+    lib().or_flip3_grid(ctypes.byref(plain.s), fp(np.ascontiguousarray(params0, F)), OrPhysics(0, 0))
+    for k in ("gu", "gv", "gw"):
+        assert np.array_equal(o.g[k].view(np.int32), plain.g[k].view(np.int32)), k
+    o.tension_grid(flip3_params(1e-3, 0, 0, 0, 400.0, 1.0, 50.0))
+    moved = np.zeros(n ** 3, bool)
+    for k in ("gu", "gv", "gw"):
+        moved |= o.g[k] != plain.g[k]
+    assert moved.any()
+    assert not (moved & (o.g["gm"] <= 1e-9)).any()

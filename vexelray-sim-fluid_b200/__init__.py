@@ -33,6 +33,7 @@ VF_EOS_TAIT = 1
 VF_WALL_STICKY_SHIFT = 8
 VF_P2G_SHIFT = 16
 VF_NO_SORT = 1 << 20
+VF_TENSION = 1 << 21
 VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED = 0, 1, 2, 3
 VF_SCATTER_GRID, VF_SCATTER_PRE_REDUCED, VF_SCATTER_GATHER, VF_SCATTER_SEGMENTED = 0, 1, 2, 3
 VF3_PASS_SORT, VF3_PASS_CLEAR, VF3_PASS_SCATTER, VF3_PASS_GRID, VF3_PASS_ADVECT = 1, 2, 4, 8, 16
@@ -773,12 +774,15 @@ class ParticleSimulation3:
     ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC, VF_P2G_WARP or VF_P2G_FIXED
     (exact: 64-bit fixed-point sums, the same grid in any order).
     ``sort=False`` keeps the particles in load order, as the reference's Flip3Step does.
+    ``tension=True`` adds surface tension's passes (ParticleSimulation3(..., tension)); its strength is sigma, the
+    seventh params word (``flip3_params(..., sigma)``).
     """
 
     @staticmethod
-    def prepare(nx, ny, nz, particles, *, tait=False, sticky=0, schedule=VF_P2G_TILE, sort=True) -> Prepared:
+    def prepare(nx, ny, nz, particles, *, tait=False, sticky=0, schedule=VF_P2G_TILE, sort=True,
+                tension=False) -> Prepared:
         flags = ((VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT) | (schedule << VF_P2G_SHIFT)
-                 | (0 if sort else VF_NO_SORT))
+                 | (0 if sort else VF_NO_SORT) | (VF_TENSION if tension else 0))
         p = _vp()
         check(lib().vf_mpm3_prepare(nx, ny, nz, particles, flags, ctypes.byref(p)))
         return Prepared(p, nx, ny, nz, particles)

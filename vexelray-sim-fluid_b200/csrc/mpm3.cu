@@ -5,7 +5,8 @@
 //   [sort]    brick scan -> cell scan -> permute -> stable fix-up       (counts from the last G2P)
 //   clear     the node windows the scatter two steps ago touched in this grid buffer
 //   scatter   k_p2g3_tile  (or k_p2g3_atomic / k_p2g3_warp after a dense clear)
-//   grid      fused into k_g2p3_tile (or k_grid3_dense for the other schedules)
+//   grid      fused into k_g2p3_tile (or k_grid3_dense for the other schedules); with VF_TENSION the colour, its
+//             blurs, the stress and k_grid3_tension write the velocity grid, which every G2P then reads
 //   advect    k_g2p3_tile  gathers each particle through the sort's permutation, writes it to its
 //             sorted slot in the other particle set, and counts its new key for the next sort
 #include <algorithm>
@@ -46,6 +47,9 @@ struct vf_mpm3 {
     DeviceBuffer status;
     DeviceBuffer scratch;     // readouts
     DeviceBuffer fixed;       // the exact schedule's grid: int64 [4][nodes], FIXED3_BITS fractional bits
+    bool tension = false;     // VF_TENSION: Tension3's passes between the scatter and the grid
+    DeviceBuffer colour[2];   // the blurs' ping-pong colour planes, nodes floats each
+    DeviceBuffer stress;      // txx tyy tzz txy txz tyz, nodes floats each
     bool fixed_valid = false; // `fixed` holds the last scatter's sums
     Params3 hparams{};
     int64_t steps = 0;
@@ -112,6 +116,26 @@ Step3 make_step(vf_mpm3* h) {
 }
 
 int persistent_blocks(int per_sm) { return sm_count() * per_sm; }
+
+// The grid update into `vel` for the step that scattered into grid[g]: Flip3.grid, or with tension the colour,
+// its blurs, the stress and Flip3.gridWithTension (Flip3Step.java:88-109).
+int32_t grid_pass(vf_mpm3* h, Step3& s, int g) {
+    s.grid = h->grid[g].as<float4>();
+    if (!h->tension) {
+        VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
+        return VF_OK;
+    }
+    const int blocks = div_up(h->nodes, 256);
+    float* c[2] = {h->colour[0].as<float>(), h->colour[1].as<float>()};
+    VF_LAUNCH(h->prof, "k_tension3_colour", h->stream, k_tension3_colour, blocks, 256, 0, s.grid, c[0], s.params, s.d);
+    for (int k = 1; k < TENSION3_BLURS; k++)
+        VF_LAUNCH(h->prof, "k_tension3_blur", h->stream, k_tension3_blur, blocks, 256, 0, c[(k - 1) % 2], c[k % 2], s.d);
+    const float* colour = c[(TENSION3_BLURS - 1) % 2];
+    VF_LAUNCH(h->prof, "k_tension3_stress", h->stream, k_tension3_stress, blocks, 256, 0, colour, h->stress.as<float>(),
+              s.d);
+    VF_LAUNCH(h->prof, "k_grid3_tension", h->stream, k_grid3_tension, blocks, 256, 0, s, colour, h->stress.as<float>());
+    return VF_OK;
+}
 
 // Zero the counts so the next count pass starts clean (after positions changed under the
 // counts of a G2P that counted ahead).
@@ -213,16 +237,23 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_ADVECT) {
         s.count_next = count_next ? 1 : 0;
+        int32_t rc;
         if (tile) {
+            // the tiled G2P updates the grid itself, unless tension's force needs the whole grid first
+            if (h->tension) {
+                if ((rc = grid_pass(h, s, g))) return rc;
+                s.vel_ready = 1;
+            }
             VF_LAUNCH(h->prof, "k_g2p3_tile", h->stream, k_g2p3_tile, persistent_blocks(4), 256, 0, s);
         } else {
-            VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
+            if ((rc = grid_pass(h, s, g))) return rc;
             VF_LAUNCH(h->prof, "k_g2p3", h->stream, k_g2p3, div_up(h->np, 256), 256, 0, s);
         }
         if (sort) h->cur ^= 1;
         h->counted = count_next;
     } else if (mask & VF3_PASS_GRID) {
-        VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
+        int32_t rc = grid_pass(h, s, g);
+        if (rc) return rc;
     }
     if (sort && !(mask & VF3_PASS_ADVECT)) {
         // the particles were not moved to their sorted slots; apply the permutation as a copy
@@ -308,6 +339,10 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
         (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc((size_t)h->nodes * 16)) ||
         (rc = h->grid[1].alloc((size_t)h->nodes * 16)) || (rc = h->vel.alloc((size_t)h->nodes * 16)) ||
         (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)))
+        return fail(rc);
+    h->tension = (flags & VF_TENSION) != 0;
+    if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
+                       (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);
     if (cudaFuncSetAttribute(k_p2g3_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_tile_smem()) !=
         cudaSuccess) {
@@ -413,9 +448,8 @@ int32_t vf_mpm3_read(vf_mpm3* h, int32_t field, float* out, int64_t n) {
         int comp = field - VF3_GM;
         if (field >= VF3_GU) {
             Step3 s = make_step(h);
-            s.grid = h->grid[h->grid_last].as<float4>();
-            k_grid3_dense<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s);
-            VF_CHECK_LAUNCH();
+            int32_t rc = grid_pass(h, s, h->grid_last);
+            if (rc) return rc;
             src = h->vel.as<float4>();
             comp = field - VF3_GU;
         }

@@ -662,8 +662,13 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
             const int gx = cx0 + wi % WIN, gy = cy0 + (wi / WIN) % WIN, gz = cz0 + wi / (WIN * WIN);
             float4 v = make_float4(0, 0, 0, 0);
             if (gx < dm.nx && gy < dm.ny && gz < dm.nz) {
-                const float3 u = grid_velocity(s.grid[((int64_t)gz * dm.ny + gy) * dm.nx + gx], gx, gy, gz, dm, p);
-                v = make_float4(u.x, u.y, u.z, 0.0f);
+                const int64_t node = ((int64_t)gz * dm.ny + gy) * dm.nx + gx;
+                if (s.vel_ready) {
+                    v = s.vel[node];
+                } else {
+                    const float3 u = grid_velocity(s.grid[node], gx, gy, gz, dm, p);
+                    v = make_float4(u.x, u.y, u.z, 0.0f);
+                }
             }
             vwin[wi] = v;
         }

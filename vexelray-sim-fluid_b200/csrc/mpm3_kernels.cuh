@@ -5,8 +5,9 @@
 //              x y z u v w m j c00 c01 c02 c10 c11 c12 c20 c21 c22   (Flip3.PARTICLE order)
 //   grid       float4 per node {m, mu, mv, mw}, node (k*ny + j)*nx + i, two buffers (one per step
 //              parity, so the last scatter stays readable while the next one accumulates)
-//   velocity   float4 per node {u, v, w, 0} (dense pipeline only; the tiled G2P computes the
-//              grid update into shared memory and never writes velocities to HBM)
+//   velocity   float4 per node {u, v, w, 0} (dense pipeline, and any step with surface tension; otherwise the
+//              tiled G2P computes the grid update into shared memory and never writes velocities to HBM)
+//   tension    two colour planes and six stress planes of nodes floats, when the step has surface tension
 //   sort       key/perm per particle; cell counts/starts/cursors over the brick-major keys; brick
 //              counts/starts and the list of non-empty bricks
 #pragma once
@@ -62,14 +63,20 @@ __device__ __forceinline__ int key3_of(float x, float y, float z, const Dims3& d
 // The grid update of one node (Flip3.grid, Flip3.java:267-311): momentum over mass plus a step of
 // gravity, zero for an empty node; the wall ring drops the velocity into the wall, or a sticky
 // wall of `sticky` nodes stops it.
-__device__ __forceinline__ float3 grid_velocity(float4 g, int i, int j, int k, const Dims3& d, const Params3& p) {
-    float v[3] = {0.0f, 0.0f, 0.0f};
+// Flip3.grid's velocity before the walls (Flip3.java:285-290): momentum over mass plus a step of gravity.
+__device__ __forceinline__ void grid_velocity_free(float4 g, const Params3& p, float v[3]) {
+    v[0] = v[1] = v[2] = 0.0f;
     const float mass = g.x;
     if (mass > EMPTY3) {
         v[0] = __fadd_rn(__fdiv_rn(g.y, mass), __fmul_rn(p.dt, p.gx));
         v[1] = __fadd_rn(__fdiv_rn(g.z, mass), __fmul_rn(p.dt, p.gy));
         v[2] = __fadd_rn(__fdiv_rn(g.w, mass), __fmul_rn(p.dt, p.gz));
     }
+}
+
+// Flip3.grid's walls (Flip3.java:302-307): the velocity into the wall ring dropped, or with sticky walls every
+// node within `sticky` of an edge stopped.
+__device__ __forceinline__ float3 grid_walls(float v[3], int i, int j, int k, const Dims3& d, const Params3& p) {
     const int at[3] = {i, j, k};
     const int size[3] = {d.nx, d.ny, d.nz};
     if (p.sticky > 0) {
@@ -85,6 +92,12 @@ __device__ __forceinline__ float3 grid_velocity(float4 g, int i, int j, int k, c
         }
     }
     return make_float3(v[0], v[1], v[2]);
+}
+
+__device__ __forceinline__ float3 grid_velocity(float4 g, int i, int j, int k, const Dims3& d, const Params3& p) {
+    float v[3];
+    grid_velocity_free(g, p, v);
+    return grid_walls(v, i, j, k, d, p);
 }
 
 // Flip3.keepInside (Flip3.java:644-655)
@@ -124,6 +137,7 @@ struct Step3 {
     int64_t nkeys;
     int nbricks;
     int count_next;         // G2P also counts keys for the next step's sort
+    int vel_ready;          // the tiled G2P reads `vel` (written by the grid pass) instead of updating the grid itself
 };
 
 // The exact (fixed-point) scatter: each node amount of Flip3.scatter in the reference's operand order without
@@ -135,6 +149,19 @@ constexpr int FIXED3_BITS = 40;
 __global__ void k_p2g3_fixed(Step3 s, unsigned long long* q);
 // q (FIXED3_BITS fractional bits) -> the float grid: float(double(q) * 2^-FIXED3_BITS) per component.
 __global__ void k_fixed_to_grid3(const long long* q, float4* grid, int64_t nodes);
+
+// Surface tension (Tension3.java), the passes between the scatter and the grid when a step has tension:
+//   blur    x TENSION3_BLURS: the [1 2 1]^3/64 blur of the node mass taken to a colour (first pass) or of the
+//           last colour, every read held to the wall ring; one thread per node
+//   stress  the capillary stress over sigma from the colour's central differences, six planes of nodes
+//           (txx tyy tzz txy txz tyz)
+//   grid    k_grid3_tension: Flip3.grid plus dt sigma F / max(m, MASS_FLOOR rho0), F the stress's flux across
+//           the node's open faces; writes `vel` for the G2P
+constexpr int TENSION3_BLURS = 6;          // Flip.TENSION_BLURS
+__global__ void k_tension3_colour(const float4* grid, float* colour, const Params3* params, Dims3 d);
+__global__ void k_tension3_blur(const float* src, float* dst, Dims3 d);
+__global__ void k_tension3_stress(const float* colour, float* stress, Dims3 d);
+__global__ void k_grid3_tension(Step3 s, const float* colour, const float* stress);
 
 __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
