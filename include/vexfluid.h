@@ -71,8 +71,10 @@ enum {
     VF_P2G_SHIFT = 16,              /* bits 16..19: the 3D scatter schedule, VF_P2G_* */
     VF_P2G_MASK = 0xfu << 16,
     VF_NO_SORT = 1u << 20,          /* 3D: keep the particles in load order (Flip3Step's behaviour) */
-    VF_TENSION = 1u << 21           /* 3D: surface tension's passes between the scatter and the grid (Flip3Step with
+    VF_TENSION = 1u << 21,          /* 3D: surface tension's passes between the scatter and the grid (Flip3Step with
                                        tension, Flip3Step.java:88-109); its strength is sigma, the params' word 6 */
+    VF_RELAX = 1u << 22             /* 2D: the advect draws J toward the volume the node mass gives (FlipStep with
+                                       relax, Flip.advectRelaxing); the rate is the params' word 11 (Flip.RELAX) */
 };
 #define VF_WALL_STICKY(t) ((uint32_t)(t) << VF_WALL_STICKY_SHIFT)
 
@@ -97,7 +99,8 @@ enum {   /* fields for vf_mpm2_read / vf_mpm2_write (FlipStep.java:95-110 buffer
 
 /* new ParticleSimulation(nx, ny, particles) (ParticleSimulation.java:39-81): nx, ny >= 3
  * (Scatter.java:516-520 needs >= 2; the quadratic stencil needs 3), particles >= 1 (FlipStep.java:86-88).
- * flags: VF_EOS_TAIT, VF_WALL_STICKY(t). The sort's counts start at zero. */
+ * flags: VF_EOS_TAIT, VF_WALL_STICKY(t), VF_RELAX (ParticleSimulation(..., relax)). The sort's counts start at
+ * zero. */
 int32_t vf_mpm2_create(int32_t nx, int32_t ny, int32_t particles, uint32_t flags, vf_mpm2** out);
 /* ParticleSimulation.load (ParticleSimulation.java:129-143): positions, velocities and masses; J = 1, C = 0;
  * params = Flip.params words (>= 5); resets the step count. */

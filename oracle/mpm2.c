@@ -131,12 +131,12 @@ static inline void keep_inside(float* at, float* vel, int size) {
     if (*at > hi) { *at = hi; *vel = fminf(*vel, 0.0f); }
 }
 
-void or_flip2_advect(or_flip2* s, const float* params) {             /* Flip.java:494-545 */
+static void advect2(or_flip2* s, const float* params, int relax) {   /* Flip.java:494-545 */
     const int nx = s->nx, ny = s->ny;
     const float dt = params[P_DT];
     for (int p = 0; p < s->np; p++) {
         stencil2 st = stencil_of(s->x[p], s->y[p], nx, ny);
-        float u = 0, w = 0, b00 = 0, b01 = 0, b10 = 0, b11 = 0;
+        float u = 0, w = 0, b00 = 0, b01 = 0, b10 = 0, b11 = 0, density = 0;
         for (int k = 0; k < 9; k++) {
             float wgt = st.wx[k % 3] * st.wy[k / 3];
             float dx = (float)(k % 3) - st.fx;
@@ -146,6 +146,7 @@ void or_flip2_advect(or_flip2* s, const float* params) {             /* Flip.jav
             float vi = wgt * s->gv[node];
             u = u + ui;
             w = w + vi;
+            if (relax) density = density + wgt * s->gm[node];         /* Flip.java:512-514 */
             b00 = b00 + ui * dx;
             b01 = b01 + ui * dy;
             b10 = b10 + vi * dx;
@@ -159,15 +160,30 @@ void or_flip2_advect(or_flip2* s, const float* params) {             /* Flip.jav
         s->x[p] = x; s->y[p] = y; s->u[p] = u; s->v[p] = w;
         s->c00[p] = c00; s->c01[p] = c01; s->c10[p] = c10; s->c11[p] = c11;
         float j = s->j[p] * (1.0f + dt * (c00 + c11));
+        if (relax && density > OR_RELAX_MIN_DENSITY * params[P_RHO0]) {   /* Flip.java:538-543 */
+            float measured = params[P_RHO0] / density;
+            j = j + (params[OR_P_RELAX] * dt) * (measured - j);
+        }
         s->j[p] = clampf(j, 1.0f / J_BOUND, J_BOUND);
     }
 }
+
+void or_flip2_advect(or_flip2* s, const float* params) { advect2(s, params, 0); }
+
+void or_flip2_advect_relaxing(or_flip2* s, const float* params) { advect2(s, params, 1); }
 
 void or_flip2_step(or_flip2* s, const float* params, or_physics ph) {   /* FlipStep.java:127-169 */
     or_flip2_clear(s);
     or_flip2_scatter(s, params, ph);
     or_flip2_grid(s, params, ph);
     or_flip2_advect(s, params);
+}
+
+void or_flip2_step_relaxing(or_flip2* s, const float* params, or_physics ph) {   /* FlipStep.java:163-166 */
+    or_flip2_clear(s);
+    or_flip2_scatter(s, params, ph);
+    or_flip2_grid(s, params, ph);
+    or_flip2_advect_relaxing(s, params);
 }
 
 /* ------------------------------------------------------------------ the sort by cell */

@@ -66,6 +66,13 @@ void or_flip2_scatter(or_flip2* s, const float* params, or_physics ph);     /* F
 void or_flip2_grid(or_flip2* s, const float* params, or_physics ph);        /* Flip.java:366-412 */
 void or_flip2_advect(or_flip2* s, const float* params);                     /* Flip.java:494-559 */
 void or_flip2_step(or_flip2* s, const float* params, or_physics ph);        /* FlipStep.step(): clear, scatter, grid, advect */
+/* Flip.advectRelaxing (Flip.java:451-464, 512-543): J drawn toward rho0 / (the stencil's mass density) at the
+ * params' RELAX word per second, where that density is at least OR_RELAX_MIN_DENSITY of rest; and FlipStep's
+ * step built with relax. params: >= 12 words. */
+#define OR_P_RELAX 11               /* Flip.java:113 */
+#define OR_RELAX_MIN_DENSITY 0.8f   /* Flip.java:449 */
+void or_flip2_advect_relaxing(or_flip2* s, const float* params);
+void or_flip2_step_relaxing(or_flip2* s, const float* params, or_physics ph);
 
 /* 2D sort key and stable counting sort (Scatter.java:458-502, FlipStep.java:183-192).
  * cells = (nx-1)(ny-1); starts has cells+1 words. The permutation is stable by key. */

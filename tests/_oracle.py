@@ -70,6 +70,7 @@ def lib():
             subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
         L = ctypes.CDLL(str(so))
         L.or_flip2_step.argtypes = [ctypes.POINTER(OrFlip2), f32p, OrPhysics]
+        L.or_flip2_step_relaxing.argtypes = [ctypes.POINTER(OrFlip2), f32p, OrPhysics]
         for n in ("or_flip2_scatter", "or_flip2_grid"):
             getattr(L, n).argtypes = [ctypes.POINTER(OrFlip2), f32p, OrPhysics]
         L.or_flip2_clear.argtypes = [ctypes.POINTER(OrFlip2)]
@@ -337,6 +338,33 @@ def drop_pressure(make, n=40, radius=8.0, sigma=0.0, sound=200.0):
     return total / samples, 2 * sigma / effective, effective, drift, fastest
 
 
+def relax_box(seed=21, n=48, fill=45, ppc=4):
+    """RelaxTest's full box (RelaxTest.java:27-49): fill x fill cells of ppc particles from the wall, mass 1/ppc,
+    J = 0.9. Returns x, y, m, j."""
+    r = JavaRandom(seed)
+    count = fill * fill * ppc
+    x, y = np.empty(count, F), np.empty(count, F)
+    k = 0
+    for row in range(fill):
+        for col in range(fill):
+            for _ in range(ppc):
+                x[k] = (WALL + F(col)) + r.next_float() * F(0.999)
+                y[k] = (WALL + F(row)) + r.next_float() * F(0.999)
+                k += 1
+    return x, y, np.full(count, F(1.0 / ppc), F), np.full(count, F(0.9), F)
+
+
+def relax_median_j(run, relax):
+    """RelaxTest.medianJ (RelaxTest.java:27-65): the box stepped for 0.5 s, sorted every 10 steps, by
+    ``run(x, y, m, j, params, steps)``, which returns the particles' J; the median J."""
+    bulk = 200.0 ** 2
+    dt = stable_step(bulk, 1, 20, 0.3)
+    params = flip_params(dt, 0, 0, bulk, 1)
+    params[11] = relax
+    j = np.sort(run(*relax_box(), params, math.ceil(0.5 / dt)))
+    return float(j[len(j) // 2])
+
+
 def check_laplace(pressure):
     """Tension3Test.aDropsPressureIsTwiceSigmaOverItsRadius's bounds (Tension3Test.java:127-150); ``pressure(radius,
     sigma)`` is drop_pressure over one step implementation."""
@@ -487,8 +515,10 @@ class Flip2State:
         self.s = OrFlip2(nx, ny, self.np, *[fp(self.a[f]) for f in self.FIELDS],
                          *[fp(self.g[f]) for f in ("gm", "gmu", "gmv", "gu", "gv")])
 
-    def step(self, params, physics=(0, 0)):
-        lib().or_flip2_step(ctypes.byref(self.s), fp(np.ascontiguousarray(params, F)), OrPhysics(*physics))
+    def step(self, params, physics=(0, 0), relax=False):
+        """One FlipStep step; with ``relax``, the step built with relaxation (Flip.advectRelaxing)."""
+        step = lib().or_flip2_step_relaxing if relax else lib().or_flip2_step
+        step(ctypes.byref(self.s), fp(np.ascontiguousarray(params, F)), OrPhysics(*physics))
 
     def sort(self):
         cells = (self.nx - 1) * (self.ny - 1)

@@ -1,5 +1,5 @@
 """2D MLS-MPM and the 2D scatter schedules on the GPU, against the oracle and the reference's FlipTest,
-ScatterTest, SortTest and FixedScatterTest (vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/).
+ScatterTest, SortTest, FixedScatterTest and RelaxTest (vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/).
 
 Tolerances: per node 1e-5 * max(1, |expected|) against the f64 reference (ScatterTest.java:140); sort starts
 and permutation bit-exact; fixed-point grids bit-exact."""
@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import vexfluid as vf
-from _oracle import F, Flip2State, JavaRandom, Particles, cells2, flip_column, lib as olib, fp, ip
+from _oracle import F, Flip2State, JavaRandom, Particles, cells2, flip_column, lib as olib, fp, ip, relax_median_j
 from test_oracle_mpm import (broken_runs, check_flip2_dam_break, flip2_dam_break, holds_what_the_particles_did,
                              scatter_reference)
 
@@ -219,3 +219,49 @@ def test_the_2d_configuration_matches_the_oracle():
             got = s.read(key)
             assert np.all(np.abs(got - e) <= 1e-4 * np.abs(e)), key
         assert np.array_equal(s.read("m"), o.a["m"])
+
+
+def test_relaxation_draws_j_to_the_volume_the_mass_gives_on_the_device():
+    """RelaxTest.jIsDrawnToTheVolumeTheMassGivesAndOnlyIfAskedTo (RelaxTest.java:67-80) with its bounds: J started
+    at 0.9 in a box full wall to wall stays within 0.05 of 0.9 at rate 0 and is drawn into (0.97, 1.03) at rate 8."""
+    def run(x, y, m, j, params, steps):
+        with vf.ParticleSimulation(48, 48, len(x), relax=True) as s:
+            s.load(x, y, np.zeros_like(x), np.zeros_like(x), m, params.view(np.int32))
+            s.write("j", j)
+            s.advance(steps, 10)
+            return s.read("j")
+
+    without = relax_median_j(run, 0.0)
+    relaxed = relax_median_j(run, 8.0)
+    assert abs(without - 0.9) <= 0.05, f"J moved by itself to {without}"
+    assert 0.97 < relaxed < 1.03, f"relaxed J is {relaxed}, not 1"
+
+
+def test_relaxing_steps_match_the_oracle():
+    """A falling column with J started at 0.9 and relaxation at rate 8: one step's J per particle within 1e-5, and
+    100 steps' positions and J within 1e-4 relative of the oracle's relaxing step (sorted every 10 on both sides)."""
+    n = 32
+    x, y, m = flip_column(71)
+    fall = math.sqrt(2 * 200 * 16)
+    bulk = (5 * fall) ** 2
+    dt = 0.3 / (math.sqrt(bulk) + fall)
+    params = vf.flip_params(dt, 0, -200, bulk, 1, relax=8.0)
+    j0 = np.full(len(x), F(0.9), F)
+    o = Flip2State(n, n, x, y, m, j=j0)
+    with vf.ParticleSimulation(n, n, len(x), relax=True) as s:
+        s.load(x, y, np.zeros_like(x), np.zeros_like(x), m, params)
+        s.write("j", j0)
+        s.advance(1, 10)
+        o.sort()
+        o.step(params.view(F), relax=True)
+        assert np.all(np.abs(s.read("j") - o.a["j"]) <= 1e-5)
+        assert np.any(s.read("j") != j0)
+        s.advance(99, 10)
+        for k in range(1, 100):
+            if k % 10 == 0:
+                o.sort()
+            o.step(params.view(F), relax=True)
+        for key in ("x", "y", "j"):
+            e = o.a[key]
+            got = s.read(key)
+            assert np.all(np.abs(got - e) <= 1e-4 * np.abs(e)), key

@@ -1,7 +1,7 @@
 """The oracle pinned by the reference's own particle tests.
 
 Each test restates one reference test (FlipTest, Flip3Test, ScatterTest, SortTest,
-FixedScatterTest, Tension3Test, under vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/)
+FixedScatterTest, Tension3Test, RelaxTest, under vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/particle/)
 with its seeded inputs regenerated by the java.util.Random restatement, and applies the
 reference's assertions to the oracle. A test here failing means the restatement is wrong,
 not the kernels.
@@ -13,8 +13,8 @@ import numpy as np
 import pytest
 
 from _oracle import (F, WALL, Flip2State, Flip3State, JavaRandom, OrPhysics, Particles, cells2, check_laplace,
-                     drop3, drop_pressure, flip3_params, flip_column, flip_params, fp, ip, key3, lib, slab3,
-                     stable_step)
+                     drop3, drop_pressure, flip3_params, flip_column, flip_params, fp, ip, key3, lib,
+                     relax_median_j, slab3, stable_step)
 
 
 # ---------------------------------------------------------------------------------- FlipTest
@@ -418,3 +418,21 @@ def test_oracle_tension_without_sigma_is_the_plain_grid():
         moved |= o.g[k] != plain.g[k]
     assert moved.any()
     assert not (moved & (o.g["gm"] <= 1e-9)).any()
+
+
+def test_oracle_relaxation_draws_j_to_the_volume_the_mass_gives():
+    """Pins the relaxing advect on RelaxTest.jIsDrawnToTheVolumeTheMassGivesAndOnlyIfAskedTo (RelaxTest.java:67-80):
+    a box full wall to wall with every J at 0.9 keeps J within 0.05 of 0.9 at rate 0, and is drawn into
+    (0.97, 1.03) at rate 8, after 0.5 s sorted every 10 steps."""
+    def run(x, y, m, j, params, steps):
+        o = Flip2State(48, 48, x, y, m, j=j)
+        for s in range(steps):
+            if s % 10 == 0:
+                o.sort()
+            o.step(params, relax=True)
+        return o.a["j"]
+
+    without = relax_median_j(run, 0.0)
+    relaxed = relax_median_j(run, 8.0)
+    assert abs(without - 0.9) <= 0.05, f"J moved by itself to {without}"
+    assert 0.97 < relaxed < 1.03, f"relaxed J is {relaxed}, not 1"

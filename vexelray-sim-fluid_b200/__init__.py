@@ -34,6 +34,7 @@ VF_WALL_STICKY_SHIFT = 8
 VF_P2G_SHIFT = 16
 VF_NO_SORT = 1 << 20
 VF_TENSION = 1 << 21
+VF_RELAX = 1 << 22
 VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED = 0, 1, 2, 3
 VF_SCATTER_GRID, VF_SCATTER_PRE_REDUCED, VF_SCATTER_GATHER, VF_SCATTER_SEGMENTED = 0, 1, 2, 3
 VF3_PASS_SORT, VF3_PASS_CLEAR, VF3_PASS_SCATTER, VF3_PASS_GRID, VF3_PASS_ADVECT = 1, 2, 4, 8, 16
@@ -335,14 +336,16 @@ class Pinned:
 
 # ------------------------------------------------------------------------------------- params
 
-def flip_params(dt, gx, gy, bulk, rho0, sigma=0.0) -> np.ndarray:
-    """Flip.params (Flip.java:145-211): 28 words of f32 bits."""
+def flip_params(dt, gx, gy, bulk, rho0, sigma=0.0, relax=0.0) -> np.ndarray:
+    """Flip.params (Flip.java:145-211): 28 words of f32 bits; ``relax`` is word 11 (Flip.RELAX), the rate at
+    which a step built with relaxation draws J toward the volume the mass gives."""
     if not (dt > 0) or not (bulk >= 0) or not (rho0 > 0):
         raise IllegalArgumentException(VF_EINVAL, f"dt > 0, bulk >= 0 and rho0 > 0, got dt {dt}, bulk {bulk}, "
                                                   f"rho0 {rho0}")
     w = np.zeros(28, np.int32)
     for k, v in enumerate((dt, gx, gy, bulk, rho0, sigma)):
         w[k] = _bits(v)
+    w[11] = _bits(relax)
     return w
 
 
@@ -386,10 +389,10 @@ def seconds(t: int) -> float:
 class ParticleSimulation:
     """ParticleSimulation (ParticleSimulation.java): a 2D particle fluid in one walled box on the GPU."""
 
-    def __init__(self, nx: int, ny: int, particles: int, *, tait: bool = False, sticky: int = 0):
+    def __init__(self, nx: int, ny: int, particles: int, *, tait: bool = False, sticky: int = 0, relax: bool = False):
         L = lib()
         h = _vp()
-        flags = (VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT)
+        flags = (VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT) | (VF_RELAX if relax else 0)
         check(L.vf_mpm2_create(nx, ny, particles, flags, ctypes.byref(h)))
         self._h = h
         self._nx, self._ny, self._np = nx, ny, particles

@@ -500,7 +500,8 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
                 Advected2 a;
                 if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
                     const int wb = ly * wx + lx;
-                    a = advect2(sn, px, py, pj, nx, ny, prm, [&](int o) { return vw[wb + (o / 3) * wx + o % 3]; });
+                    a = advect2(sn, px, py, pj, nx, ny, prm, [&](int o) { return vw[wb + (o / 3) * wx + o % 3]; },
+                                [](int) { return 0.0f; });
                 } else {
                     set_status(B.status, ST_OOB);
                     a = Advected2{px, py, in[PU * st + src], in[PV * st + src], in[PC00 * st + src],
@@ -719,6 +720,7 @@ int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t 
     VF_REQUIRE(out, VF_EINVAL, "out is null");
     *out = nullptr;
     VF_REQUIRE(scenes && nscenes >= 1, VF_EINVAL, "a batch needs scenes, got %d", nscenes);
+    VF_REQUIRE(!(flags & (VF_RELAX | VF_TENSION)), VF_EINVAL, "a batch steps plain scenes: no relaxation or tension");
     if (block == 0) block = 256;
     VF_REQUIRE(block_ok(block), VF_EINVAL, "block %d is not one of VF_BATCH_BLOCKS", block);
     std::vector<Scene2> sc((size_t)nscenes);

@@ -92,10 +92,13 @@ __global__ void __launch_bounds__(256) k_flip2_advect(float* __restrict__ p, int
     const Params2 q = *prm;
     const float px = p[PX * st + i], py = p[PY * st + i];
     const Stencil2 s = stencil2(px, py, nx, ny);
-    const Advected2 a = advect2(s, px, py, p[PJ * st + i], nx, ny, q, [&](int k) {
-        const int node = s.base + (k / 3) * nx + k % 3;
-        return make_float2(g.gu[node], g.gv[node]);
-    });
+    const Advected2 a = advect2(
+        s, px, py, p[PJ * st + i], nx, ny, q,
+        [&](int k) {
+            const int node = s.base + (k / 3) * nx + k % 3;
+            return make_float2(g.gu[node], g.gv[node]);
+        },
+        [&](int k) { return g.gm[s.base + (k / 3) * nx + k % 3]; });
     p[PX * st + i] = a.x;
     p[PY * st + i] = a.y;
     p[PU * st + i] = a.u;
@@ -339,7 +342,8 @@ int32_t upload_params2(vf_mpm2* h, const int32_t* params, int32_t nparams) {
     VF_REQUIRE(w[0] > 0 && w[3] >= 0 && w[4] > 0, VF_EINVAL,      // Flip.java:204-207
                "dt > 0, bulk >= 0 and rho0 > 0, got dt %g, bulk %g, rho0 %g", w[0], w[3], w[4]);
     Params2 p{w[0], w[1], w[2], w[3], w[4], (h->flags & VF_EOS_TAIT) ? 1 : 0,
-              (int)((h->flags & VF_WALL_STICKY_MASK) >> VF_WALL_STICKY_SHIFT)};
+              (int)((h->flags & VF_WALL_STICKY_MASK) >> VF_WALL_STICKY_SHIFT),
+              nparams > 11 ? bits_to_float(params[11]) : 0.0f, (h->flags & VF_RELAX) ? 1 : 0};
     VF_TRY_CUDA(cudaMemcpyAsync(h->params.ptr, &p, sizeof p, cudaMemcpyHostToDevice, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     return VF_OK;

@@ -14,10 +14,13 @@ enum Field2 { PX = 0, PY, PU, PV, PM, PJ, PC00, PC01, PC10, PC11, NF2 };
 struct Params2 {
     float dt, gx, gy, bulk, rho0;
     int tait, sticky;
+    float relax;     // Flip.params' RELAX word (Flip.java:113): J's pull toward the mass's volume, per second
+    int relaxing;    // VF_RELAX: the step's advect is Flip.advectRelaxing
 };
 
 constexpr float EMPTY2 = 1e-9f;     // Flip.java:316
 constexpr float J_BOUND2 = 10.0f;   // Flip.java:430
+constexpr float RELAX_MIN_DENSITY2 = 0.8f;   // Flip.java:449
 
 // Flip.Stencil.of (Flip.java:572-581): the lower-left node of the 3x3 stencil, the offsets in
 // [1/2, 3/2] and the quadratic B-spline weights per axis.
@@ -146,15 +149,17 @@ __device__ __forceinline__ void keep_inside2(float& at, float& vel, int size) {
 
 // Flip.advectBody (Flip.java:494-545) of one particle, given its stencil and the node velocities
 // through vel(k) for stencil node k: the velocity and affine matrix gathered, the position moved
-// and kept inside, J updated and clamped.
+// and kept inside, J updated and clamped. With q.relaxing (Flip.advectRelaxing, Flip.java:451-464, 512-541),
+// the stencil's mass density(k) summed too, and J drawn toward rho0 / density at q.relax per second wherever
+// that density is at least RELAX_MIN_DENSITY2 of rest.
 struct Advected2 {
     float x, y, u, w, c00, c01, c10, c11, j;
 };
 
-template <class Vel>
+template <class Vel, class Mass>
 __device__ __forceinline__ Advected2 advect2(const Stencil2& s, float px, float py, float pj, int nx, int ny,
-                                             const Params2& q, Vel vel) {
-    float u = 0, w = 0, b00 = 0, b01 = 0, b10 = 0, b11 = 0;
+                                             const Params2& q, Vel vel, Mass mass) {
+    float u = 0, w = 0, b00 = 0, b01 = 0, b10 = 0, b11 = 0, density = 0;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
         const float wgt = s.wx[k % 3] * s.wy[k / 3];
@@ -163,6 +168,7 @@ __device__ __forceinline__ Advected2 advect2(const Stencil2& s, float px, float 
         const float ui = wgt * g.x, vi = wgt * g.y;
         u += ui;
         w += vi;
+        if (q.relaxing) density = __fadd_rn(density, __fmul_rn(wgt, mass(k)));
         b00 += ui * dx;
         b01 += ui * dy;
         b10 += vi * dx;
@@ -179,7 +185,11 @@ __device__ __forceinline__ Advected2 advect2(const Stencil2& s, float px, float 
     keep_inside2(a.y, w, ny);
     a.u = u;
     a.w = w;
-    const float j = pj * (1.0f + q.dt * (a.c00 + a.c11));
+    float j = pj * (1.0f + q.dt * (a.c00 + a.c11));
+    if (q.relaxing && density > __fmul_rn(RELAX_MIN_DENSITY2, q.rho0)) {
+        const float measured = __fdiv_rn(q.rho0, density);
+        j = __fadd_rn(j, __fmul_rn(__fmul_rn(q.relax, q.dt), __fsub_rn(measured, j)));
+    }
     a.j = clampf(j, 1.0f / J_BOUND2, J_BOUND2);
     return a;
 }
