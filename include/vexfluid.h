@@ -225,6 +225,18 @@ enum {   /* fields (Flip3.PARTICLE, Flip3.java:112-115; grid names Flip3Step.jav
  * With VF_TENSION the grid readouts VF3_GU..GW include the tension's force. */
 int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
                         vf_mpm3_prepared** out);
+/* As vf_mpm3_prepare, with the grid stored sparsely: no counterpart in the reference, which plans it
+ * (docs/sparse-fluid.md:19-62). The nodes live in a pool of pool_bricks bricks of 8^3 nodes (8 KB each, two pools,
+ * one per step parity) through a page table over the domain's bricks, rebuilt every step from the bricks the
+ * particles' stencils reach; memory for the grid follows the fluid, not the box. The tiled schedule only, sorted,
+ * without tension (VF_EINVAL otherwise). A step that needs more bricks than the pool holds skips the nodes of the
+ * bricks past it and reports VF_EDEVICE (status bit 8) at the next blocking call. Readouts of the grid unpack the
+ * pool into a dense box made on first use. pool_bricks above the domain's brick count is cut to it. */
+int32_t vf_mpm3_prepare_sparse(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
+                               int32_t pool_bricks, vf_mpm3_prepared** out);
+/* The bricks the last scatter took from the pool (blocking; VF_ESTATE for a dense grid), and the pool's size. */
+int32_t vf_mpm3_pool_used(vf_mpm3* h, int32_t* used);
+int32_t vf_mpm3_pool_capacity(const vf_mpm3* h);
 /* Prepared.close (ParticleSimulation3.java:94-102): frees a preparation never finished. Idempotent. */
 void vf_mpm3_prepared_close(vf_mpm3_prepared* p);
 /* new ParticleSimulation3(Prepared) (ParticleSimulation3.java:181-190), on the owning thread: clears the

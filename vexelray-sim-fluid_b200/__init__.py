@@ -129,6 +129,10 @@ def lib() -> ctypes.CDLL:
                               + [_i32p] * 3, ctypes.c_int32),
         "vf_sort2": ([ctypes.c_int32] * 2 + [_f32p] * 2 + [ctypes.c_int64, _i32p, _i32p], ctypes.c_int32),
         "vf_mpm3_prepare": ([ctypes.c_int32] * 4 + [ctypes.c_uint32, ctypes.POINTER(_vp)], ctypes.c_int32),
+        "vf_mpm3_prepare_sparse": ([ctypes.c_int32] * 4 + [ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(_vp)],
+                                   ctypes.c_int32),
+        "vf_mpm3_pool_used": ([_vp, _i32p], ctypes.c_int32),
+        "vf_mpm3_pool_capacity": ([_vp], ctypes.c_int32),
         "vf_mpm3_prepared_close": ([_vp], None),
         "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm3_load": ([_vp] + [_f32p] * 7 + [_i32p, ctypes.c_int32], ctypes.c_int32),
@@ -779,15 +783,20 @@ class ParticleSimulation3:
     ``sort=False`` keeps the particles in load order, as the reference's Flip3Step does.
     ``tension=True`` adds surface tension's passes (ParticleSimulation3(..., tension)); its strength is sigma, the
     seventh params word (``flip3_params(..., sigma)``).
+    ``pool_bricks=N`` stores the grid sparsely, in a pool of N bricks of 8^3 nodes through a page table over the
+    domain (the tiled schedule only, without tension); ``pool_used()`` is what the last step took.
     """
 
     @staticmethod
     def prepare(nx, ny, nz, particles, *, tait=False, sticky=0, schedule=VF_P2G_TILE, sort=True,
-                tension=False) -> Prepared:
+                tension=False, pool_bricks=None) -> Prepared:
         flags = ((VF_EOS_TAIT if tait else 0) | (int(sticky) << VF_WALL_STICKY_SHIFT) | (schedule << VF_P2G_SHIFT)
                  | (0 if sort else VF_NO_SORT) | (VF_TENSION if tension else 0))
         p = _vp()
-        check(lib().vf_mpm3_prepare(nx, ny, nz, particles, flags, ctypes.byref(p)))
+        if pool_bricks is None:
+            check(lib().vf_mpm3_prepare(nx, ny, nz, particles, flags, ctypes.byref(p)))
+        else:
+            check(lib().vf_mpm3_prepare_sparse(nx, ny, nz, particles, flags, int(pool_bricks), ctypes.byref(p)))
         return Prepared(p, nx, ny, nz, particles)
 
     def __init__(self, nx_or_prepared, ny=None, nz=None, particles=None, **kw):
@@ -905,6 +914,14 @@ class ParticleSimulation3:
     def restore(self, blob: bytes) -> None:
         """Resume from snapshot(); the grid, particle count and physics flags must match (ValueError otherwise)."""
         check(lib().vf_mpm3_restore(self._h, blob, len(blob)))
+
+    def pool_used(self) -> int:
+        out = ctypes.c_int32()
+        check(lib().vf_mpm3_pool_used(self._h, ctypes.byref(out)))
+        return out.value
+
+    def pool_capacity(self) -> int:
+        return int(lib().vf_mpm3_pool_capacity(self._h))
 
     def touched_nodes(self) -> int:
         out = ctypes.c_int64()

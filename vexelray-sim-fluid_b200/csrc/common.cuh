@@ -53,7 +53,8 @@ EncodeTiled tensor_map_encoder();
 enum : uint32_t {
     ST_OOB = 1u << 0,        // an index fell outside its buffer; the access was skipped
     ST_TIMEOUT = 1u << 1,    // a bounded wait gave up
-    ST_RANK = 1u << 2        // a sort rank fell outside its cell's run
+    ST_RANK = 1u << 2,       // a sort rank fell outside its cell's run
+    ST_POOL = 1u << 3        // a step needed more grid bricks than the sparse pool holds; their nodes were skipped
 };
 
 // ------------------------------------------------------------------ device helpers

@@ -50,6 +50,16 @@ struct vf_mpm3 {
     bool tension = false;     // VF_TENSION: Tension3's passes between the scatter and the grid
     DeviceBuffer colour[2];   // the blurs' ping-pong colour planes, nodes floats each
     DeviceBuffer stress;      // txx tyy tzz txy txz tyz, nodes floats each
+    // sparse node storage (vf_mpm3_prepare_sparse): grid[g] is a pool of pool_cap bricks of 8^3 nodes and page[g]
+    // maps the domain's brick positions (pnx x pny x pnz) into it, rebuilt by every scatter into grid[g]
+    bool sparse = false;
+    int pool_cap = 0;
+    int pnx = 0, pny = 0, pnz = 0;
+    int npages = 0;
+    DeviceBuffer page[2], mark;
+    DeviceBuffer n_used;      // int[2]: the slots the last scatter into each pool took
+    DeviceBuffer view;        // sparse: the last grid unpacked into the dense box for readouts, made on first use
+    bool view_fresh = false;  // `view` holds the last grid
     bool fixed_valid = false; // `fixed` holds the last scatter's sums
     Params3 hparams{};
     int64_t steps = 0;
@@ -112,6 +122,11 @@ Step3 make_step(vf_mpm3* h) {
     s.brick_start = h->brick_start.as<int>();
     s.nkeys = h->nkeys;
     s.nbricks = h->nbricks;
+    s.sparse = h->sparse ? 1 : 0;
+    s.pool_cap = h->pool_cap;
+    s.pnx = h->pnx;
+    s.pny = h->pny;
+    s.pnz = h->pnz;
     return s;
 }
 
@@ -156,17 +171,27 @@ int32_t run_sort(vf_mpm3* h, int g, bool will_scatter, bool fused_fixup) {
     // the old windows of grid[g] must be cleared before its brick list is overwritten; a sort with
     // no scatter after it leaves the grid alone and marks it for a dense clear instead
     if (h->grid_dirty[g] == 1 && !will_scatter) h->grid_dirty[g] = 2;
+    s.grid = h->grid[g].as<float4>();
+    s.active = h->active[g].as<int>();
+    s.n_active = h->n_active.as<int>() + g;
     if (h->grid_dirty[g] == 1) {
-        s.grid = h->grid[g].as<float4>();
-        s.active = h->active[g].as<int>();
-        s.n_active = h->n_active.as<int>() + g;
-        VF_LAUNCH(h->prof, "k_clear_bricks3", h->stream, k_clear_bricks3, persistent_blocks(8), 256, 0, s);
+        if (h->sparse)
+            VF_LAUNCH(h->prof, "k_pool_clear3", h->stream, k_pool_clear3, persistent_blocks(8), 256, 0, s.grid,
+                      h->n_used.as<int>() + g);
+        else
+            VF_LAUNCH(h->prof, "k_clear_bricks3", h->stream, k_clear_bricks3, persistent_blocks(8), 256, 0, s);
         h->grid_dirty[g] = 0;
     }
     int* active = h->active[g].as<int>();
     int* n_active = h->n_active.as<int>() + g;
     VF_LAUNCH(h->prof, "k_brick_scan", h->stream, k_brick_scan, 1, 1024, 0, h->brick_count.as<int>(), h->brick_start.as<int>(), active, n_active,
                                            h->nbricks);
+    if (h->sparse && will_scatter) {
+        // the page of grid[g] for this step: the node bricks the non-empty cell bricks' windows reach
+        VF_LAUNCH(h->prof, "k_pool_mark3", h->stream, k_pool_mark3, persistent_blocks(2), 256, 0, s, h->mark.as<int>());
+        VF_LAUNCH(h->prof, "k_pool_page3", h->stream, k_pool_page3, 1, 1024, 0, h->mark.as<int>(), h->page[g].as<int>(),
+                  h->npages, h->n_used.as<int>() + g, h->pool_cap, h->status.as<uint32_t>());
+    }
     VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(),
               h->cell_start.as<int>(), h->cursor.as<int>(),
                                                           h->brick_start.as<int>(), active, n_active);
@@ -199,6 +224,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     s.grid = h->grid[g].as<float4>();
     s.active = h->active[g].as<int>();
     s.n_active = h->n_active.as<int>() + g;
+    s.page = h->sparse ? h->page[g].as<int>() : nullptr;
     if (sort) {
         s.perm = h->perm.as<int>();
         s.out = h->part[h->cur ^ 1].as<float>();
@@ -233,6 +259,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
         VF_CHECK_LAUNCH();
         h->grid_dirty[g] = tile ? 1 : 2;
         h->grid_last = g;
+        h->view_fresh = false;
         h->fixed_valid = h->p2g == VF_P2G_FIXED;
     }
     if (mask & VF3_PASS_ADVECT) {
@@ -271,9 +298,34 @@ int32_t check_status(vf_mpm3* h) {
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     if (st) {
         VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
-        set_error("a kernel flagged device status 0x%x (1 index out of range, 2 wait timeout, 4 sort rank)", st);
+        set_error("a kernel flagged device status 0x%x (1 index out of range, 2 wait timeout, 4 sort rank, 8 the "
+                  "sparse grid's brick pool is full)", st);
         return VF_EDEVICE;
     }
+    return VF_OK;
+}
+
+// The last scatter's grid as the dense box: grid[grid_last], or for sparse storage the pool unpacked through its
+// page into `view` (allocated on first use, unpacked once per scatter).
+int32_t last_grid(vf_mpm3* h, float4** out) {
+    if (!h->sparse) {
+        *out = h->grid[h->grid_last].as<float4>();
+        return VF_OK;
+    }
+    if (!h->view.ptr) {
+        int32_t rc = h->view.alloc((size_t)h->nodes * 16);
+        if (rc) return rc;
+        VF_TRY_CUDA(cudaMemsetAsync(h->view.ptr, 0, h->view.bytes, h->stream));
+    }
+    if (!h->view_fresh) {
+        Step3 s = make_step(h);
+        s.grid = h->grid[h->grid_last].as<float4>();
+        s.page = h->page[h->grid_last].as<int>();
+        k_pool_unpack3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(s, h->view.as<float4>());
+        VF_CHECK_LAUNCH();
+        h->view_fresh = true;
+    }
+    *out = h->view.as<float4>();
     return VF_OK;
 }
 
@@ -291,8 +343,12 @@ int32_t field_pointer(vf_mpm3* h, int32_t field, float** ptr, int64_t* n) {
 
 extern "C" {
 
-int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
-                        vf_mpm3_prepared** out) {
+}  // extern "C"
+
+namespace {
+
+int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags, int32_t pool_bricks,
+                 vf_mpm3_prepared** out) {
     VF_REQUIRE(out, VF_EINVAL, "out is null");
     *out = nullptr;
     VF_REQUIRE(particles >= 1, VF_EINVAL, "a step needs particles, got %d", particles);
@@ -300,6 +356,9 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
                nx, ny, nz);
     int p2g = (int)((flags & VF_P2G_MASK) >> VF_P2G_SHIFT);
     VF_REQUIRE(p2g <= VF_P2G_FIXED, VF_EINVAL, "no scatter schedule %d", p2g);
+    VF_REQUIRE(pool_bricks == 0 || (p2g == VF_P2G_TILE && !(flags & (VF_NO_SORT | VF_TENSION))), VF_EINVAL,
+               "sparse storage runs the sorted tiled schedule without tension");
+    VF_REQUIRE(pool_bricks >= 0, VF_EINVAL, "a pool needs bricks, got %d", pool_bricks);
     int32_t rc = require_device();
     if (rc) return rc;
     vf_mpm3* h = new vf_mpm3();
@@ -320,6 +379,13 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
     h->nkeys = (int64_t)h->nbricks * 512;
     h->nodes = (int64_t)nx * ny * nz;
     h->stride = ((int64_t)particles + 63) / 64 * 64;
+    h->sparse = pool_bricks > 0;
+    h->pnx = (nx + POOL_BRICK - 1) / POOL_BRICK;
+    h->pny = (ny + POOL_BRICK - 1) / POOL_BRICK;
+    h->pnz = (nz + POOL_BRICK - 1) / POOL_BRICK;
+    h->npages = h->pnx * h->pny * h->pnz;
+    h->pool_cap = h->sparse ? std::min(pool_bricks, h->npages) : 0;
+    const size_t grid_bytes = h->sparse ? (size_t)h->pool_cap * POOL_NODES * 16 : (size_t)h->nodes * 16;
     auto fail = [&](int32_t code) {
         delete h;
         return code;
@@ -336,9 +402,12 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
         (rc = h->brick_count.alloc((size_t)h->nbricks * 4)) ||
         (rc = h->brick_start.alloc((size_t)(h->nbricks + 1) * 4)) ||
         (rc = h->active[0].alloc((size_t)h->nbricks * 4)) || (rc = h->active[1].alloc((size_t)h->nbricks * 4)) ||
-        (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc((size_t)h->nodes * 16)) ||
-        (rc = h->grid[1].alloc((size_t)h->nodes * 16)) || (rc = h->vel.alloc((size_t)h->nodes * 16)) ||
+        (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc(grid_bytes)) ||
+        (rc = h->grid[1].alloc(grid_bytes)) || (!h->sparse && (rc = h->vel.alloc((size_t)h->nodes * 16))) ||
         (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)))
+        return fail(rc);
+    if (h->sparse && ((rc = h->page[0].alloc((size_t)h->npages * 4)) || (rc = h->page[1].alloc((size_t)h->npages * 4)) ||
+                      (rc = h->mark.alloc((size_t)h->npages * 4)) || (rc = h->n_used.alloc(2 * sizeof(int)))))
         return fail(rc);
     h->tension = (flags & VF_TENSION) != 0;
     if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
@@ -354,6 +423,31 @@ int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, u
     *out = p;
     return VF_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+int32_t vf_mpm3_prepare(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
+                        vf_mpm3_prepared** out) {
+    return prepare3(nx, ny, nz, particles, flags, 0, out);
+}
+
+int32_t vf_mpm3_prepare_sparse(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t flags,
+                               int32_t pool_bricks, vf_mpm3_prepared** out) {
+    VF_REQUIRE(pool_bricks >= 1, VF_EINVAL, "a sparse grid needs a pool of at least one brick, got %d", pool_bricks);
+    return prepare3(nx, ny, nz, particles, flags, pool_bricks, out);
+}
+
+int32_t vf_mpm3_pool_used(vf_mpm3* h, int32_t* used) {
+    VF_REQUIRE(h && used, VF_EINVAL, "null argument");
+    VF_REQUIRE(h->sparse, VF_ESTATE, "this simulation's grid is dense");
+    VF_TRY_CUDA(cudaMemcpyAsync(used, h->n_used.as<int>() + h->grid_last, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
+int32_t vf_mpm3_pool_capacity(const vf_mpm3* h) { return h ? h->pool_cap : 0; }
 
 void vf_mpm3_prepared_close(vf_mpm3_prepared* p) {
     if (!p) return;
@@ -375,8 +469,16 @@ int32_t vf_mpm3_create(vf_mpm3_prepared* p, vf_mpm3** out) {
     // ParticleSimulation3(Prepared) clears every buffer (runner.clear(), ParticleSimulation3.java:189)
     for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->cursor, &h->perm, &h->cell_count, &h->cell_start,
                             &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
-                            &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch}) {
-        if (cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream) != cudaSuccess) {
+                            &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch, &h->mark,
+                            &h->n_used}) {
+        if (b->ptr && cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream) != cudaSuccess) {
+            set_error("clearing buffers failed");
+            vf_mpm3_destroy(h);
+            return VF_ECUDA;
+        }
+    }
+    for (DeviceBuffer* b : {&h->page[0], &h->page[1]}) {
+        if (b->ptr && cudaMemsetAsync(b->ptr, 0xff, b->bytes, h->stream) != cudaSuccess) {   // no brick has a slot
             set_error("clearing buffers failed");
             vf_mpm3_destroy(h);
             return VF_ECUDA;
@@ -409,6 +511,7 @@ int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z,
     VF_TRY_CUDA(cudaMemsetAsync(h->grid[1].ptr, 0, h->grid[1].bytes, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     h->grid_dirty[0] = h->grid_dirty[1] = 0;
+    h->view_fresh = false;
     h->steps = 0;
     h->loaded = true;
     return VF_OK;
@@ -442,17 +545,27 @@ int32_t vf_mpm3_read(vf_mpm3* h, int32_t field, float* out, int64_t n) {
     VF_REQUIRE(h && out, VF_EINVAL, "null argument");
     if (field >= VF3_GM && field <= VF3_GW) {
         VF_REQUIRE(n == h->nodes, VF_EINVAL, "grid fields hold %lld floats, got %lld", (long long)h->nodes, (long long)n);
-        float* tmp = nullptr;
-        VF_TRY_CUDA(cudaMallocAsync((void**)&tmp, (size_t)h->nodes * 4, h->stream));
-        const float4* src = h->grid[h->grid_last].as<float4>();
+        float4* last;
+        int32_t rc = last_grid(h, &last);
+        if (rc) return rc;
+        const float4* src = last;
         int comp = field - VF3_GM;
         if (field >= VF3_GU) {
             Step3 s = make_step(h);
-            int32_t rc = grid_pass(h, s, h->grid_last);
-            if (rc) return rc;
+            if (h->sparse) {
+                // the grid update over the unpacked box (sparse storage has no tension)
+                if (!h->vel.ptr && (rc = h->vel.alloc((size_t)h->nodes * 16))) return rc;
+                s.grid = last;
+                s.vel = h->vel.as<float4>();
+                VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
+            } else if ((rc = grid_pass(h, s, h->grid_last))) {
+                return rc;
+            }
             src = h->vel.as<float4>();
             comp = field - VF3_GU;
         }
+        float* tmp = nullptr;
+        VF_TRY_CUDA(cudaMallocAsync((void**)&tmp, (size_t)h->nodes * 4, h->stream));
         k_unpack_grid3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(src, tmp, h->nodes, comp);
         VF_CHECK_LAUNCH();
         VF_TRY_CUDA(cudaMemcpyAsync(out, tmp, (size_t)h->nodes * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -514,7 +627,10 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
     static const char* grid_names[4] = {"gm", "gmu", "gmv", "gmw"};
     for (int k = 0; k < 4; k++)
         if (!strcmp(name, grid_names[k])) {
-            *ptr = h->grid[h->grid_last].as<float>() + k;
+            float4* last;
+            int32_t rc = last_grid(h, &last);
+            if (rc) return rc;
+            *ptr = reinterpret_cast<float*>(last) + k;
             *stride = 4;
             return VF_OK;
         }
@@ -545,6 +661,7 @@ int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n) {
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
     VF_REQUIRE(schedule >= VF_P2G_TILE && schedule <= VF_P2G_FIXED, VF_EINVAL, "no scatter schedule %d", schedule);
+    VF_REQUIRE(!h->sparse || schedule == VF_P2G_TILE, VF_EINVAL, "sparse storage runs the tiled schedule only");
     if (schedule == VF_P2G_TILE && h->p2g != VF_P2G_TILE) {
         // the dense pipeline leaves both grids dense-dirty
         for (int g = 0; g < 2; g++)
@@ -558,7 +675,10 @@ int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out) {
     VF_REQUIRE(h && out, VF_EINVAL, "null argument");
     unsigned long long* c = h->scratch.as<unsigned long long>();
     VF_TRY_CUDA(cudaMemsetAsync(c, 0, 8, h->stream));
-    k_touched3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(h->grid[h->grid_last].as<float4>(), h->nodes, c);
+    float4* last;
+    int32_t rc = last_grid(h, &last);
+    if (rc) return rc;
+    k_touched3<<<div_up(h->nodes, 256), 256, 0, h->stream>>>(last, h->nodes, c);
     VF_CHECK_LAUNCH();
     unsigned long long v = 0;
     VF_TRY_CUDA(cudaMemcpyAsync(&v, c, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -634,7 +754,10 @@ int32_t vf_mpm3_snapshot(vf_mpm3* h, void* buf, int64_t cap, int64_t* size) {
     for (int f = 0; f < NF3; f++)
         VF_TRY_CUDA(cudaMemcpyAsync(dst + (size_t)f * h->np * 4, base + f * h->stride, (size_t)h->np * 4,
                                     cudaMemcpyDeviceToHost, h->stream));
-    VF_TRY_CUDA(cudaMemcpyAsync(dst + fields, h->grid[h->grid_last].ptr, grid, cudaMemcpyDeviceToHost, h->stream));
+    float4* last;
+    int32_t rc0 = last_grid(h, &last);
+    if (rc0) return rc0;
+    VF_TRY_CUDA(cudaMemcpyAsync(dst + fields, last, grid, cudaMemcpyDeviceToHost, h->stream));
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     int32_t rc = check_status(h);
     if (rc) return rc;
@@ -663,7 +786,15 @@ int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size) {
         VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src + (size_t)f * h->np * 4, (size_t)h->np * 4,
                                     cudaMemcpyHostToDevice, h->stream));
     // the last grid goes back where readouts look for it; both buffers are cleared densely before their next scatter
-    VF_TRY_CUDA(cudaMemcpyAsync(h->grid[h->grid_last].ptr, src + fields, grid, cudaMemcpyHostToDevice, h->stream));
+    if (h->sparse) {
+        // readouts look in the unpacked box, which holds the snapshot's grid until the next scatter
+        if (!h->view.ptr && (rc = h->view.alloc((size_t)h->nodes * 16))) return rc;
+        VF_TRY_CUDA(cudaMemcpyAsync(h->view.ptr, src + fields, grid, cudaMemcpyHostToDevice, h->stream));
+        h->view_fresh = true;
+    } else {
+        VF_TRY_CUDA(cudaMemcpyAsync(h->grid[h->grid_last].ptr, src + fields, grid, cudaMemcpyHostToDevice,
+                                    h->stream));
+    }
     if ((rc = reset_counts(h))) return rc;
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     h->grid_dirty[0] = h->grid_dirty[1] = 2;

@@ -519,7 +519,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
                 set_status(s.status, ST_OOB);
                 continue;
             }
-            red_add_v4(&s.grid[((int64_t)gz * dm.ny + gy) * dm.nx + gx], t.x, t.y, t.z, t.w);
+            float4* node = node_addr(s, gx, gy, gz);
+            if (!node) {
+                set_status(s.status, ST_POOL);
+                continue;
+            }
+            red_add_v4(node, t.x, t.y, t.z, t.w);
         }
         __syncwarp();
     }
@@ -662,12 +667,13 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
             const int gx = cx0 + wi % WIN, gy = cy0 + (wi / WIN) % WIN, gz = cz0 + wi / (WIN * WIN);
             float4 v = make_float4(0, 0, 0, 0);
             if (gx < dm.nx && gy < dm.ny && gz < dm.nz) {
-                const int64_t node = ((int64_t)gz * dm.ny + gy) * dm.nx + gx;
                 if (s.vel_ready) {
-                    v = s.vel[node];
-                } else {
-                    const float3 u = grid_velocity(s.grid[node], gx, gy, gz, dm, p);
+                    v = s.vel[((int64_t)gz * dm.ny + gy) * dm.nx + gx];
+                } else if (const float4* node = node_addr(s, gx, gy, gz)) {
+                    const float3 u = grid_velocity(*node, gx, gy, gz, dm, p);
                     v = make_float4(u.x, u.y, u.z, 0.0f);
+                } else {
+                    set_status(s.status, ST_POOL);
                 }
             }
             vwin[wi] = v;

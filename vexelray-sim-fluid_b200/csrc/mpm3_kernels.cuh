@@ -138,7 +138,25 @@ struct Step3 {
     int nbricks;
     int count_next;         // G2P also counts keys for the next step's sort
     int vel_ready;          // the tiled G2P reads `vel` (written by the grid pass) instead of updating the grid itself
+    // sparse node storage: the grid is a pool of POOL_BRICK^3-node bricks, `page` maps each brick position of the
+    // domain (pnx x pny x pnz, x fastest) to its slot in the pool, or -1
+    int sparse;
+    const int* page;
+    int pool_cap;           // slots in the pool
+    int pnx, pny, pnz;
 };
+
+constexpr int POOL_BRICK = 8;
+constexpr int POOL_NODES = POOL_BRICK * POOL_BRICK * POOL_BRICK;   // 512 nodes, 8 KB of float4 a brick
+
+// The address of node (gx, gy, gz) in this step's grid: the dense box, or the node's brick's slot in the pool,
+// nodes x fastest within a brick. Null for a brick with no slot (the pool overflowed).
+__device__ __forceinline__ float4* node_addr(const Step3& s, int gx, int gy, int gz) {
+    if (!s.sparse) return s.grid + ((int64_t)gz * s.d.ny + gy) * s.d.nx + gx;
+    const int slot = s.page[((gz >> 3) * s.pny + (gy >> 3)) * s.pnx + (gx >> 3)];
+    if ((unsigned)slot >= (unsigned)s.pool_cap) return nullptr;
+    return s.grid + (int64_t)slot * POOL_NODES + (((gz & 7) * POOL_BRICK + (gy & 7)) * POOL_BRICK + (gx & 7));
+}
 
 // The exact (fixed-point) scatter: each node amount of Flip3.scatter in the reference's operand order without
 // FMA contraction, quantized to FIXED3_BITS fractional bits (round to nearest even) and added with 64-bit
@@ -162,6 +180,16 @@ __global__ void k_tension3_colour(const float4* grid, float* colour, const Param
 __global__ void k_tension3_blur(const float* src, float* dst, Dims3 d);
 __global__ void k_tension3_stress(const float* colour, float* stress, Dims3 d);
 __global__ void k_grid3_tension(Step3 s, const float* colour, const float* stress);
+
+// Sparse node storage (a page table of 8^3-node bricks over one pool). Each step that scatters rebuilds the
+// page of the grid buffer it scatters into from that step's non-empty cell bricks: a cell brick's 10^3 node
+// window covers its own node brick and the next one along each axis, so those 8 are marked, and the marked
+// bricks take slots 0.. in brick order. The grid holds nothing from one step to the next, so no slot is kept.
+__global__ void k_pool_mark3(Step3 s, int* mark);
+__global__ void k_pool_page3(int* mark, int* page, int npages, int* n_used, int cap, uint32_t* status);
+__global__ void k_pool_clear3(float4* pool, const int* n_used);
+// The pool through its page as a dense grid (zero where no brick is), for readouts.
+__global__ void k_pool_unpack3(Step3 s, float4* dense);
 
 __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
