@@ -537,6 +537,7 @@ def run_ours(args, dist: Dist):
                "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
 
     batch = None if args.no_batch else run_batch(args, vf, dist, peak)
+    next_rows = None if args.no_next else run_next_rows(args, vf, peak)
     learned = None if args.no_learned else run_learned(args, vf)
 
     if dist.rank != 0:
@@ -567,11 +568,87 @@ def run_ours(args, dist: Dist):
         "batch": batch,
         "learned": learned,
         "p2g_variants": variants,
+        "next_rows": next_rows,
     }
     print(json.dumps(line), flush=True)
 
 
 CNN_FLOPS_PER_CELL = 2 * 25 * (3 * 32 + 32 * 32 + 32 * 6)   # 65.6 kFLOP: the three convolutions, algorithmic
+
+
+def timed_steps(vf, sim, steps):
+    """ms per step of `steps` steps on the handle's stream, then the same steps profiled per kernel."""
+    ev0, ev1 = vf.Event(), vf.Event()
+    sim.advance(3)
+    sim.finish()
+    ev0.record(sim.stream())
+    sim.advance(steps)
+    ev1.record(sim.stream())
+    ms = ev0.elapsed_ms(ev1) / steps
+    sim.profile(True)
+    sim.advance(steps)
+    sim.finish()
+    prof = {k: v[0] / steps for k, v in sim.profile_read().items()}
+    sim.profile(False)
+    return ms, prof
+
+
+TENSION_KERNELS = {"k_tension3_colour": 8.0, "k_tension3_blur": 8.0 * 5, "k_tension3_stress": 28.0,
+                   "k_grid3_tension": 60.0}   # algorithmic bytes per node per step (5 blur launches)
+
+
+def run_next_rows(args, vf, peak):
+    """Surface tension on the 3D configuration, and sparse storage on it and on a blob in a wide domain."""
+    x, y, z, m, params = dam3()
+    np3 = len(x)
+    zeros = np.zeros(np3, np.float32)
+    nodes = N3 ** 3
+    steps = args.variant_steps
+    out = {}
+    sigma = 0.01 * params[4]
+    with vf.ParticleSimulation3(N3, N3, N3, np3, tension=True) as sim:
+        sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params, sigma))
+        ms, prof = timed_steps(vf, sim, steps)
+    t_ms = sum(prof.get(k, 0.0) for k in TENSION_KERNELS)
+    t_bytes = sum(TENSION_KERNELS.values()) * nodes
+    out["tension"] = {
+        "workload": f"{WORKLOAD3}, with Tension3's passes (sigma {sigma:.4g})", "steps": steps,
+        "ms_per_step": ms, "particle_steps_per_s": np3 / (ms / 1e3), "tension_ms_per_step": t_ms,
+        "roofline": {"bound": "hbm", "kernels": sorted(TENSION_KERNELS), "bytes_per_node": sum(TENSION_KERNELS.values()),
+                     "achieved": t_bytes / (t_ms / 1e3) / 1e9, "peak": peak,
+                     "frac": t_bytes / (t_ms / 1e3) / 1e9 / peak, "unit": "GB/s"},
+        "kernels_ms_per_step": prof}
+
+    sparse = {}
+    pages = (N3 // 8) ** 3
+    with vf.ParticleSimulation3(N3, N3, N3, np3, pool_bricks=pages) as sim:
+        sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params))
+        ms, prof = timed_steps(vf, sim, steps)
+        used = sim.pool_used()
+    sparse["config"] = {"workload": WORKLOAD3, "steps": steps, "ms_per_step": ms,
+                        "particle_steps_per_s": np3 / (ms / 1e3), "pool_bricks": pages, "bricks_used": used,
+                        "p2g_g2p_ms_per_step": prof.get("k_p2g3_tile", 0.0) + prof.get("k_g2p3_tile", 0.0)}
+    # a ball of water (radius 24 nodes) falling in the middle of the same 256^3 domain
+    rng = np.random.default_rng(5)
+    c = np.argwhere(np.ones((48, 48, 48), bool)).astype(np.float32) + np.float32(104)
+    c = c[((c + 0.5 - 128.0) ** 2).sum(1) <= 24.0 ** 2]
+    pos = (np.repeat(c, PPC3, axis=0) + rng.random((len(c) * PPC3, 3), dtype=np.float32) * np.float32(0.999))
+    bx, by, bz = (np.ascontiguousarray(pos[:, a], np.float32) for a in range(3))
+    bm = np.full(len(bx), np.float32(1.0 / PPC3), np.float32)
+    bz0 = np.zeros_like(bx)
+    blob = {"workload": f"a ball of radius 24 nodes ({len(bx)} particles, 8 per cell) falling in a {N3}^3 domain",
+            "steps": steps}
+    for name, kw in (("dense", {}), ("sparse", {"pool_bricks": 512})):
+        with vf.ParticleSimulation3(N3, N3, N3, len(bx), **kw) as sim:
+            sim.load([bx, by, bz], [bz0, bz0, bz0], bm, vf.flip3_params(*params))
+            ms, _ = timed_steps(vf, sim, steps)
+            blob[name] = {"ms_per_step": ms, "particle_steps_per_s": len(bx) / (ms / 1e3),
+                          "grid_bytes": 2 * (512 * 512 * 16 if kw else nodes * 16)}
+            if kw:
+                blob[name]["bricks_used"] = sim.pool_used()
+    sparse["blob"] = blob
+    out["sparse"] = sparse
+    return out
 
 
 def run_learned(args, vf):
@@ -728,6 +805,8 @@ def main():
     ap.add_argument("--no-literal", action="store_true", help="skip the 12.7M-particle literal-box sub-measurement")
     ap.add_argument("--no-c0", action="store_true", help="skip the 2D configuration's sub-measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned shallow-water sub-measurement")
+    ap.add_argument("--no-next", action="store_true",
+                    help="skip the surface-tension and sparse-storage sub-measurements")
     ap.add_argument("--learned-seeds", type=int, default=64, help="held-out seeds of the learned evaluation")
     ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
                     help="the batched step's autotune cache (JSON)")
