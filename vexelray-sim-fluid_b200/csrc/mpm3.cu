@@ -142,12 +142,18 @@ int32_t grid_pass(vf_mpm3* h, Step3& s, int g) {
     }
     const int blocks = div_up(h->nodes, 256);
     float* c[2] = {h->colour[0].as<float>(), h->colour[1].as<float>()};
-    VF_LAUNCH(h->prof, "k_tension3_colour", h->stream, k_tension3_colour, blocks, 256, 0, s.grid, c[0], s.params, s.d);
-    for (int k = 1; k < TENSION3_BLURS; k++)
-        VF_LAUNCH(h->prof, "k_tension3_blur", h->stream, k_tension3_blur, blocks, 256, 0, c[(k - 1) % 2], c[k % 2], s.d);
+    for (int k = 0; k < TENSION3_BLURS; k++) {
+        h->prof.begin(k == 0 ? "k_tension3_colour" : "k_tension3_blur", h->stream);
+        const cudaError_t e = launch_tension3_blur(k == 0, k == 0 ? (const void*)s.grid : (const void*)c[(k - 1) % 2],
+                                                   c[k % 2], s.params, s.d, h->stream);
+        h->prof.end(h->stream);
+        VF_TRY_CUDA(e);
+    }
     const float* colour = c[(TENSION3_BLURS - 1) % 2];
-    VF_LAUNCH(h->prof, "k_tension3_stress", h->stream, k_tension3_stress, blocks, 256, 0, colour, h->stress.as<float>(),
-              s.d);
+    h->prof.begin("k_tension3_stress", h->stream);
+    const cudaError_t e = launch_tension3_stress(colour, h->stress.as<float>(), s.d, h->stream);
+    h->prof.end(h->stream);
+    VF_TRY_CUDA(e);
     VF_LAUNCH(h->prof, "k_grid3_tension", h->stream, k_grid3_tension, blocks, 256, 0, s, colour, h->stress.as<float>());
     return VF_OK;
 }

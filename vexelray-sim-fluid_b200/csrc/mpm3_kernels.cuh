@@ -176,9 +176,10 @@ __global__ void k_fixed_to_grid3(const long long* q, float4* grid, int64_t nodes
 //   grid    k_grid3_tension: Flip3.grid plus dt sigma F / max(m, MASS_FLOOR rho0), F the stress's flux across
 //           the node's open faces; writes `vel` for the G2P
 constexpr int TENSION3_BLURS = 6;          // Flip.TENSION_BLURS
-__global__ void k_tension3_colour(const float4* grid, float* colour, const Params3* params, Dims3 d);
-__global__ void k_tension3_blur(const float* src, float* dst, Dims3 d);
-__global__ void k_tension3_stress(const float* colour, float* stress, Dims3 d);
+// One blur: scaled (the first, src = the grid's float4 {m, ...}) or of the last colour (src = float[nodes]).
+cudaError_t launch_tension3_blur(bool scaled, const void* src, float* dst, const Params3* params, const Dims3& d,
+                                 cudaStream_t stream);
+cudaError_t launch_tension3_stress(const float* colour, float* stress, const Dims3& d, cudaStream_t stream);
 __global__ void k_grid3_tension(Step3 s, const float* colour, const float* stress);
 
 // Sparse node storage (a page table of 8^3-node bricks over one pool). Each step that scatters rebuilds the
