@@ -593,6 +593,19 @@ def timed_steps(vf, sim, steps):
     return ms, prof
 
 
+def plain_ms(vf, sim, steps):
+    """ms per step of `steps` steps on the handle's stream, after a few untimed ones."""
+    ev0, ev1 = vf.Event(), vf.Event()
+    sim.advance(4)
+    sim.finish()
+    ev0.record(sim.stream())
+    sim.advance(steps)
+    ev1.record(sim.stream())
+    ms = ev0.elapsed_ms(ev1) / steps
+    sim.finish()
+    return ms
+
+
 TENSION_KERNELS = {"k_tension3_colour": 8.0, "k_tension3_blur": 8.0 * 5, "k_tension3_stress": 28.0,
                    "k_grid3_tension": 60.0}   # algorithmic bytes per node per step (5 blur launches)
 
@@ -618,6 +631,34 @@ def run_next_rows(args, vf, peak):
                      "achieved": t_bytes / (t_ms / 1e3) / 1e9, "peak": peak,
                      "frac": t_bytes / (t_ms / 1e3) / 1e9 / peak, "unit": "GB/s"},
         "kernels_ms_per_step": prof}
+
+    # the same configuration with advance() replayed from a captured two-step graph
+    with vf.ParticleSimulation3(N3, N3, N3, np3) as sim:
+        sim.set_graph(True)
+        sim.load([x, y, z], [zeros, zeros, zeros], m, vf.flip3_params(*params))
+        ms = plain_ms(vf, sim, steps)
+    out["graph_config"] = {"workload": WORKLOAD3, "steps": steps, "ms_per_step": ms,
+                           "particle_steps_per_s": np3 / (ms / 1e3)}
+    # the reference's scale: Tension3Test's drop (radius 8 in a 40^3 box), launched kernel by kernel and replayed
+    rng = np.random.default_rng(7)
+    c = np.argwhere(np.ones((16, 16, 16), bool)).astype(np.float32) + np.float32(12)
+    c = c[((c + 0.5 - 20.0) ** 2).sum(1) <= 64.0]
+    pos = np.repeat(c, PPC3, axis=0) + rng.random((len(c) * PPC3, 3), dtype=np.float32) * np.float32(0.999)
+    sx, sy, sz = (np.ascontiguousarray(pos[:, a], np.float32) for a in range(3))
+    sm = np.full(len(sx), np.float32(1.0 / PPC3), np.float32)
+    s0 = np.zeros_like(sx)
+    bulk_s = 200.0 ** 2
+    small = {"workload": f"a drop of radius 8 ({len(sx)} particles) at rest in a 40^3 box, no gravity (Tension3Test)",
+             "steps": 400}
+    for tension in (False, True):
+        for graph in (False, True):
+            with vf.ParticleSimulation3(40, 40, 40, len(sx), tension=tension) as sim:
+                sim.set_graph(graph)
+                sim.load([sx, sy, sz], [s0, s0, s0], sm,
+                         vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0))
+                ms = plain_ms(vf, sim, 400)
+            small[f"{'tension' if tension else 'plain'}_{'graph' if graph else 'launched'}_ms_per_step"] = ms
+    out["small_scene"] = small
 
     sparse = {}
     pages = (N3 // 8) ** 3

@@ -249,6 +249,12 @@ int32_t vf_mpm3_params(vf_mpm3* h, const int32_t* params, int32_t nparams);
 /* ParticleSimulation3.advance (ParticleSimulation3.java:291-296); with the default flags each step sorts the
  * particles by stencil cell first. */
 int32_t vf_mpm3_advance(vf_mpm3* h, int32_t count);
+/* advance's steps replayed from a CUDA graph: once the step's host-side state recurs every two steps (after two or
+ * three steps), two steps are captured and then replayed, one graph launch per pair, for as long as the state
+ * before a pair is the one captured; a change of schedule, a load or a restore is met by a new capture. Results
+ * are those of the launched steps. Off by default; no counterpart in the reference, whose runner records each pass
+ * into a command buffer. With per-kernel profiling on, steps are launched one by one. */
+int32_t vf_mpm3_set_graph(vf_mpm3* h, int32_t on);
 /* Passes of one step, for tests (Flip3Test runs clear+scatter alone, Flip3Test.java:90):
  * bit 0 sort, bit 1 clear, bit 2 scatter, bit 3 grid, bit 4 advect. Does not count a step. */
 enum { VF3_PASS_SORT = 1, VF3_PASS_CLEAR = 2, VF3_PASS_SCATTER = 4, VF3_PASS_GRID = 8, VF3_PASS_ADVECT = 16 };

@@ -133,6 +133,7 @@ def lib() -> ctypes.CDLL:
                                    ctypes.c_int32),
         "vf_mpm3_pool_used": ([_vp, _i32p], ctypes.c_int32),
         "vf_mpm3_pool_capacity": ([_vp], ctypes.c_int32),
+        "vf_mpm3_set_graph": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm3_prepared_close": ([_vp], None),
         "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm3_load": ([_vp] + [_f32p] * 7 + [_i32p, ctypes.c_int32], ctypes.c_int32),
@@ -919,6 +920,10 @@ class ParticleSimulation3:
         out = ctypes.c_int32()
         check(lib().vf_mpm3_pool_used(self._h, ctypes.byref(out)))
         return out.value
+
+    def set_graph(self, on: bool) -> None:
+        """advance() replays its steps two at a time from a captured CUDA graph (off by default)."""
+        check(lib().vf_mpm3_set_graph(self._h, 1 if on else 0))
 
     def pool_capacity(self) -> int:
         return int(lib().vf_mpm3_pool_capacity(self._h))

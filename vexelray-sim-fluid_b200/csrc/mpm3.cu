@@ -72,6 +72,12 @@ struct vf_mpm3 {
     bool sorted_valid = false;
     bool loaded = false;
     Profiler prof;
+    // vf_mpm3_set_graph: two steps captured as one CUDA graph from a host state that recurs every two steps, and
+    // replayed while the state before a pair is the one it was captured from
+    bool use_graph = false;
+    cudaGraphExec_t pair = nullptr;
+    uint64_t pair_sig = 0;
+    int64_t pair_launches = 0;
 };
 
 struct vf_mpm3_prepared {
@@ -296,6 +302,57 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_SCATTER) h->passes_run++;
     return VF_OK;
+}
+
+// The host state a step's launches and their arguments depend on (everything else is in device memory or fixed
+// at creation): which particle set is current, whether the counts were made ahead, the grid parity and each grid
+// buffer's clear, the schedule, and whether the exact schedule's buffer exists.
+uint64_t step_sig(const vf_mpm3* h) {
+    return (uint64_t)h->cur | (uint64_t)h->counted << 1 | (uint64_t)(h->passes_run & 1) << 2 |
+           (uint64_t)h->grid_dirty[0] << 3 | (uint64_t)h->grid_dirty[1] << 5 | (uint64_t)h->grid_last << 7 |
+           (uint64_t)h->p2g << 8 | (uint64_t)(h->fixed.ptr != nullptr) << 12 | 1ull << 63;
+}
+
+constexpr uint32_t STEP_PASSES = VF3_PASS_SORT | VF3_PASS_CLEAR | VF3_PASS_SCATTER | VF3_PASS_GRID | VF3_PASS_ADVECT;
+
+// Two steps into h->pair by stream capture, then launched once. The host state the capture advanced is put back
+// if the capture fails, and the steps are left to run uncaptured.
+int32_t capture_pair(vf_mpm3* h, uint64_t sig) {
+    const int cur = h->cur, dirty0 = h->grid_dirty[0], dirty1 = h->grid_dirty[1], last = h->grid_last;
+    const bool counted = h->counted, sorted = h->sorted_valid, fresh = h->view_fresh, fixed = h->fixed_valid;
+    const int64_t passes = h->passes_run, launches = h->prof.launches;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return VF_ECUDA;
+    }
+    int32_t rc = run_passes(h, STEP_PASSES, h->sort);
+    if (!rc) rc = run_passes(h, STEP_PASSES, h->sort);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (!rc && end == cudaSuccess && step_sig(h) == sig &&
+        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        if (h->pair) cudaGraphExecDestroy(h->pair);
+        h->pair = exec;
+        h->pair_sig = sig;
+        h->pair_launches = h->prof.launches - launches;
+        VF_TRY_CUDA(cudaGraphLaunch(h->pair, h->stream));
+        return VF_OK;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    h->cur = cur;
+    h->grid_dirty[0] = dirty0;
+    h->grid_dirty[1] = dirty1;
+    h->grid_last = last;
+    h->counted = counted;
+    h->sorted_valid = sorted;
+    h->view_fresh = fresh;
+    h->fixed_valid = fixed;
+    h->passes_run = passes;
+    h->prof.launches = launches;
+    return VF_ECUDA;
 }
 
 int32_t check_status(vf_mpm3* h) {
@@ -531,12 +588,42 @@ int32_t vf_mpm3_params(vf_mpm3* h, const int32_t* params, int32_t nparams) {
 int32_t vf_mpm3_advance(vf_mpm3* h, int32_t count) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
     VF_REQUIRE(count >= 0, VF_EINVAL, "count must be >= 0, got %d", count);
-    for (int k = 0; k < count; k++) {
-        int32_t rc = run_passes(h, VF3_PASS_SORT | VF3_PASS_CLEAR | VF3_PASS_SCATTER | VF3_PASS_GRID | VF3_PASS_ADVECT,
-                                h->sort);
+    uint64_t seen[2] = {0, 0};   // the state before each of the last two steps
+    for (int k = 0; k < count;) {
+        const uint64_t sig = step_sig(h);
+        if (h->use_graph && !h->prof.on && count - k >= 2) {
+            if (h->pair && h->pair_sig == sig) {
+                // the pair leaves the state it started from; only the counters move
+                VF_TRY_CUDA(cudaGraphLaunch(h->pair, h->stream));
+                h->passes_run += 2;
+                h->prof.launches += h->pair_launches;
+                h->view_fresh = false;
+                h->steps += 2;
+                k += 2;
+                continue;
+            }
+            if (sig == seen[1] && (h->p2g != VF_P2G_FIXED || h->fixed.ptr)) {
+                if (capture_pair(h, sig) == VF_OK) {
+                    h->steps += 2;
+                    k += 2;
+                    continue;
+                }
+                h->use_graph = false;   // this handle's steps do not capture; they run as launches
+            }
+        }
+        int32_t rc = run_passes(h, STEP_PASSES, h->sort);
         if (rc) return rc;
         h->steps++;
+        k++;
+        seen[1] = seen[0];
+        seen[0] = sig;
     }
+    return VF_OK;
+}
+
+int32_t vf_mpm3_set_graph(vf_mpm3* h, int32_t on) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->use_graph = on != 0;
     return VF_OK;
 }
 
@@ -814,6 +901,7 @@ int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size) {
 void vf_mpm3_destroy(vf_mpm3* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->pair) cudaGraphExecDestroy(h->pair);
     for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->cursor, &h->perm, &h->cell_count, &h->cell_start,
                             &h->brick_count, &h->brick_start, &h->active[0], &h->active[1], &h->n_active,
                             &h->grid[0], &h->grid[1], &h->vel, &h->params, &h->status, &h->scratch})
