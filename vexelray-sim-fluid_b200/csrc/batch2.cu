@@ -843,8 +843,7 @@ int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, con
     const float* src[5] = {x, y, u, v, m};
     for (int f = 0; f < 5; f++)
         VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src[f], (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
-    std::vector<float> ones((size_t)h->np, 1.0f);
-    VF_TRY_CUDA(cudaMemcpyAsync(base + PJ * h->stride, ones.data(), (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(fill_f32(base + PJ * h->stride, h->np, 1.0f, h->stream));
     VF_TRY_CUDA(cudaMemsetAsync(base + PC00 * h->stride, 0, (size_t)4 * h->stride * 4, h->stream));
     for (DeviceBuffer* b : {&h->cell_count, &h->tile_count, &h->tile_start[0], &h->tile_start[1], &h->grid[0],
                             &h->grid[1], &h->ctl, &h->status})

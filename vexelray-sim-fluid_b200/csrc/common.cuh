@@ -49,6 +49,9 @@ typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 EncodeTiled tensor_map_encoder();
 
+// Sets n floats at p to v on stream s (a kernel: no host buffer, no pageable copy).
+cudaError_t fill_f32(float* p, int64_t n, float v, cudaStream_t s);
+
 // Device status word bits, set by kernels' own bounds checks (never a trap).
 enum : uint32_t {
     ST_OOB = 1u << 0,        // an index fell outside its buffer; the access was skipped

@@ -565,8 +565,7 @@ int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z,
     const float* src[7] = {x, y, z, u, v, w, m};
     for (int f = 0; f < 7; f++)
         VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src[f], (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
-    std::vector<float> ones((size_t)h->np, 1.0f);
-    VF_TRY_CUDA(cudaMemcpyAsync(base + J * h->stride, ones.data(), (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(fill_f32(base + J * h->stride, h->np, 1.0f, h->stream));
     VF_TRY_CUDA(cudaMemsetAsync(base + C00 * h->stride, 0, (size_t)9 * h->stride * 4, h->stream));
     rc = reset_counts(h);
     if (rc) return rc;

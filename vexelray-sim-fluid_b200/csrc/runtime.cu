@@ -53,6 +53,18 @@ int sm_count() {
     return cached;
 }
 
+__global__ void k_fill_f32(float* p, int64_t n, float v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+cudaError_t fill_f32(float* p, int64_t n, float v, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
+    k_fill_f32<<<blocks, 256, 0, s>>>(p, n, v);
+    return cudaGetLastError();
+}
+
 EncodeTiled tensor_map_encoder() {
     static EncodeTiled fn = nullptr;
     static bool tried = false;
