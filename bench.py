@@ -658,6 +658,14 @@ def run_next_rows(args, vf, peak):
                          vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0))
                 ms = plain_ms(vf, sim, 400)
             small[f"{'tension' if tension else 'plain'}_{'graph' if graph else 'launched'}_ms_per_step"] = ms
+    names = {vf.VF_P2G_TILE: "tile", vf.VF_P2G_ATOMIC: "atomic", vf.VF_P2G_WARP: "warp"}
+    for sched in names:
+        with vf.ParticleSimulation3(40, 40, 40, len(sx), schedule=sched) as sim:
+            sim.set_graph(True)
+            sim.load([sx, sy, sz], [s0, s0, s0], sm, vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0))
+            small[f"plain_graph_{names[sched]}_ms_per_step"] = plain_ms(vf, sim, 400)
+            _, prof = timed_steps(vf, sim, 100)
+            small[f"plain_{names[sched]}_kernels_ms_per_step"] = {k: round(v, 5) for k, v in prof.items()}
     out["small_scene"] = small
 
     sparse = {}
