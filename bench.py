@@ -658,7 +658,7 @@ def run_next_rows(args, vf, peak):
                          vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0))
                 ms = plain_ms(vf, sim, 400)
             small[f"{'tension' if tension else 'plain'}_{'graph' if graph else 'launched'}_ms_per_step"] = ms
-    names = {vf.VF_P2G_TILE: "tile", vf.VF_P2G_ATOMIC: "atomic", vf.VF_P2G_WARP: "warp"}
+    names = {vf.VF_P2G_TILE: "tile", vf.VF_P2G_ATOMIC: "atomic", vf.VF_P2G_WARP: "warp", vf.VF_P2G_AUTO: "auto"}
     for sched in names:
         with vf.ParticleSimulation3(40, 40, 40, len(sx), schedule=sched) as sim:
             sim.set_graph(True)

@@ -84,9 +84,14 @@ enum {
     VF_P2G_ATOMIC = 1,  /* one thread per particle, 27 vector atomics (Flip3.java:225-243's direct scatter) */
     VF_P2G_WARP = 2,    /* one thread per particle, runs of one cell summed across the warp first
                            (Scatter.segmentedDeposit, Scatter.java:385-439, over 27 nodes x 4 fields) */
-    VF_P2G_FIXED = 3    /* exact: every node amount quantized to 2^-40 and added with 64-bit integer atomics, so the
+    VF_P2G_FIXED = 3,   /* exact: every node amount quantized to 2^-40 and added with 64-bit integer atomics, so the
                            grid is the same to the bit in any order and its total mass is the particles' quantized
                            masses' sum exactly (the 3D form of FixedScatter.java:24-60, with 64-bit sums) */
+    VF_P2G_AUTO = 4     /* the schedule measured fastest for the handle's size, chosen once at creation (or by
+                           vf_mpm3_set_p2g): warp-aggregated below 1.5M particles on grids under 2^22 nodes, where
+                           the tile's one warp per 8x8x2-cell unit leaves the GPU idle (3.2x at 17k particles),
+                           the tile otherwise and always with sparse storage. The scenes of the reference's scale
+                           (32 to 96 nodes a side) take the warp-aggregated scatter */
 };
 
 /* ------------------------------------------------------------------ 2D particles (ParticleSimulation) */
@@ -277,6 +282,8 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
 void* vf_mpm3_stream(vf_mpm3* h);
 /* Change the scatter schedule (VF_P2G_*) between steps. */
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
+/* The schedule the steps run (VF_P2G_AUTO resolved). */
+int32_t vf_mpm3_schedule(const vf_mpm3* h);
 /* The last scatter's exact grid when it ran VF_P2G_FIXED (VF_ESTATE otherwise): field 0..3 = m, mu, mv, mw as
  * int64 with 40 fractional bits, n = nx*ny*nz values. No counterpart in the reference. */
 int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n);

@@ -18,7 +18,7 @@ from _oracle import F, Flip3State, JavaRandom, flip3_params, slab3, stable_step
 pytestmark = pytest.mark.gpu
 
 SCHEDULES = [("tile", vf.VF_P2G_TILE, True), ("atomic", vf.VF_P2G_ATOMIC, True), ("warp", vf.VF_P2G_WARP, True),
-             ("atomic-unsorted", vf.VF_P2G_ATOMIC, False), ("fixed", vf.VF_P2G_FIXED, True)]
+             ("atomic-unsorted", vf.VF_P2G_ATOMIC, False), ("fixed", vf.VF_P2G_FIXED, True), ("auto", vf.VF_P2G_AUTO, True)]
 
 
 def sim3(n, count, schedule, sort, **kw):
@@ -239,3 +239,17 @@ def test_the_exact_scatter_is_bit_exact_against_the_oracle_in_any_order():
         for f in range(4):
             assert np.array_equal(got[f], want[f]), f
     assert int(want[0].sum()) == int(np.rint(m.astype(np.float64) * 2.0 ** 40).astype(np.int64).sum())
+
+
+def test_the_automatic_schedule_picks_by_size():
+    """VF_P2G_AUTO: the warp-aggregated scatter for a scene of the reference's scale, the tile for many particles,
+    for a large grid and for sparse storage; set_p2g resolves it the same way."""
+    cases = [((40, 40, 40), 17408, {}, vf.VF_P2G_WARP), ((64, 64, 64), 1_600_000, {}, vf.VF_P2G_TILE),
+             ((256, 256, 256), 1000, {}, vf.VF_P2G_TILE), ((40, 40, 40), 17408, {"pool_bricks": 125}, vf.VF_P2G_TILE)]
+    for dims, count, kw, want in cases:
+        with vf.ParticleSimulation3(*dims, count, schedule=vf.VF_P2G_AUTO, **kw) as s:
+            assert s.schedule() == want, (dims, count, kw)
+    with vf.ParticleSimulation3(40, 40, 40, 17408) as s:
+        assert s.schedule() == vf.VF_P2G_TILE
+        s.set_schedule(vf.VF_P2G_AUTO)
+        assert s.schedule() == vf.VF_P2G_WARP

@@ -35,7 +35,7 @@ VF_P2G_SHIFT = 16
 VF_NO_SORT = 1 << 20
 VF_TENSION = 1 << 21
 VF_RELAX = 1 << 22
-VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED = 0, 1, 2, 3
+VF_P2G_TILE, VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED, VF_P2G_AUTO = 0, 1, 2, 3, 4
 VF_SCATTER_GRID, VF_SCATTER_PRE_REDUCED, VF_SCATTER_GATHER, VF_SCATTER_SEGMENTED = 0, 1, 2, 3
 VF3_PASS_SORT, VF3_PASS_CLEAR, VF3_PASS_SCATTER, VF3_PASS_GRID, VF3_PASS_ADVECT = 1, 2, 4, 8, 16
 EDGE_WALL, EDGE_OPEN = 0, 1
@@ -134,6 +134,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_pool_used": ([_vp, _i32p], ctypes.c_int32),
         "vf_mpm3_pool_capacity": ([_vp], ctypes.c_int32),
         "vf_mpm3_set_graph": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_schedule": ([_vp], ctypes.c_int32),
         "vf_mpm3_prepared_close": ([_vp], None),
         "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm3_load": ([_vp] + [_f32p] * 7 + [_i32p, ctypes.c_int32], ctypes.c_int32),
@@ -779,8 +780,9 @@ class Prepared:
 class ParticleSimulation3:
     """ParticleSimulation3 (ParticleSimulation3.java): a 3D particle fluid in one walled box on the GPU.
 
-    ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC, VF_P2G_WARP or VF_P2G_FIXED
-    (exact: 64-bit fixed-point sums, the same grid in any order).
+    ``schedule`` is the scatter: VF_P2G_TILE (default; sorts every step), VF_P2G_ATOMIC, VF_P2G_WARP, VF_P2G_FIXED
+    (exact: 64-bit fixed-point sums, the same grid in any order) or VF_P2G_AUTO (the fastest for the size: the
+    warp-aggregated scatter for scenes of the reference's scale, the tile for large ones).
     ``sort=False`` keeps the particles in load order, as the reference's Flip3Step does.
     ``tension=True`` adds surface tension's passes (ParticleSimulation3(..., tension)); its strength is sigma, the
     seventh params word (``flip3_params(..., sigma)``).
@@ -920,6 +922,10 @@ class ParticleSimulation3:
         out = ctypes.c_int32()
         check(lib().vf_mpm3_pool_used(self._h, ctypes.byref(out)))
         return out.value
+
+    def schedule(self) -> int:
+        """The scatter schedule the steps run (VF_P2G_AUTO resolved for this size)."""
+        return int(lib().vf_mpm3_schedule(self._h))
 
     def set_graph(self, on: bool) -> None:
         """advance() replays its steps two at a time from a captured CUDA graph (off by default)."""
