@@ -437,6 +437,28 @@ int32_t vf_cnn_profile_read(vf_cnn* h, int32_t index, char* name, size_t cap, do
 int64_t vf_cnn_launches(const vf_cnn* h);
 void vf_cnn_destroy(vf_cnn* h);
 
+/* ------------------------------------------------------------------ the learned coarse solver */
+/* The learned coarse shallow-water solver as one handle; no counterpart in the reference, judged against the
+ * plain fine solver. An nx x ny coarse patch with walls (cells 2 dx wide) stepped by the plain HLL step; every
+ * `interval_ticks` the network `net` (borrowed; NULL: the plain coarse solver) predicts a correction from the
+ * interval's start state, on the coarse stream, and it is applied at the interval's end. With `fallback`, tiles
+ * of `tile` coarse cells whose relative depth jump (vf_swe_jump_indicator) exceeds `threshold` at an interval's
+ * start are stepped by the fine solver instead: the tile and `margin` coarse cells around it, prolonged into a
+ * fine patch (open edges inside the domain), stepped through the interval and restricted back. load takes a
+ * coarse state with the coarse params (g 9.81, Courant 0.45, dry 1e-6). */
+typedef struct vf_swe_learned vf_swe_learned;
+int32_t vf_swe_learned_create(int32_t nx, int32_t ny, vf_cnn* net, int64_t interval_ticks, int32_t tile,
+                              int32_t fallback, float threshold, int32_t margin, float dx, vf_swe_learned** out);
+int32_t vf_swe_learned_load(vf_swe_learned* h, const float* hcell, const float* hu, const float* hv);
+/* Intervals until `ticks` are spent (the last one shortened to fit). */
+int32_t vf_swe_learned_advance(vf_swe_learned* h, int64_t ticks);
+int32_t vf_swe_learned_read(vf_swe_learned* h, float* hcell, float* hu, float* hv);
+/* out = {coarse steps, corrections applied, fallback tiles stepped}. */
+int32_t vf_swe_learned_counts(const vf_swe_learned* h, int64_t out[3]);
+/* The coarse patch, for its readouts (diagnostics, wave speed); owned by the handle. */
+vf_swe* vf_swe_learned_coarse(vf_swe_learned* h);
+void vf_swe_learned_destroy(vf_swe_learned* h);
+
 /* ------------------------------------------------------------------ particle diagnostics */
 /* ParticleDiagnostics.of over a device-resident J (ParticleDiagnostics.java:126-148): out = {minDensity,
  * maxDensity, lowDensity, highDensity, mach, courant, nonFinite}. */

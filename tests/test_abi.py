@@ -75,3 +75,17 @@ def test_no_device_is_an_error_not_a_fallback():
     assert L.vf_mpm2_create(32, 32, 10, 0, ctypes.byref(h)) == vexfluid.VF_ENODEV
     with pytest.raises(vexfluid.VfError):
         vexfluid.ParticleSimulation(32, 32, 10)
+
+
+def test_the_learned_handle_is_created_or_refused_cleanly():
+    """vf_swe_learned_create through its declared signature: a handle where there is a device, VF_ENODEV where there
+    is none; never a crash."""
+    import ctypes
+    import vexfluid as vf
+    h = ctypes.c_void_p()
+    rc = vf.lib().vf_swe_learned_create(64, 64, None, 1000, 16, 1, 0.5, 4, 1.0, ctypes.byref(h))
+    if rc == 0:
+        vf.lib().vf_swe_learned_destroy(h)
+    else:
+        assert rc == vf.VF_ENODEV, rc
+        assert not h.value

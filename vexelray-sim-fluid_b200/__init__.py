@@ -200,6 +200,16 @@ def lib() -> ctypes.CDLL:
                                  _i64p], ctypes.c_int32),
         "vf_cnn_launches": ([_vp], ctypes.c_int64),
         "vf_cnn_destroy": ([_vp], None),
+        "vf_swe_learned_create": ([ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64, ctypes.c_int32,
+                                   ctypes.c_int32, ctypes.c_float, ctypes.c_int32, ctypes.c_float,
+                                   ctypes.POINTER(_vp)],
+                                  ctypes.c_int32),
+        "vf_swe_learned_load": ([_vp, _f32p, _f32p, _f32p], ctypes.c_int32),
+        "vf_swe_learned_advance": ([_vp, ctypes.c_int64], ctypes.c_int32),
+        "vf_swe_learned_read": ([_vp, _f32p, _f32p, _f32p], ctypes.c_int32),
+        "vf_swe_learned_counts": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int32),
+        "vf_swe_learned_coarse": ([_vp], _vp),
+        "vf_swe_learned_destroy": ([_vp], None),
         "vf_swe_create": ([ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_swe_load": ([_vp] + [_f32p] * 3 + [_i32p, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
@@ -985,6 +995,52 @@ class Advance:
 
     def mean_step(self) -> float:
         return 0.0 if self.steps == 0 else seconds(self.spent_ticks) / self.steps
+
+
+class LearnedSimulation:
+    """The learned coarse shallow-water solver as one native handle (vf_swe_learned_*): an nx x ny coarse patch,
+    the network's correction every `interval` ticks (`net` None: the plain coarse solver), and with a `threshold`
+    the tiles whose depth jump exceeds it stepped by the fine solver. The same calls, in the same order, as
+    learned.LearnedShallowWater."""
+
+    def __init__(self, nx: int, ny: int, net: "FluxNet | None", interval: int, *, tile: int = 64,
+                 threshold: float | None = None, margin: int = 8, dx: float = 1.0):
+        h = _vp()
+        check(lib().vf_swe_learned_create(nx, ny, net._h if net is not None else None, int(interval), tile,
+                                          0 if threshold is None else 1,
+                                          0.0 if threshold is None else float(threshold), margin, dx,
+                                          ctypes.byref(h)))
+        self._h, self.nx, self.ny, self.net = h, nx, ny, net
+
+    def load(self, h, hu, hv) -> None:
+        n = self.nx * self.ny
+        a = [_f32(np.ravel(q), n) for q in (h, hu, hv)]
+        check(lib().vf_swe_learned_load(self._h, *[_fp(q) for q in a]))
+
+    def advance(self, ticks_: int) -> None:
+        check(lib().vf_swe_learned_advance(self._h, int(ticks_)))
+
+    def read(self):
+        out = [np.empty(self.nx * self.ny, np.float32) for _ in range(3)]
+        check(lib().vf_swe_learned_read(self._h, *[_fp(q) for q in out]))
+        return [q.reshape(self.ny, self.nx) for q in out]
+
+    def counts(self) -> tuple:
+        """(coarse steps, corrections applied, fallback tiles stepped)."""
+        out = (ctypes.c_int64 * 3)()
+        check(lib().vf_swe_learned_counts(self._h, out))
+        return tuple(out)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vf_swe_learned_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class PatchSimulation:
