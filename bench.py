@@ -298,14 +298,18 @@ def run_c0(args, vf, dist):
     params = vf.flip_params(*p)
     steps = 1000
     zeros = np.zeros_like(x)
-    with vf.ParticleSimulation(n, n, len(x), tait=True, sticky=WALL_BATCH) as s:
-        s.load(x, y, zeros, zeros, m, params)
-        s.advance(10, 10)
-        s.read("m")   # a blocking read: the device is idle
-        t0 = time.perf_counter()
-        s.advance(steps, 10)
-        s.read("m")
-        ms = 1e3 * (time.perf_counter() - t0)   # host clock: launches and the final read included
+    ms_by = {}
+    for graph in (False, True):
+        with vf.ParticleSimulation(n, n, len(x), tait=True, sticky=WALL_BATCH) as s:
+            s.set_graph(graph)
+            s.load(x, y, zeros, zeros, m, params)
+            s.advance(20, 10)
+            s.read("m")   # a blocking read: the device is idle
+            t0 = time.perf_counter()
+            s.advance(steps, 10)
+            s.read("m")
+            ms_by[graph] = 1e3 * (time.perf_counter() - t0)   # host clock: launches and the final read included
+    ms = ms_by[False]
     cpu = None
     if not args.no_cpu and dist.rank == 0:
         sys.path.insert(0, str(ROOT / "tests"))
@@ -324,7 +328,10 @@ def run_c0(args, vf, dist):
     return {"workload": "2D dam break 128^2 (config 0): 8192 particles, Tait k=50, sticky walls 3, dt 1e-4, sorted "
                         "every 10 steps; host-clock time of 1000 steps (launch-bound at this size)",
             "particles": len(x), "steps": steps, "ms_per_step": ms / steps,
-            "particle_steps_per_s": len(x) * steps / (ms / 1e3), "cpu_baseline": cpu}
+            "particle_steps_per_s": len(x) * steps / (ms / 1e3),
+            "graph": {"ms_per_step": ms_by[True] / steps, "particle_steps_per_s": len(x) * steps / (ms_by[True] / 1e3),
+                      "how": "vf_mpm2_set_graph: a sort and the ten steps after it per graph launch"},
+            "cpu_baseline": cpu}
 
 
 def cpu_swe_rate(h, budget_s=10.0):

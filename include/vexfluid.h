@@ -116,6 +116,11 @@ int32_t vf_mpm2_params(vf_mpm2* h, const int32_t* params, int32_t nparams);
 /* ParticleSimulation.advance(count, sortEvery) (ParticleSimulation.java:175-183): sorts first on every step
  * whose number (counted across calls) is a multiple of sort_every (>= 1). */
 int32_t vf_mpm2_advance(vf_mpm2* h, int32_t count, int32_t sort_every);
+/* advance's steps replayed from CUDA graphs, a sort and the sort_every steps after it per graph launch (one graph
+ * for each of the two particle sets a sort leaves current, captured on first use); steps that do not fill such a
+ * block are launched one by one. Results are those of the launched steps. Off by default; no counterpart in the
+ * reference. */
+int32_t vf_mpm2_set_graph(vf_mpm2* h, int32_t on);
 /* One FlipStep.step() (clear, scatter, grid, advect), and one FlipStep.sort(), without counting a step:
  * what the reference's test Rig runs (Rig.java:30-34). */
 int32_t vf_mpm2_step(vf_mpm2* h);

@@ -265,3 +265,29 @@ def test_relaxing_steps_match_the_oracle():
             e = o.a[key]
             got = s.read(key)
             assert np.all(np.abs(got - e) <= 1e-4 * np.abs(e)), key
+
+
+def test_replayed_steps_match_the_oracle():
+    """advance() from captured graphs (a sort and the ten steps after it per graph): 1, 25 and 74 steps (blocks
+    and loose steps) of the falling column, positions within the 100-step bar of the oracle's sorted run."""
+    n = 32
+    x, y, m = flip_column(71)
+    fall = math.sqrt(2 * 200 * 16)
+    bulk = (5 * fall) ** 2
+    dt = 0.3 / (math.sqrt(bulk) + fall)
+    params = vf.flip_params(dt, 0, -200, bulk, 1)
+    o = Flip2State(n, n, x, y, m)
+    with vf.ParticleSimulation(n, n, len(x)) as s:
+        s.set_graph(True)
+        s.load(x, y, np.zeros_like(x), np.zeros_like(x), m, params)
+        for count in (1, 25, 74):
+            s.advance(count, 10)
+        assert s.steps() == 100
+        for k in range(100):
+            if k % 10 == 0:
+                o.sort()
+            o.step(params.view(F))
+        for key in ("x", "y"):
+            e = o.a[key]
+            got = s.read(key)
+            assert np.all(np.abs(got - e) <= 1e-4 * np.abs(e)), key

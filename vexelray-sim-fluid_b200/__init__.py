@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm2_create": ([ctypes.c_int32] * 3 + [ctypes.c_uint32, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm2_load": ([_vp] + [_f32p] * 5 + [_i32p, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_params": ([_vp, _i32p, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm2_set_graph": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_advance": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_step": ([_vp], ctypes.c_int32),
         "vf_mpm2_sort": ([_vp], ctypes.c_int32),
@@ -437,6 +438,10 @@ class ParticleSimulation:
 
     def advance(self, count: int, sort_every: int) -> None:
         check(lib().vf_mpm2_advance(self._h, count, sort_every))
+
+    def set_graph(self, on: bool) -> None:
+        """advance() replays a sort and the sort_every steps after it from one captured CUDA graph (off by default)."""
+        check(lib().vf_mpm2_set_graph(self._h, 1 if on else 0))
 
     def step(self) -> None:
         """One FlipStep.step() without counting it (the test Rig's run(step.step()))."""

@@ -326,6 +326,10 @@ struct vf_mpm2 {
     DeviceBuffer params, status;
     int64_t steps = 0;
     bool sorted = false;
+    // vf_mpm2_set_graph: a sort and the sort_every steps after it, captured once per current particle set
+    bool use_graph = false;
+    cudaGraphExec_t block[2] = {nullptr, nullptr};
+    int block_every = 0;   // the sort_every the blocks were captured for
 };
 
 namespace {
@@ -466,16 +470,72 @@ int32_t vf_mpm2_params(vf_mpm2* h, const int32_t* params, int32_t nparams) {
     return upload_params2(h, params, nparams);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The block from a sort to the step before the next sort, captured for the current particle set (the sort moves
+// the particles into the other set, so two blocks alternate); false if capture failed, with the state restored.
+bool capture_block(vf_mpm2* h, int sort_every) {
+    const int cur = h->cur;
+    const bool sorted = h->sorted;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int32_t rc = sort2(h);
+    for (int k = 0; !rc && k < sort_every; k++) rc = step2(h);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = !rc && end == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    h->cur = cur;
+    h->sorted = sorted;
+    if (!ok) return false;
+    if (h->block[cur]) cudaGraphExecDestroy(h->block[cur]);
+    h->block[cur] = exec;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t vf_mpm2_advance(vf_mpm2* h, int32_t count, int32_t sort_every) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
     VF_REQUIRE(count >= 0 && sort_every >= 1, VF_EINVAL, "count >= 0 and sortEvery >= 1, got %d, %d", count,
                sort_every);
-    for (int k = 0; k < count; k++) {
+    for (int k = 0; k < count;) {
         int32_t rc;
+        if (h->use_graph && h->steps % sort_every == 0 && count - k >= sort_every) {
+            if (h->block_every != sort_every) {
+                for (auto& b : h->block)
+                    if (b) cudaGraphExecDestroy(b), b = nullptr;
+                h->block_every = sort_every;
+            }
+            if (h->block[h->cur] || capture_block(h, sort_every)) {
+                VF_TRY_CUDA(cudaGraphLaunch(h->block[h->cur], h->stream));
+                h->cur ^= 1;
+                h->sorted = true;
+                h->steps += sort_every;
+                k += sort_every;
+                continue;
+            }
+            h->use_graph = false;   // this handle's steps do not capture; they run as launches
+        }
         if (h->steps % sort_every == 0 && (rc = sort2(h))) return rc;
         if ((rc = step2(h))) return rc;
         h->steps++;
+        k++;
     }
+    return VF_OK;
+}
+
+int32_t vf_mpm2_set_graph(vf_mpm2* h, int32_t on) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->use_graph = on != 0;
     return VF_OK;
 }
 
@@ -537,6 +597,8 @@ int32_t vf_mpm2_on_gpu(const vf_mpm2* h) { return h ? 1 : 0; }
 void vf_mpm2_destroy(vf_mpm2* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& b : h->block)
+        if (b) cudaGraphExecDestroy(b);
     for (DeviceBuffer* b : {&h->part[0], &h->part[1], &h->key, &h->rank, &h->perm, &h->counts, &h->starts, &h->grid,
                             &h->params, &h->status})
         b->release();
