@@ -443,8 +443,8 @@ int64_t vf_cnn_launches(const vf_cnn* h);
 void vf_cnn_destroy(vf_cnn* h);
 
 /* ------------------------------------------------------------------ the learned coarse solver */
-/* The learned coarse shallow-water solver as one handle; no counterpart in the reference, judged against the
- * plain fine solver. An nx x ny coarse patch with walls (cells 2 dx wide) stepped by the plain HLL step; every
+/* The learned coarse shallow-water solver as one handle; no counterpart in the reference, its error measured
+ * against the plain fine solver. An nx x ny coarse patch with walls (cells 2 dx wide) stepped by the plain HLL step; every
  * `interval_ticks` the network `net` (borrowed; NULL: the plain coarse solver) predicts a correction from the
  * interval's start state, on the coarse stream, and it is applied at the interval's end. With `fallback`, tiles
  * of `tile` coarse cells whose relative depth jump (vf_swe_jump_indicator) exceeds `threshold` at an interval's

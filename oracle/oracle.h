@@ -4,11 +4,11 @@
  *
  * This is test infrastructure. Nothing in the product library links, loads or
  * calls it: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
- * --impl reference legs use it, and only as the checker or the CPU comparison.
+ * --impl reference legs use it, and only to check results against or as the CPU comparison.
  *
  * The reference (sibarum/vexelray-sim-fluid) is Java that builds SupirVast IR
  * (dev.supirvast:vastir 0.2.3-SNAPSHOT, not vendored, no JDK here), so it cannot
- * run in this container. Every function below restates one IR kernel expression
+ * run here. Every function below restates one IR kernel expression
  * by expression, in the operand order the IR builds it, in IEEE f32 with no
  * contraction (built -ffp-contract=off), which is what Java's strict float
  * arithmetic computes. Each function cites the reference file:line it follows;
@@ -46,7 +46,8 @@ void   or_jrand_floats(or_jrand* r, float* out, int64_t n);
 
 /* ---------------------------------------------------------------- physics options */
 /* Equation of state and wall model. REF follows Flip.java / Flip3.java exactly;
- * TAIT and STICKY are the benchmark-config physics (documented in DESIGN.md). */
+ * TAIT and STICKY are the benchmark configurations' physics: p = k((1/J)^7 - 1) with k the bulk word, and
+ * every node within `sticky` nodes of an edge stopped. */
 enum { OR_EOS_REF = 0, OR_EOS_TAIT = 1 };
 typedef struct {
     int eos;          /* OR_EOS_REF: p = B(1/J - 1); OR_EOS_TAIT: p = k((1/J)^7 - 1) */
@@ -135,7 +136,8 @@ void or_flip3_step_tension(or_flip3* s, const float* params, or_physics ph, floa
 
 /* The 3D sort key: the stencil base cell of Flip3.Stencil3 (Flip3.java:664-678), base
  * cells 0..n-3 per axis, linearised brick-major in 8x8x8 bricks (the reference has no
- * 3D sort; the key is defined here). */
+ * 3D sort; the key is defined here: bricks in x-fastest order, cells x-fastest within a brick, so each brick's
+ * particles form one contiguous run). */
 enum { OR_BRICK = 8, OR_BRICK_CELLS = 512 };
 int32_t or_key3(float x, float y, float z, int nx, int ny, int nz);
 int64_t or_key3_count(int nx, int ny, int nz);   /* number of keys (starts has this + 1 words) */

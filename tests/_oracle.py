@@ -1,7 +1,7 @@
 """ctypes bindings to the oracle (oracle/liboracle.so) and the reference tests' input generators.
 
-Test infrastructure: the oracle is the CPU restatement of the reference step and is
-only ever the checker here. The generators regenerate the reference tests' seeded
+Test infrastructure: the oracle is the CPU restatement of the reference step, and the
+tests only ever check results against it. The generators regenerate the reference tests' seeded
 inputs through a java.util.Random restatement:
 
 * ``JavaRandom``          -- java.util.Random (Java SE API specification), pure Python.

@@ -1,4 +1,4 @@
-"""The learned coarse shallow-water solver against the plain fine solver (its judge) and the plain coarse solver
+"""The learned coarse shallow-water solver against the plain fine solver (its error's measure) and the plain coarse solver
 (the method without the network).
 
 * ablation: a network trained here (512^2 fine, 16 seeds) lowers the coarse solver's h RMS error on a held-out

@@ -2,7 +2,7 @@
 // convolutions (3 -> 32 -> 32 -> 6 channels, ReLU between), bf16 weights and activations, fp32
 // accumulation on the tensor cores (tcgen05 for the 32-channel inputs, mma.sync m16n8k16 for the 8-channel ones
 // and as an alternative), trained with Adam on fp32 master weights.
-// No counterpart in the reference; its judge is the plain fine solver (ShallowWater.kernel).
+// No counterpart in the reference; its error is measured against the plain fine solver (ShallowWater.kernel).
 //
 // Layouts (per sample, row-major cells, channels innermost):
 //   x0   bf16 [H][W][8]   features (h - 1) * 4, hu * 4, hv * 4, then zeros

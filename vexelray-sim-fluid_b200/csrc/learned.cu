@@ -1,7 +1,7 @@
 // learned.cu -- the learned coarse shallow-water solver's driver as a native handle (vf_swe_learned_*): a coarse
 // patch stepped by the plain HLL step, the flux-correction network's correction applied once an interval, and
 // tiles whose relative depth jump crosses a threshold stepped by the fine solver instead. No counterpart in the
-// reference, whose judge of it is the plain fine solver (ShallowWater.kernel, ShallowWater.java:166-242).
+// reference; its error is measured against the plain fine solver (ShallowWater.kernel, ShallowWater.java:166-242).
 //
 // One interval of `interval` ticks:
 //   [fallback]  the coarse state's per-tile jump (vf_swe_jump_indicator); if any tile trips, the state is kept

@@ -1,7 +1,7 @@
 """The learned coarse shallow-water solver: the plain HLL step (ShallowWater.kernel) on a 2x-coarsened grid,
 corrected once per interval by the flux-correction network (FluxNet), with a per-tile indicator whose tiles fall
-back to the plain fine solver for that interval. No counterpart in the reference; the plain fine solver is its
-judge (the error is measured against the fine solution restricted to the coarse grid) and its fallback.
+back to the plain fine solver for that interval. No counterpart in the reference; its error is measured against
+the plain fine solver's solution restricted to the coarse grid, and the fine solver is also its fallback.
 
   generate + train   fine runs (PatchSimulation at the fine resolution) give samples (S, P, T): the coarse
                      state (the fine state averaged over 2x2 cells), the plain coarse solver after one
