@@ -703,6 +703,45 @@ def run_next_rows(args, vf, peak):
             if kw:
                 blob[name]["bricks_used"] = sim.pool_used()
     sparse["blob"] = blob
+    # many blobs in one pool (the reference's planned experiment): n balls of radius 8 spread through a 256^3 domain
+    # and stepped together, against the same balls as n separate 40^3 boxes stepped one after another
+    drop = np.argwhere(np.ones((16, 16, 16), bool)).astype(np.float32)
+    drop = drop[((drop + 0.5 - 8.0) ** 2).sum(1) <= 64.0]
+    many = {"workload": "n balls of radius 8 (1,704 cells, 8 particles each) in one 256^3 domain with sparse storage, "
+                        "against n separate 40^3 boxes (VF_P2G_AUTO, graph replay)", "steps": 100}
+    for nb in (1, 4, 16):
+        sites = [(48 + 48 * (k % 4), 48 + 48 * ((k // 4) % 4), 128) for k in range(nb)]
+        cells = np.concatenate([drop + np.array(c, np.float32) - 8.0 for c in sites])
+        pos = np.repeat(cells, PPC3, axis=0) + rng.random((len(cells) * PPC3, 3), dtype=np.float32) * np.float32(0.999)
+        mx, my, mz = (np.ascontiguousarray(pos[:, a], np.float32) for a in range(3))
+        mm = np.full(len(mx), np.float32(1.0 / PPC3), np.float32)
+        m0 = np.zeros_like(mx)
+        with vf.ParticleSimulation3(N3, N3, N3, len(mx), pool_bricks=64 * nb) as sim:
+            sim.set_graph(True)
+            sim.load([mx, my, mz], [m0, m0, m0], mm, vf.flip3_params(*params))
+            pooled = plain_ms(vf, sim, 100)
+            used = sim.pool_used()
+        one = len(drop) * PPC3
+        boxes = []
+        for k in range(nb):
+            sl = slice(k * one, (k + 1) * one)
+            b = vf.ParticleSimulation3(40, 40, 40, one, schedule=vf.VF_P2G_AUTO)
+            b.set_graph(True)
+            off = np.array(sites[k], np.float32) - 20.0
+            b.load([mx[sl] - off[0], my[sl] - off[1], mz[sl] - off[2]], [m0[sl]] * 3, mm[sl], vf.flip3_params(*params))
+            b.advance(4)
+            b.finish()
+            boxes.append(b)
+        t0 = time.perf_counter()
+        for b in boxes:   # each box on its own stream, so their steps may overlap on the device
+            b.advance(100)
+        for b in boxes:
+            b.finish()
+        separate = 1e3 * (time.perf_counter() - t0) / 100   # host clock over all boxes' streams
+        for b in boxes:
+            b.close()
+        many[str(nb)] = {"pool_ms_per_step": pooled, "bricks_used": used, "separate_boxes_ms_per_step": separate}
+    sparse["many_blobs"] = many
     out["sparse"] = sparse
     return out
 

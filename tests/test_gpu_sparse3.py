@@ -166,3 +166,26 @@ def test_a_dense_snapshot_resumes_in_sparse_storage():
     with vf.ParticleSimulation3(n, n, n, len(x)) as c:
         c.restore(again)
         assert c.steps() == 10
+
+
+def test_several_blobs_share_one_pool():
+    """Four separated balls in one 160^3 domain are more bricks of the same pool, stepped by the same launches: the
+    pool holds each blob's bricks (the sum, as they are far apart), and 20 steps follow the oracle's dense box."""
+    n = 160
+    centres = [(30.0, 40.0, 30.0), (120.0, 40.0, 40.0), (40.0, 100.0, 120.0), (120.0, 120.0, 110.0)]
+    parts = [ball(n, n, n, c, 6.0, seed=k) for k, c in enumerate(centres)]
+    x, y, z, m = (np.concatenate([p[a] for p in parts]) for a in range(4))
+    m = (m.view(np.int32) + np.arange(len(m), dtype=np.int32)).view(F)
+    each = sum(reached_bricks(p[0], p[1], p[2], n, n, n) for p in parts)
+    assert reached_bricks(x, y, z, n, n, n) == each
+    p = (2e-3, 0.0, -100.0, 0.0, 400.0, 1.0)
+    o = Flip3State(n, n, n, x, y, z, m)
+    with vf.ParticleSimulation3(n, n, n, len(x), pool_bricks=each + 16) as s:
+        s.load([x, y, z], [np.zeros_like(x)] * 3, m, vf.flip3_params(*p))
+        s.advance(1)
+        assert s.pool_used() == each
+        s.advance(19)
+        pos, mass = s.positions(), s.read("m")
+    for _ in range(20):
+        o.step(flip3_params(*p))
+    check_positions(pos, mass, o, "four blobs, 20 steps")
