@@ -544,7 +544,7 @@ def run_ours(args, dist: Dist):
                "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
 
     batch = None if args.no_batch else run_batch(args, vf, dist, peak)
-    next_rows = None if args.no_next else run_next_rows(args, vf, peak)
+    next_rows = None if args.no_next else run_next_rows(args, vf, peak, cpu=not args.no_cpu and dist.rank == 0)
     learned = None if args.no_learned else run_learned(args, vf)
 
     if dist.rank != 0:
@@ -617,7 +617,34 @@ TENSION_KERNELS = {"k_tension3_colour": 8.0, "k_tension3_blur": 8.0 * 5, "k_tens
                    "k_grid3_tension": 60.0}   # algorithmic bytes per node per step (5 blur launches)
 
 
-def run_next_rows(args, vf, peak):
+def cpu_tension_rate(n, x, y, z, m, params, tension, budget_s, max_steps):
+    """The oracle's threaded 3D step (with tension's passes if asked) on the host cores: particle-steps/s."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _oracle import Flip3State, OrPhysics, fp, lib as olib
+    s = Flip3State(n, n, n, x, y, z, m)
+    pw = np.ascontiguousarray(np.array(params, np.float32))
+    scratch = np.zeros(8 * n ** 3, np.float32) if tension else None
+
+    def step():
+        if tension:
+            olib().or_flip3_step_tension_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None, fp(scratch))
+        else:
+            olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)
+
+    t0 = time.perf_counter()
+    step()   # warm-up (page faults)
+    first = time.perf_counter() - t0
+    steps = max(1, min(max_steps, int(budget_s / max(first, 1e-4))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    el = time.perf_counter() - t0
+    return {"value": len(x) * steps / el, "unit": "particle-steps/s", "cores": olib().or_baseline_threads(),
+            "kind": "port", "sample": f"{steps} steps of the same workload, oracle C port of Flip3Step"
+                                      f"{' with tension' if tension else ''}, OpenMP, {el:.1f} s"}
+
+
+def run_next_rows(args, vf, peak, cpu=False):
     """Surface tension on the 3D configuration, and sparse storage on it and on a blob in a wide domain."""
     x, y, z, m, params = dam3()
     np3 = len(x)
@@ -637,7 +664,8 @@ def run_next_rows(args, vf, peak):
         "roofline": {"bound": "hbm", "kernels": sorted(TENSION_KERNELS), "bytes_per_node": sum(TENSION_KERNELS.values()),
                      "achieved": t_bytes / (t_ms / 1e3) / 1e9, "peak": peak,
                      "frac": t_bytes / (t_ms / 1e3) / 1e9 / peak, "unit": "GB/s"},
-        "kernels_ms_per_step": prof}
+        "kernels_ms_per_step": prof,
+        "cpu_baseline": cpu_tension_rate(N3, x, y, z, m, (*params, sigma), True, 10.0, 8) if cpu else None}
 
     # the same configuration with advance() replayed from a captured two-step graph
     with vf.ParticleSimulation3(N3, N3, N3, np3) as sim:
@@ -665,6 +693,10 @@ def run_next_rows(args, vf, peak):
                          vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0))
                 ms = plain_ms(vf, sim, 400)
             small[f"{'tension' if tension else 'plain'}_{'graph' if graph else 'launched'}_ms_per_step"] = ms
+        if cpu and not graph:
+            small[f"{'tension' if tension else 'plain'}_cpu_baseline"] = cpu_tension_rate(
+                40, sx, sy, sz, sm, (0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0),
+                tension, 3.0, 400)
     names = {vf.VF_P2G_TILE: "tile", vf.VF_P2G_ATOMIC: "atomic", vf.VF_P2G_WARP: "warp", vf.VF_P2G_AUTO: "auto"}
     for sched in names:
         with vf.ParticleSimulation3(40, 40, 40, len(sx), schedule=sched) as sim:

@@ -312,7 +312,7 @@ int or_baseline_threads(void) {
  * particles into a private grid, over only the z-planes its slice touches, and the private
  * grids are summed plane by plane. Grid update and advect are plain parallel loops. The
  * arithmetic per particle and per node is that of the sequential functions above. */
-void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* scratch) {
+static void step_omp(or_flip3* s, const float* params, or_physics ph, float* scratch, float* tension) {
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     const int64_t plane = (int64_t)nx * ny, nodes = plane * nz;
     const float dt = params[P_DT], bulk = params[P_BULK], rho0 = params[P_RHO0];
@@ -391,8 +391,13 @@ void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* s
     /* grid update and advect: independent per node / per particle */
     const int size[3] = {nx, ny, nz};
     const float gr[3] = {params[P_GX], params[P_GY], params[P_GZ]};
+    if (tension) {   /* Flip3Step with tension: the colour, its blurs, the stress, the grid with the force */
+        const float* colour = or_tension3_colour(nx, ny, nz, s->gm, params, tension, tension + nodes);
+        or_tension3_stress(nx, ny, nz, colour, tension + 2 * nodes);
+        or_flip3_grid_tension(s, params, ph, colour, tension + 2 * nodes);
+    }
 #pragma omp parallel for schedule(static) num_threads(nt)
-    for (int64_t node = 0; node < nodes; node++) {
+    for (int64_t node = 0; node < (tension ? 0 : nodes); node++) {
         int at[3] = {(int)(node % nx), (int)((node / nx) % ny), (int)(node / plane)};
         float mass = s->gm[node];
         float vel[3] = {0.0f, 0.0f, 0.0f};
@@ -424,4 +429,12 @@ void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* s
         mine.np = (int)(p1 - p0);
         or_flip3_advect(&mine, params);
     }
+}
+
+void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* scratch) {
+    step_omp(s, params, ph, scratch, NULL);
+}
+
+void or_flip3_step_tension_omp(or_flip3* s, const float* params, or_physics ph, float* scratch, float* tension) {
+    step_omp(s, params, ph, scratch, tension);
 }

@@ -175,6 +175,9 @@ void or_particle_diagnostics(const float* j, int64_t n, double speed, double sou
  * grids then a reduction; everything else a parallel loop. Returns threads used. */
 int or_baseline_threads(void);
 void or_flip3_step_omp(or_flip3* s, const float* params, or_physics ph, float* scratch_grids /* threads*4*nodes */);
+/* The same with tension's passes (Flip3Step with tension); tension: 8 * nodes floats. */
+void or_flip3_step_tension_omp(or_flip3* s, const float* params, or_physics ph, float* scratch_grids,
+                               float* tension);
 void or_swe_dispatch_omp(int nx, int ny, const int32_t edges[4], const float* params,
                          const float* in_h, const float* in_hu, const float* in_hv,
                          float* out_h, float* out_hu, float* out_hv,

@@ -99,6 +99,7 @@ def lib():
         L.or_flip3_advect.argtypes = [ctypes.POINTER(OrFlip3), f32p]
         L.or_flip3_sort.argtypes = [ctypes.POINTER(OrFlip3), i32p, i32p, i32p, f32p]
         L.or_flip3_step_omp.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, f32p]
+        L.or_flip3_step_tension_omp.argtypes = [ctypes.POINTER(OrFlip3), f32p, OrPhysics, f32p, f32p]
         L.or_baseline_threads.restype = ctypes.c_int
         L.or_key3.argtypes = [ctypes.c_float] * 3 + [ctypes.c_int] * 3
         L.or_key3.restype = ctypes.c_int32

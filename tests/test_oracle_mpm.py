@@ -436,3 +436,20 @@ def test_oracle_relaxation_draws_j_to_the_volume_the_mass_gives():
     relaxed = relax_median_j(run, 8.0)
     assert abs(without - 0.9) <= 0.05, f"J moved by itself to {without}"
     assert 0.97 < relaxed < 1.03, f"relaxed J is {relaxed}, not 1"
+
+
+def test_the_threaded_tension_step_is_the_serial_one_to_rounding():
+    """The CPU baseline's threaded step with tension (private grids per thread, summed) against the serial step:
+    positions after 5 steps of a drop within 1e-5 relative (only the scatter's summation order differs)."""
+    n = 24
+    x, y, z, m, _ = drop3(n, radius=5.0)
+    p = flip3_params(stable_step(40000.0, 1, 20, 0.3), 0, 0, 0, 40000.0, 1.0, 3200.0)
+    a = Flip3State(n, n, n, x, y, z, m)
+    b = Flip3State(n, n, n, x, y, z, m)
+    t = np.zeros(8 * n ** 3, F)
+    for _ in range(5):
+        a.step(p, tension=True)
+        lib().or_flip3_step_tension_omp(ctypes.byref(b.s), fp(p), OrPhysics(0, 0), None, fp(t))
+    for key in ("x", "y", "z"):
+        assert np.all(np.abs(a.a[key] - b.a[key]) <= 1e-5 * np.abs(a.a[key])), key
+    assert np.any(a.a["x"] != x)
