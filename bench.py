@@ -601,9 +601,10 @@ def timed_steps(vf, sim, steps):
 
 
 def plain_ms(vf, sim, steps):
-    """ms per step of `steps` steps on the handle's stream, after a few untimed ones."""
+    """ms per step of `steps` steps on the handle's stream, after ten untimed ones (a replayed run captures its
+    graph within them)."""
     ev0, ev1 = vf.Event(), vf.Event()
-    sim.advance(4)
+    sim.advance(10)
     sim.finish()
     ev0.record(sim.stream())
     sim.advance(steps)
@@ -693,7 +694,7 @@ def run_next_rows(args, vf, peak, cpu=False):
                          vf.flip3_params(0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0))
                 ms = plain_ms(vf, sim, 400)
             small[f"{'tension' if tension else 'plain'}_{'graph' if graph else 'launched'}_ms_per_step"] = ms
-        if cpu and not graph:
+        if cpu:
             small[f"{'tension' if tension else 'plain'}_cpu_baseline"] = cpu_tension_rate(
                 40, sx, sy, sz, sm, (0.3 / 220.0, 0.0, 0.0, 0.0, bulk_s, 1.0, 0.08 * bulk_s if tension else 0.0),
                 tension, 3.0, 400)
@@ -761,7 +762,7 @@ def run_next_rows(args, vf, peak, cpu=False):
             b.set_graph(True)
             off = np.array(sites[k], np.float32) - 20.0
             b.load([mx[sl] - off[0], my[sl] - off[1], mz[sl] - off[2]], [m0[sl]] * 3, mm[sl], vf.flip3_params(*params))
-            b.advance(4)
+            b.advance(10)   # the graph is captured here, not in the timed steps
             b.finish()
             boxes.append(b)
         t0 = time.perf_counter()
