@@ -289,6 +289,10 @@ void* vf_mpm3_stream(vf_mpm3* h);
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
 /* The schedule the steps run (VF_P2G_AUTO resolved). */
 int32_t vf_mpm3_schedule(const vf_mpm3* h);
+/* The smallest positive mass of the last load (or restore), FLT_MAX if none: ParticleSimulation3's nominalMass
+ * (ParticleSimulation3.java:248-253), measured on the device during the load; compression() keeps the particles
+ * holding at least half of it (ParticleSimulation3.java:312-333). Blocking. */
+int32_t vf_mpm3_nominal_mass(vf_mpm3* h, float* out);
 /* The last scatter's exact grid when it ran VF_P2G_FIXED (VF_ESTATE otherwise): field 0..3 = m, mu, mv, mw as
  * int64 with 40 fractional bits, n = nx*ny*nz values. No counterpart in the reference. */
 int32_t vf_mpm3_read_fixed(vf_mpm3* h, int32_t field, int64_t* out, int64_t n);

@@ -253,3 +253,24 @@ def test_the_automatic_schedule_picks_by_size():
         assert s.schedule() == vf.VF_P2G_TILE
         s.set_schedule(vf.VF_P2G_AUTO)
         assert s.schedule() == vf.VF_P2G_WARP
+
+
+def test_the_nominal_mass_is_measured_at_load():
+    """ParticleSimulation3's nominalMass (ParticleSimulation3.java:248-253) and compression (312-333): the smallest
+    positive mass loaded, measured on the device; compression keeps the particles holding at least half of it."""
+    import ctypes
+    n = 24
+    x, y, z, m, p, _ = dam3(n)
+    m = m.copy()
+    m[5] = F(0.0)                 # an empty slot: below half the nominal mass, left out
+    m[9] = F(0.01)                # the smallest positive mass sets the nominal
+    with vf.ParticleSimulation3(n, n, n, len(x)) as s:
+        s.load([x, y, z], [np.zeros_like(x)] * 3, m, vf.flip3_params(*p))
+        got = np.empty(1, F)
+        vf.check(vf.lib().vf_mpm3_nominal_mass(s._h, got.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        assert got[0] == F(0.01)
+        assert len(s.compression()) == len(x) - 1
+        s.load([x, y, z], [np.zeros_like(x)] * 3, np.zeros_like(m), vf.flip3_params(*p))
+        vf.check(vf.lib().vf_mpm3_nominal_mass(s._h, got.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        assert got[0] == np.finfo(F).max
+        assert len(s.compression()) == 0

@@ -136,6 +136,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_pool_capacity": ([_vp], ctypes.c_int32),
         "vf_mpm3_set_graph": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm3_schedule": ([_vp], ctypes.c_int32),
+        "vf_mpm3_nominal_mass": ([_vp, _f32p], ctypes.c_int32),
         "vf_mpm3_prepared_close": ([_vp], None),
         "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_mpm3_load": ([_vp] + [_f32p] * 7 + [_i32p, ctypes.c_int32], ctypes.c_int32),
@@ -827,7 +828,6 @@ class ParticleSimulation3:
         prepared._p = None
         self._h = h
         self._nx, self._ny, self._nz, self._np = prepared.nx, prepared.ny, prepared.nz, prepared.particles
-        self._nominal = 0.0
 
     def nx(self):
         return self._nx
@@ -849,8 +849,6 @@ class ParticleSimulation3:
         a = [_f32(q, n) for q in (at[0], at[1], at[2], velocity[0], velocity[1], velocity[2], mass)]
         w = _words(params)
         check(lib().vf_mpm3_load(self._h, *[_fp(q) for q in a], _ip(w), len(w)))
-        pos = a[6][a[6] > 0]
-        self._nominal = float(pos.min()) if len(pos) else 0.0
 
     def params(self, params) -> None:
         w = _words(params)
@@ -888,7 +886,9 @@ class ParticleSimulation3:
         half the smallest loaded mass."""
         j = self.read("j")
         m = self.read("m")
-        keep = m >= 0.5 * self._nominal
+        nominal = np.empty(1, np.float32)
+        check(lib().vf_mpm3_nominal_mass(self._h, _fp(nominal)))
+        keep = m >= np.float32(0.5) * nominal[0]
         return j if keep.all() else j[keep]
 
     def key_count(self) -> int:

@@ -46,6 +46,7 @@ struct vf_mpm3 {
     DeviceBuffer params;
     DeviceBuffer status;
     DeviceBuffer scratch;     // readouts
+    DeviceBuffer nominal;     // the smallest positive mass loaded, as float bits (ParticleSimulation3.java:248-253)
     DeviceBuffer fixed;       // the exact schedule's grid: int64 [4][nodes], FIXED3_BITS fractional bits
     bool tension = false;     // VF_TENSION: Tension3's passes between the scatter and the grid
     DeviceBuffer colour[2];   // the blurs' ping-pong colour planes, nodes floats each
@@ -173,6 +174,15 @@ int32_t grid_pass(vf_mpm3* h, Step3& s, int g) {
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
     VF_LAUNCH(h->prof, "k_grid3_tension", h->stream, k_grid3_tension, blocks, 256, 0, s, colour, h->stress.as<float>());
+    return VF_OK;
+}
+
+// The nominal mass of the current set's masses, on the device: the smallest positive one, FLT_MAX if none.
+int32_t measure_nominal(vf_mpm3* h) {
+    VF_TRY_CUDA(fill_f32(h->nominal.as<float>(), 1, 3.402823466e+38f, h->stream));
+    k_min_positive3<<<std::max(1, std::min(div_up(h->np, 256), sm_count() * 4)), 256, 0, h->stream>>>(
+        h->part[h->cur].as<float>() + (int64_t)M * h->stride, h->np, h->nominal.as<unsigned>());
+    VF_CHECK_LAUNCH();
     return VF_OK;
 }
 
@@ -480,7 +490,8 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
         (rc = h->active[0].alloc((size_t)h->nbricks * 4)) || (rc = h->active[1].alloc((size_t)h->nbricks * 4)) ||
         (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc(grid_bytes)) ||
         (rc = h->grid[1].alloc(grid_bytes)) || (!h->sparse && (rc = h->vel.alloc((size_t)h->nodes * 16))) ||
-        (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)))
+        (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)) ||
+        (rc = h->nominal.alloc(16)))
         return fail(rc);
     if (h->sparse && ((rc = h->page[0].alloc((size_t)h->npages * 4)) || (rc = h->page[1].alloc((size_t)h->npages * 4)) ||
                       (rc = h->mark.alloc((size_t)h->npages * 4)) || (rc = h->n_used.alloc(2 * sizeof(int)))))
@@ -580,6 +591,7 @@ int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z,
         VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src[f], (size_t)h->np * 4, cudaMemcpyHostToDevice, h->stream));
     VF_TRY_CUDA(fill_f32(base + J * h->stride, h->np, 1.0f, h->stream));
     VF_TRY_CUDA(cudaMemsetAsync(base + C00 * h->stride, 0, (size_t)9 * h->stride * 4, h->stream));
+    if ((rc = measure_nominal(h))) return rc;
     rc = reset_counts(h);
     if (rc) return rc;
     VF_TRY_CUDA(cudaMemsetAsync(h->grid[0].ptr, 0, h->grid[0].bytes, h->stream));
@@ -779,6 +791,13 @@ int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule) {
 
 int32_t vf_mpm3_schedule(const vf_mpm3* h) { return h ? h->p2g : -1; }
 
+int32_t vf_mpm3_nominal_mass(vf_mpm3* h, float* out) {
+    VF_REQUIRE(h && out, VF_EINVAL, "null argument");
+    VF_TRY_CUDA(cudaMemcpyAsync(out, h->nominal.ptr, 4, cudaMemcpyDeviceToHost, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return VF_OK;
+}
+
 int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out) {
     VF_REQUIRE(h && out, VF_EINVAL, "null argument");
     unsigned long long* c = h->scratch.as<unsigned long long>();
@@ -893,6 +912,7 @@ int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size) {
     for (int f = 0; f < NF3; f++)
         VF_TRY_CUDA(cudaMemcpyAsync(base + f * h->stride, src + (size_t)f * h->np * 4, (size_t)h->np * 4,
                                     cudaMemcpyHostToDevice, h->stream));
+    if ((rc = measure_nominal(h))) return rc;
     // the last grid goes back where readouts look for it; both buffers are cleared densely before their next scatter
     if (h->sparse) {
         // readouts look in the unpacked box, which holds the snapshot's grid until the next scatter

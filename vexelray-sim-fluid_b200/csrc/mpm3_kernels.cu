@@ -805,6 +805,17 @@ __global__ void __launch_bounds__(256) k_clear_bricks3(Step3 s) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_min_positive3(const float* m, int n, unsigned* out) {
+    unsigned best = 0x7f7fffffu;   // FLT_MAX
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float v = m[i];
+        if (v > 0.0f) best = min(best, __float_as_uint(v));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0 && best != 0x7f7fffffu) atomicMin(out, best);
+}
+
 __global__ void k_touched3(const float4* grid, int64_t nodes, unsigned long long* out) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool t = i < nodes && grid[i].x > 0.0f;

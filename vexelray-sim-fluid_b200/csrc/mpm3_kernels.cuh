@@ -202,6 +202,9 @@ __global__ void k_g2p3(Step3 s);
 __global__ void k_g2p3_tile(Step3 s);
 __global__ void k_clear_bricks3(Step3 s);
 __global__ void k_touched3(const float4* grid, int64_t nodes, unsigned long long* out);
+// The smallest positive mass as float bits into *out (which starts at FLT_MAX's bits): positive floats order as
+// their bits do, so an integer atomicMin finds it.
+__global__ void k_min_positive3(const float* m, int n, unsigned* out);
 __global__ void k_unpack_grid3(const float4* grid, float* out, int64_t nodes, int comp);
 
 }  // namespace vf
