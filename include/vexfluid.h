@@ -88,10 +88,10 @@ enum {
                            grid is the same to the bit in any order and its total mass is the particles' quantized
                            masses' sum exactly (the 3D form of FixedScatter.java:24-60, with 64-bit sums) */
     VF_P2G_AUTO = 4     /* the schedule measured fastest for the handle's size, chosen once at creation (or by
-                           vf_mpm3_set_p2g): warp-aggregated below 1.5M particles on grids under 2^22 nodes, where
-                           the tile's one warp per 8x8x2-cell unit leaves the GPU idle (3.2x at 17k particles),
-                           the tile otherwise and always with sparse storage. The scenes of the reference's scale
-                           (32 to 96 nodes a side) take the warp-aggregated scatter */
+                           vf_mpm3_set_p2g): warp-aggregated below 600k particles on grids under 2^22 nodes, where
+                           the tile's one warp per unit of cells leaves much of the GPU idle (1.8x at 17k
+                           particles), the tile otherwise and always with sparse storage. The scenes of the
+                           reference's scale (32 to 96 nodes a side) take the warp-aggregated scatter */
 };
 
 /* ------------------------------------------------------------------ 2D particles (ParticleSimulation) */

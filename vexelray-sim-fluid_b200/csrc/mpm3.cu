@@ -129,6 +129,9 @@ Step3 make_step(vf_mpm3* h) {
     s.brick_start = h->brick_start.as<int>();
     s.nkeys = h->nkeys;
     s.nbricks = h->nbricks;
+    // the tiled G2P's items per brick: bricks hold about 2,048 particles or more, and the G2P keeps four CTAs an SM
+    // busy; the 256^3 configuration's 2,000 bricks need no split, a 17k-particle drop's dozen take eight items each
+    s.g2p_split = (int)std::min<int64_t>(8, std::max<int64_t>(1, (int64_t)sm_count() * 4 / std::max(1, h->np / 2048)));
     s.sparse = h->sparse ? 1 : 0;
     s.pool_cap = h->pool_cap;
     s.pnx = h->pnx;
@@ -139,12 +142,12 @@ Step3 make_step(vf_mpm3* h) {
 
 int persistent_blocks(int per_sm) { return sm_count() * per_sm; }
 
-// VF_P2G_AUTO: the schedule measured fastest for the handle's size. Below about 1.5M particles the tiled scatter,
-// one warp per 8x8x2-cell unit, leaves most of the GPU idle: the warp-aggregated scatter over the dense grid is
-// 3.2x faster at 17k particles in a 40^3 box and 1.1x at 0.9M in 128^3. Above that, or on grids where the dense
-// passes (clear, grid update: 48 B a node) would cost more than the particles, the tile wins (1.36x at 7.2M in
-// 256^3). Sparse storage always runs the tile.
-constexpr int64_t AUTO_TILE_PARTICLES = 1500000;
+// VF_P2G_AUTO: the schedule measured fastest for the handle's size. Below about 600k particles the tiled scatter,
+// one warp per unit of 8x8x1 cells (8x8x2 from a million particles), leaves much of the GPU idle: the
+// warp-aggregated scatter over the dense grid is 1.8x faster at 17k particles in a 40^3 box and 1.2x at 358k in
+// 96^3. Above that, or on grids where the dense passes (clear, grid update: 48 B a node) would cost more than the
+// particles, the tile wins (1.05x at 0.9M in 128^3, 1.35x at 7.2M in 256^3). Sparse storage always runs the tile.
+constexpr int64_t AUTO_TILE_PARTICLES = 600000;
 constexpr int64_t AUTO_TILE_NODES = int64_t(1) << 22;
 int resolve_p2g(int schedule, int64_t particles, int64_t nodes, bool sparse) {
     if (schedule != VF_P2G_AUTO) return schedule;
@@ -274,7 +277,11 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_SCATTER) {
         if (tile) {
-            VF_LAUNCH(h->prof, "k_p2g3_tile", h->stream, k_p2g3_tile, persistent_blocks(2), 128, p2g_tile_smem(), s);
+            // half-depth units below a million particles, where 8x8x2-cell units would leave SMs idle
+            h->prof.begin("k_p2g3_tile", h->stream);
+            const cudaError_t e = launch_p2g3_tile(h->np < (1 << 20) ? 1 : 2, persistent_blocks(2), s, h->stream);
+            h->prof.end(h->stream);
+            VF_TRY_CUDA(e);
         } else if (h->p2g == VF_P2G_WARP) {
             VF_LAUNCH(h->prof, "k_p2g3_warp", h->stream, k_p2g3_warp, div_up(h->np, 256), 256, 0, s);
         } else if (h->p2g == VF_P2G_FIXED) {
@@ -500,9 +507,8 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
     if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
                        (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);
-    if (cudaFuncSetAttribute(k_p2g3_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_tile_smem()) !=
-        cudaSuccess) {
-        set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem());
+    if (p2g_tile_prepare() != cudaSuccess) {
+        set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem(2));
         return fail(VF_ECUDA);
     }
     vf_mpm3_prepared* p = new vf_mpm3_prepared();

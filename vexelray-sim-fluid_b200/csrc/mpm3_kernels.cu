@@ -215,9 +215,9 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 
 // ------------------------------------------------------------------ P2G: sorted brick tile
 
-// Each warp takes work units of (non-empty brick, 8 x 8 x 2 cells), four per brick, with no barrier between warps.
+// Each warp takes work units of (non-empty brick, 8 x 8 x UZ cells), 8 / UZ per brick, with no barrier between warps.
 //
-//  1. A unit's 128 cells are consecutive keys, so their particle runs form one contiguous range of the sort's
+//  1. A unit's 64 UZ cells are consecutive keys, so their particle runs form one contiguous range of the sort's
 //     permutation. The warp stages it in shared memory, puts each cell's run in ascending order there (the stable
 //     sort's fix-up, fused here: G2P then reads the stable permutation), and writes the range back.
 //  2. Cells are dealt to lanes from a queue ordered by particle count, largest first: a lane sums one whole cell's
@@ -235,22 +235,28 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 // which is (w m)(v_a + C_a . d) + w s d_a with d = o - f (Flip3.java:225-243).
 constexpr int P2G_THREADS = 128;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
-constexpr int UZ = 2;                                      // brick z-layers per work unit
-constexpr int UCELLS = BRICK * BRICK * UZ;                 // 128 cells
-constexpr int UPB = BRICK / UZ;                            // units per brick
-constexpr int WWX = WIN, WWY = WIN, WWZ = UZ + 2, WW = WWX * WWY * WWZ;   // a warp's window: 400 nodes
+// A work unit is UZ brick z-layers: 2 (8x8x2 cells, about 1,000 particles) by default, 1 for scenes of few bricks,
+// where twice the units keep more of the GPU busy.
+constexpr int WWX = WIN, WWY = WIN;
 constexpr int RUN_CAP = 2048;   // particle slots of one unit staged in shared memory (more: sorted in place)
 constexpr int NBUCKET = 32;     // count buckets of the cell queue (counts of 31 and more share the last)
 
+template <int UZ>
+struct P2GUnit {
+    static constexpr int UCELLS = BRICK * BRICK * UZ;            // 64 UZ cells
+    static constexpr int UPB = BRICK / UZ;                       // units per brick
+    static constexpr int WWZ = UZ + 2, WW = WWX * WWY * WWZ;     // a warp's window: 100 (UZ + 2) nodes
+};
+
+template <int UZ>
 struct P2GShared {
-    float4 wwin[P2G_WARPS][WW];
+    float4 wwin[P2G_WARPS][P2GUnit<UZ>::WW];
     int run[P2G_WARPS][RUN_CAP];         // the unit's range of the permutation, sorted per cell here
-    int start[P2G_WARPS][UCELLS + 1];    // cell c's particles: [start[c], start[c + 1])
-    unsigned char order[P2G_WARPS][UCELLS];   // non-empty cells by descending count
+    int start[P2G_WARPS][P2GUnit<UZ>::UCELLS + 1];    // cell c's particles: [start[c], start[c + 1])
+    unsigned char order[P2G_WARPS][P2GUnit<UZ>::UCELLS];   // non-empty cells by descending count
     int bucket[P2G_WARPS][NBUCKET];
     int next[P2G_WARPS];                 // the queue's head
 };
-constexpr size_t P2G_SMEM = sizeof(P2GShared);
 // One particle's fields, as the scatter reads them.
 struct PIn {
     float x, y, z, u, v, w, m, j, c[9];
@@ -279,9 +285,11 @@ __device__ __forceinline__ int checked_src(const int* run, int i, int np, uint32
     return src;
 }
 
+template <int UZ>
 __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
+    constexpr int UCELLS = P2GUnit<UZ>::UCELLS, UPB = P2GUnit<UZ>::UPB, WW = P2GUnit<UZ>::WW;
     extern __shared__ __align__(16) unsigned char p2g_raw[];
-    P2GShared& S = *reinterpret_cast<P2GShared*>(p2g_raw);
+    P2GShared<UZ>& S = *reinterpret_cast<P2GShared<UZ>*>(p2g_raw);
     const Params3 p = *s.params;
     const float vol = __fdiv_rn(1.0f, p.rho0);                 // V0 = m / rho0 as m * (1/rho0)
     const float k4dt = 4.0f * p.dt;
@@ -530,7 +538,23 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
     }
 }
 
-size_t p2g_tile_smem() { return P2G_SMEM; }
+size_t p2g_tile_smem(int uz) { return uz == 1 ? sizeof(P2GShared<1>) : sizeof(P2GShared<2>); }
+
+cudaError_t p2g_tile_prepare() {
+    cudaError_t e = cudaFuncSetAttribute(k_p2g3_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)p2g_tile_smem(1));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_p2g3_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_tile_smem(2));
+    return e;
+}
+
+cudaError_t launch_p2g3_tile(int uz, int blocks, const Step3& s, cudaStream_t stream) {
+    if (uz == 1)
+        k_p2g3_tile<1><<<blocks, P2G_THREADS, p2g_tile_smem(1), stream>>>(s);
+    else
+        k_p2g3_tile<2><<<blocks, P2G_THREADS, p2g_tile_smem(2), stream>>>(s);
+    return cudaGetLastError();
+}
 
 // ------------------------------------------------------------------ grid update (dense)
 
@@ -653,14 +677,15 @@ __global__ void __launch_bounds__(256) k_g2p3(Step3 s) {
 //   C_ae = 4 (S_ae - f_e vel_a)      (= 4 sum w v_a (o_e - f_e), Flip3.java:349-365).
 constexpr int G2P_THREADS = 256;
 
-__global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
+__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p3_tile(Step3 s) {
     __shared__ float4 vwin[WIN3];
     const Params3 p = *s.params;
     const Dims3 dm = s.d;
     const int64_t st = s.stride;
     const int na = *s.n_active;
-    for (int a = blockIdx.x; a < na; a += gridDim.x) {
-        const int b = s.active[a];
+    const int split = max(s.g2p_split, 1);
+    for (int a = blockIdx.x; a < na * split; a += gridDim.x) {
+        const int b = s.active[a / split], part = a % split;
         const int bx = b % dm.nbx, by = (b / dm.nbx) % dm.nby, bz = b / (dm.nbx * dm.nby);
         const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK;
         for (int wi = threadIdx.x; wi < WIN3; wi += G2P_THREADS) {
@@ -684,6 +709,11 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p3_tile(Step3 s) {
             set_status(s.status, ST_OOB);
             bs = max(bs, 0);
             be = min(max(be, bs), s.np);
+        }
+        if (split > 1) {   // this item's slice of the brick's particles
+            const int64_t len = be - bs;
+            be = bs + (int)(len * (part + 1) / split);
+            bs = bs + (int)(len * part / split);
         }
         // Every thread walks the same number of iterations so the warp-level count is converged. The
         // permutation is read two iterations ahead and the particle one iteration ahead of its use.

@@ -138,6 +138,8 @@ struct Step3 {
     int nbricks;
     int count_next;         // G2P also counts keys for the next step's sort
     int vel_ready;          // the tiled G2P reads `vel` (written by the grid pass) instead of updating the grid itself
+    int g2p_split;          // the tiled G2P's work items per brick (>= 1): each loads the brick's window and takes
+                            // one slice of its particles, so a scene of few bricks still fills the GPU
     // sparse node storage: the grid is a pool of POOL_BRICK^3-node bricks, `page` maps each brick position of the
     // domain (pnx x pny x pnz, x fastest) to its slot in the pool, or -1
     int sparse;
@@ -195,8 +197,10 @@ __global__ void k_pool_unpack3(Step3 s, float4* dense);
 __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
 __global__ void k_p2g3_warp(Step3 s);
-__global__ void k_p2g3_tile(Step3 s);
-size_t p2g_tile_smem();
+// The tiled scatter with work units of uz brick z-layers (1 or 2): 128 threads a CTA, two CTAs an SM.
+cudaError_t launch_p2g3_tile(int uz, int blocks, const Step3& s, cudaStream_t stream);
+size_t p2g_tile_smem(int uz);
+cudaError_t p2g_tile_prepare();   // the shared-memory attribute of both unit depths
 __global__ void k_grid3_dense(Step3 s);
 __global__ void k_g2p3(Step3 s);
 __global__ void k_g2p3_tile(Step3 s);
