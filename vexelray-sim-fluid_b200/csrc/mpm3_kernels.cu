@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 //     permutation. The warp stages it in shared memory, puts each cell's run in ascending order there (the stable
 //     sort's fix-up, fused here: G2P then reads the stable permutation), and writes the range back.
 //  2. Cells are dealt to lanes from a queue ordered by particle count, largest first: a lane sums one whole cell's
-//     27 x 4 deposits in registers (loading two particles ahead), adds them into the warp's 10 x 10 x 4 node
+//     27 x 4 deposits in registers (loading two particles ahead), adds them into the warp's 10 x 10 x (UZ + 2) node
 //     window in shared memory when the cell is done, and takes the next cell. A cell's count varies (about
 //     8 +- 2.6 at 8 per cell), so one fixed cell per lane left half the lanes idle behind each warp's fullest cell;
 //     the queue keeps them busy. Lanes that finish together add at the same stencil offset into distinct cells'
