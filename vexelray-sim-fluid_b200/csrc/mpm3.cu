@@ -143,7 +143,7 @@ Step3 make_step(vf_mpm3* h) {
 int persistent_blocks(int per_sm) { return sm_count() * per_sm; }
 
 // VF_P2G_AUTO: the schedule measured fastest for the handle's size. Below about 600k particles the tiled scatter,
-// one warp per unit of 8x8x1 cells (8x8x2 from a million particles), leaves much of the GPU idle: the
+// one warp per unit of 8x8x1 cells, leaves much of the GPU idle: the
 // warp-aggregated scatter over the dense grid is 1.8x faster at 17k particles in a 40^3 box and 1.2x at 358k in
 // 96^3. Above that, or on grids where the dense passes (clear, grid update: 48 B a node) would cost more than the
 // particles, the tile wins (1.05x at 0.9M in 128^3, 1.35x at 7.2M in 256^3). Sparse storage always runs the tile.
@@ -277,9 +277,8 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     }
     if (mask & VF3_PASS_SCATTER) {
         if (tile) {
-            // half-depth units below a million particles, where 8x8x2-cell units would leave SMs idle
             h->prof.begin("k_p2g3_tile", h->stream);
-            const cudaError_t e = launch_p2g3_tile(h->np < (1 << 20) ? 1 : 2, persistent_blocks(2), s, h->stream);
+            const cudaError_t e = launch_p2g3_tile(persistent_blocks(2), s, h->stream);
             h->prof.end(h->stream);
             VF_TRY_CUDA(e);
         } else if (h->p2g == VF_P2G_WARP) {
@@ -508,7 +507,7 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
                        (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);
     if (p2g_tile_prepare() != cudaSuccess) {
-        set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem(2));
+        set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem());
         return fail(VF_ECUDA);
     }
     vf_mpm3_prepared* p = new vf_mpm3_prepared();

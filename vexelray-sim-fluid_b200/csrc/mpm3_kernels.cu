@@ -235,8 +235,9 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 // which is (w m)(v_a + C_a . d) + w s d_a with d = o - f (Flip3.java:225-243).
 constexpr int P2G_THREADS = 128;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
-// A work unit is UZ brick z-layers: 2 (8x8x2 cells, about 1,000 particles) by default, 1 for scenes of few bricks,
-// where twice the units keep more of the GPU busy.
+// A work unit is UZ brick z-layers. One layer (8x8x1 cells, about 500 particles at 8 a cell) measured fastest at
+// every size: 0.54x the time of two layers at 17k particles, 0.91x at 2.9M, 0.95x at 7.2M (more units even out
+// the warps' queues and shorten their tails). Deeper units measured slower (4 layers: 2.6x at 8.2M).
 constexpr int WWX = WIN, WWY = WIN;
 constexpr int RUN_CAP = 2048;   // particle slots of one unit staged in shared memory (more: sorted in place)
 constexpr int NBUCKET = 32;     // count buckets of the cell queue (counts of 31 and more share the last)
@@ -538,21 +539,17 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
     }
 }
 
-size_t p2g_tile_smem(int uz) { return uz == 1 ? sizeof(P2GShared<1>) : sizeof(P2GShared<2>); }
+constexpr int P2G_UZ = 1;   // the unit depth the scatter runs
+
+size_t p2g_tile_smem() { return sizeof(P2GShared<P2G_UZ>); }
 
 cudaError_t p2g_tile_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_p2g3_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p2g_tile_smem(1));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_p2g3_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_tile_smem(2));
-    return e;
+    return cudaFuncSetAttribute(k_p2g3_tile<P2G_UZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)p2g_tile_smem());
 }
 
-cudaError_t launch_p2g3_tile(int uz, int blocks, const Step3& s, cudaStream_t stream) {
-    if (uz == 1)
-        k_p2g3_tile<1><<<blocks, P2G_THREADS, p2g_tile_smem(1), stream>>>(s);
-    else
-        k_p2g3_tile<2><<<blocks, P2G_THREADS, p2g_tile_smem(2), stream>>>(s);
+cudaError_t launch_p2g3_tile(int blocks, const Step3& s, cudaStream_t stream) {
+    k_p2g3_tile<P2G_UZ><<<blocks, P2G_THREADS, p2g_tile_smem(), stream>>>(s);
     return cudaGetLastError();
 }
 

@@ -197,10 +197,10 @@ __global__ void k_pool_unpack3(Step3 s, float4* dense);
 __global__ void k_key_count3(Step3 s);
 __global__ void k_p2g3_atomic(Step3 s);
 __global__ void k_p2g3_warp(Step3 s);
-// The tiled scatter with work units of uz brick z-layers (1 or 2): 128 threads a CTA, two CTAs an SM.
-cudaError_t launch_p2g3_tile(int uz, int blocks, const Step3& s, cudaStream_t stream);
-size_t p2g_tile_smem(int uz);
-cudaError_t p2g_tile_prepare();   // the shared-memory attribute of both unit depths
+// The tiled scatter (work units of 8x8x1 cells): 128 threads a CTA, two CTAs an SM.
+cudaError_t launch_p2g3_tile(int blocks, const Step3& s, cudaStream_t stream);
+size_t p2g_tile_smem();
+cudaError_t p2g_tile_prepare();   // its shared-memory attribute
 __global__ void k_grid3_dense(Step3 s);
 __global__ void k_g2p3(Step3 s);
 __global__ void k_g2p3_tile(Step3 s);
