@@ -1,13 +1,17 @@
 #!/usr/bin/env python
-"""bench.py -- the 3D MLS-MPM dam break at 256^3 (about 8.2M particles), one B200 per rank.
+"""bench.py -- the 3D MLS-MPM dam break at 256^3 (8,156,736 particles), one B200 per rank.
 
 A step is one full ParticleSimulation3.advance(1): the per-step counting sort by stencil cell, the
-sorted brick-tile P2G, the grid update fused into the brick-tile G2P, on inputs resident in HBM.
-The line reports particle-steps/s for the whole job, the P2G+G2P roofline against the measured HBM
+scatter (P2G), the grid update and the gather (G2P), on inputs resident in HBM. The last stdout line
+is the headline: particle-steps/s for the whole job, the P2G+G2P roofline against the measured HBM
 bandwidth, the same metric end to end through the public API (host arrays in, positions out), the
-oracle's threaded CPU step as the CPU baseline, and a shallow-water sub-measurement (4096^2, HLL).
+oracle's threaded CPU step as the CPU baseline, and the SM clocks sampled in the timed region.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--only swe,batch,...]
+
+--only runs sub-measurements of the other configurations (shallow water, the 2D dam break, the literal
+box, the batched scenes, the learned solver, the P2G schedules, tension and sparse storage) first, each
+printed as one JSON line ahead of the headline.
 
 Under torchrun each rank runs an independent replica on its own GPU (the 3D step does not shard
 across GPUs here: replicas only); the time is the max over ranks and the value the sum of work.
@@ -41,11 +45,9 @@ BOX3_LITERAL = ((0.05, 0.45), (0.05, 0.65), (0.05, 0.45))   # the literal box: 1
 DT3 = 5e-5
 G_SI = 9.8
 SEED3 = 1
-WORKLOAD3 = ("3D MLS-MPM APIC dam break, 256^3 nodes, dx=1/256, 8 particles/cell jittered from seed 1 in "
-             "[0.05,0.45]x[0.05,0.4325]x[0.05,0.45] (8,156,736 particles; the literal [0.05,0.65] y-extent gives "
-             "12,734,496: literal_box), "
-             "dt=5e-5, gravity -9.8 m/s^2, p=B(1/J-1) with B=(5 sqrt(2gH))^2, counting sort by stencil cell "
-             "every step, sorted shared-memory-tile P2G")
+WORKLOAD3 = ("3D MLS-MPM APIC dam break, 256^3 nodes, dx=1/256, 8 ppc jittered (seed 1) in "
+             "[0.05,0.45]x[0.05,0.4325]x[0.05,0.45] = 8,156,736 particles, dt=5e-5, g=-9.8 m/s^2, "
+             "counting sort by stencil cell every step")
 
 N_SWE = 4096
 SEED_SWE = 2
@@ -154,33 +156,72 @@ def batch_scenes(seed=SEED_BATCH, count=N_BATCH, np_range=BATCH_NP, grids=BATCH_
 # ---------------------------------------------------------------------------------------------- helpers
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during a timed region."""
+    """SM clock and throttle reasons sampled during a timed region: NVML polled every 2 ms from a thread (the timed
+    region of the default run is tens of milliseconds), or nvidia-smi every 200 ms where NVML cannot be loaded."""
 
+    REASONS = {"hw_slowdown": 0x2, "sw_power_cap": 0x4, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
+        self.samples: list[tuple[float, int]] = []   # (SM MHz, reason bits)
+        self.max_mhz = None
         self.proc = None
-        self.lines: list[str] = []
+        self.stop = threading.Event()
+        self.thread = None
+        self.nvml = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-            self.reader = threading.Thread(target=self._read, daemon=True)
-            self.reader.start()
-        except OSError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM))
+            self.nvml = pynvml
+
+            def poll():
+                while not self.stop.is_set():
+                    mhz = pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM)
+                    bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    self.samples.append((float(mhz), int(bits)))
+                    time.sleep(0.002)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            time.sleep(0.005)
+        except Exception:
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._read_smi, daemon=True)
+                self.thread.start()
+            except OSError:
+                self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz, self.max_mhz = float(f[1]), float(f[2])
+            except ValueError:
+                continue
+            bits = 0
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower().startswith("active"):
+                    bits |= self.REASONS[name]
+            self.samples.append((mhz, bits))
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=1)
         if self.proc:
             time.sleep(0.25)
             self.proc.terminate()
@@ -190,23 +231,12 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [v.strip() for v in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
+        reasons = sorted({name for name, bit in self.REASONS.items() for _, b in self.samples if b & bit})
+        return {"sm_mhz": statistics.median(s for s, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "nvml every 2 ms" if self.nvml is not None else "nvidia-smi every 200 ms"}
 
 
 def measured_peaks():
@@ -382,8 +412,9 @@ def run_literal(args, vf):
             "p2g_g2p_hbm_frac": (152.0 * np3 + 28.0 * touched) / (pg / 1e3) / 1e9 / measured_peaks()[0]}
 
 
-def cpu_step_rate(x, y, z, m, params, budget_s=20.0, max_steps=3):
-    """The oracle's threaded 3D step on the host cores over the full workload: particle-steps/s."""
+def cpu_step_rate(x, y, z, m, params, budget_s=10.0, min_steps=10, max_steps=40, warmup=1):
+    """The oracle's threaded 3D step on the host cores over the full workload: particle-steps/s over at least
+    `min_steps` steps (more while the budget lasts), after `warmup` untimed steps."""
     sys.path.insert(0, str(ROOT / "tests"))
     from _oracle import Flip3State, OrPhysics, fp, lib as olib
     n = N3
@@ -391,9 +422,10 @@ def cpu_step_rate(x, y, z, m, params, budget_s=20.0, max_steps=3):
     pw = np.ascontiguousarray(np.array(params, np.float32))
     threads = olib().or_baseline_threads()
     t0 = time.perf_counter()
-    olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)   # warm-up (page faults)
-    first = time.perf_counter() - t0
-    steps = max(1, min(max_steps, int(budget_s / max(first, 1e-3))))
+    for _ in range(max(1, warmup)):   # warm-up (page faults)
+        olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)
+    first = (time.perf_counter() - t0) / max(1, warmup)
+    steps = max(min_steps, min(max_steps, int(budget_s / max(first, 1e-3))))
     t0 = time.perf_counter()
     for _ in range(steps):
         olib().or_flip3_step_omp(ctypes.byref(s.s), fp(pw), OrPhysics(0, 0), None)
@@ -403,22 +435,39 @@ def cpu_step_rate(x, y, z, m, params, budget_s=20.0, max_steps=3):
 
 # ---------------------------------------------------------------------------------------------- arms
 
+METRIC = "MPM particle-steps/s"
+DATA = "synthetic (seeded jittered dam break)"
+
+
 def run_reference(args, dist: Dist):
+    """The reference arm: the oracle's C restatement of Flip3Step (the reference's own CPU path cannot run here),
+    OpenMP on all host threads, W untimed steps then K timed steps of the full workload, on rank 0 only."""
     if dist.rank != 0:
         return
     x, y, z, m, params = dam3()
-    rate, threads, steps, el = cpu_step_rate(x, y, z, m, params, budget_s=60.0, max_steps=max(1, args.steps))
-    sample = (f"{steps} full steps of the 8.16M-particle 256^3 workload (oracle C port of Flip3Step, OpenMP, "
-              f"{threads} threads), {el:.1f} s")
-    line = {"metric": "MPM particle-steps/s", "value": rate, "unit": "particle-steps/s", "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered dam break)",
+    rate, threads, steps, el = cpu_step_rate(x, y, z, m, params, budget_s=0.0, min_steps=max(1, args.steps),
+                                             max_steps=max(1, args.steps), warmup=max(1, args.warmup))
+    sample = (f"{steps} full steps of the 8.16M-particle 256^3 workload after {max(1, args.warmup)} untimed ones "
+              f"(oracle C port of Flip3Step, OpenMP, {threads} threads), {el:.1f} s")
+    line = {"metric": METRIC, "value": rate, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": el / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
             "config": {"workload": WORKLOAD3, "particles": len(x), "grid": [N3] * 3},
             "impl": "reference",
             "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def emit(name, result, detail):
+    """A sub-measurement: one JSON line on stdout (before the headline, which is always the last line), and the
+    same object into the detail file when one is named."""
+    if result is None:
+        return
+    print(json.dumps({"sub": name, **result}), flush=True)
+    if detail is not None:
+        detail[name] = result
 
 
 def run_ours(args, dist: Dist):
@@ -458,45 +507,13 @@ def run_ours(args, dist: Dist):
     prof = sim.profile_read()
     sim.profile(False)
     touched = sim.touched_nodes()
-    t_p2g = prof.get("k_p2g3_tile", (0.0, 1))
-    t_g2p = prof.get("k_g2p3_tile", (0.0, 1))
-    per_step_ms = (t_p2g[0] + t_g2p[0]) / args.steps
-    alg_bytes = 152.0 * np3 + 28.0 * touched
-    achieved = alg_bytes / (per_step_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    tr_p2g, tr_g2p = profiled_traffic("k_p2g3_tile"), profiled_traffic("k_g2p3_tile")
-    traffic = (tr_p2g + tr_g2p) if (tr_p2g is not None and tr_g2p is not None) else None
+    roof = roofline3(prof, args.steps, np3, touched)
     total_prof = sum(v[0] for v in prof.values())
-    kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1], "share": v[0] / total_prof}
-               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
-
-    # the three P2G schedules the 3D config compares, each for K profiled steps from the same state
-    variants = {}
-    if not args.no_variants:
-        names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile",
-                 vf.VF_P2G_FIXED: "exact_fixed_point"}
-        for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_FIXED, vf.VF_P2G_TILE):
-            sim.set_schedule(sched)
-            sim.advance(2)
-            sim.finish()
-            sim.profile(True)
-            ev0.record(stream)
-            sim.advance(args.variant_steps)
-            ev1.record(stream)
-            v_ms = ev0.elapsed_ms(ev1)
-            vp = sim.profile_read()
-            sim.profile(False)
-            p2g = [k for k in vp if k.startswith("k_p2g3") or k == "k_fixed_to_grid3"]
-            variants[names[sched]] = {
-                "ms_per_step": v_ms / args.variant_steps,
-                "p2g_ms_per_step": sum(vp[k][0] for k in p2g) / args.variant_steps,
-                "kernels_ms_per_step": {k: v[0] / args.variant_steps for k, v in vp.items()}}
-        sim.set_schedule(vf.VF_P2G_TILE)
+    kernels = {k: round(v[0] / total_prof, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])[:4]}
 
     # end to end through the public API: pinned host arrays in (load), K steps, positions out (read)
     outs = [np.empty(np3, np.float32) for _ in range(3)]
-    ins = [x, y, z, zeros, zeros, zeros, m]
-    with vf.Pinned(*([a for a in ins[:3]] + [zeros, m] + outs)):
+    with vf.Pinned(*([x, y, z] + [zeros, m] + outs)):
         dist.barrier()
         sim.finish()
         ev0.record(stream)
@@ -508,76 +525,125 @@ def run_ours(args, dist: Dist):
         e2e_ms = dist.max(ev0.elapsed_ms(ev1))
     e2e = {"value": dist.sum(float(np3) * args.steps) / (e2e_ms / 1e3), "unit": "particle-steps/s",
            "h2d_bytes_per_step": 7 * np3 * 4 / args.steps, "d2h_bytes_per_step": 3 * np3 * 4 / args.steps,
-           "job": f"load (7 fields) + {args.steps} steps + read x,y,z, one job per rank"}
+           "job": f"load 7 fields + {args.steps} steps + read x,y,z"}
+    detail = {} if args.detail else None
+    if "variants" in args.extras:
+        emit("p2g_variants", run_variants(args, vf, sim), detail)
     sim.close()
-    literal = None if args.no_literal else run_literal(args, vf)
-    c0 = None if args.no_c0 else run_c0(args, vf, dist)
 
-    # shallow water, 4096^2 HLL, a sub-measurement (cells/s and its own roofline)
-    swe = None
-    if not args.no_swe:
-        h = swe_bumps()
-        zero2 = np.zeros_like(h)
-        with vf.PatchSimulation(N_SWE, N_SWE) as p:
-            p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
-            p.write_budget(0, 2 ** 31 - 1)
-            p.dispatch(3)
-            p.read_budget(0)
-            k_swe = max(10, args.steps)
-            s_stream = p.stream()
-            ev0.record(s_stream)
-            p.dispatch(k_swe)
-            ev1.record(s_stream)
-            swe_ms = ev0.elapsed_ms(ev1)
-            p.profile(True)
-            p.dispatch(k_swe)
-            p.read_budget(0)
-            sp = p.profile_read()
-            p.profile(False)
-        cells = N_SWE * N_SWE
-        k_ms = sp["k_swe_tile"][0] / sp["k_swe_tile"][1]
-        swe = {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)",
-               "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
-               "roofline": {"bound": "hbm", "achieved": 24.0 * cells / (k_ms / 1e3) / 1e9, "peak": peak,
-                            "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
-                            "kernel": "k_swe_tile", "bytes_per_cell": 24},
-               "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
-
-    batch = None if args.no_batch else run_batch(args, vf, dist, peak)
-    next_rows = None if args.no_next else run_next_rows(args, vf, peak, cpu=not args.no_cpu and dist.rank == 0)
-    learned = None if args.no_learned else run_learned(args, vf)
+    peak, _ = measured_peaks()
+    if "literal" in args.extras:
+        emit("literal_box", run_literal(args, vf), detail)
+    if "c0" in args.extras:
+        emit("c0_2d", run_c0(args, vf, dist), detail)
+    if "swe" in args.extras:
+        emit("swe", run_swe(args, vf, dist, peak), detail)
+    if "batch" in args.extras:
+        emit("batch", run_batch(args, vf, dist, peak), detail)
+    if "next" in args.extras:
+        emit("next_rows", run_next_rows(args, vf, peak, cpu=not args.no_cpu and dist.rank == 0), detail)
+    if "learned" in args.extras:
+        emit("learned", run_learned(args, vf), detail)
+    if detail is not None and dist.rank == 0:
+        pathlib.Path(args.detail).write_text(json.dumps(detail, indent=1))
 
     if dist.rank != 0:
         return
-    cpu_rate, threads, cpu_steps, cpu_el = (None, 0, 0, 0.0)
+    cpu = None
     if not args.no_cpu:
-        cpu_rate, threads, cpu_steps, cpu_el = cpu_step_rate(x, y, z, m, params, budget_s=20.0)
+        rate, threads, cpu_steps, cpu_el = cpu_step_rate(x, y, z, m, params)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{cpu_steps} full steps of this workload, oracle C port of Flip3Step, OpenMP, {cpu_el:.1f} s"}
     line = {
-        "metric": "MPM particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered dam break)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD3, "particles": np3, "grid": [N3] * 3, "parallelism": f"replicas x{dist.world}",
-                   "l2": "inputs larger than L2 (particles 555 MB per set, grid 268 MB per buffer)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_p2g3_tile + k_g2p3_tile (P2G+G2P)", "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_step": alg_bytes, "touched_nodes": touched,
-                     "p2g_g2p_ms_per_step": per_step_ms},
-        "kernels": kernels,
-        "cpu_baseline": None if cpu_rate is None else {
-            "value": cpu_rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{cpu_steps} full steps of the same workload, oracle C port of Flip3Step, OpenMP, {cpu_el:.1f} s"},
+                   "l2": "inputs larger than L2 (particles 555 MB a set)"},
+        "roofline": roof,
+        "kernels_share": kernels,
+        "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
-        "swe": swe,
-        "c0_2d": c0,
-        "literal_box": literal,
-        "batch": batch,
-        "learned": learned,
-        "p2g_variants": variants,
-        "next_rows": next_rows,
     }
-    print(json.dumps(line), flush=True)
+    text = json.dumps(line)
+    assert len(text) < 2048, f"the headline line grew to {len(text)} bytes"
+    print(text, flush=True)
+
+
+def roofline3(prof, steps, np3, touched):
+    """The P2G+G2P roofline from a profiled run: algorithmic bytes 152 Np + 28 N_t per step over the two kernels'
+    event-timed device time."""
+    t_p2g = prof.get("k_p2g3_tile", (0.0, 1))
+    t_g2p = prof.get("k_g2p3_tile", (0.0, 1))
+    per_step_ms = (t_p2g[0] + t_g2p[0]) / steps
+    alg_bytes = 152.0 * np3 + 28.0 * touched
+    achieved = alg_bytes / (per_step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    tr_p2g, tr_g2p = profiled_traffic("k_p2g3_tile"), profiled_traffic("k_g2p3_tile")
+    traffic = (tr_p2g + tr_g2p) if (tr_p2g is not None and tr_g2p is not None) else None
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "kernel": "k_p2g3_tile + k_g2p3_tile", "peak_kind": peak_kind,
+            "algorithmic_bytes_per_step": alg_bytes, "touched_nodes": touched, "kernels_ms_per_step": round(per_step_ms, 4)}
+
+
+def run_variants(args, vf, sim):
+    """The P2G schedules the 3D configuration compares, each for K profiled steps from the same state."""
+    ev0, ev1 = vf.Event(), vf.Event()
+    stream = sim.stream()
+    variants = {}
+    names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile",
+             vf.VF_P2G_FIXED: "exact_fixed_point"}
+    for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_FIXED, vf.VF_P2G_TILE):
+        sim.set_schedule(sched)
+        sim.advance(2)
+        sim.finish()
+        sim.profile(True)
+        ev0.record(stream)
+        sim.advance(args.variant_steps)
+        ev1.record(stream)
+        v_ms = ev0.elapsed_ms(ev1)
+        vp = sim.profile_read()
+        sim.profile(False)
+        p2g = [k for k in vp if k.startswith("k_p2g3") or k == "k_fixed_to_grid3"]
+        variants[names[sched]] = {
+            "ms_per_step": v_ms / args.variant_steps,
+            "p2g_ms_per_step": sum(vp[k][0] for k in p2g) / args.variant_steps,
+            "kernels_ms_per_step": {k: v[0] / args.variant_steps for k, v in vp.items()}}
+    sim.set_schedule(vf.VF_P2G_TILE)
+    return {"workload": WORKLOAD3, "steps": args.variant_steps, "schedules": variants}
+
+
+def run_swe(args, vf, dist, peak):
+    """Shallow water, 4096^2 HLL: cell-updates/s, the k_swe_tile roofline at 24 B a cell, the oracle on one core."""
+    h = swe_bumps()
+    zero2 = np.zeros_like(h)
+    ev0, ev1 = vf.Event(), vf.Event()
+    with vf.PatchSimulation(N_SWE, N_SWE) as p:
+        p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
+        p.write_budget(0, 2 ** 31 - 1)
+        p.dispatch(3)
+        p.read_budget(0)
+        k_swe = max(10, args.steps)
+        s_stream = p.stream()
+        ev0.record(s_stream)
+        p.dispatch(k_swe)
+        ev1.record(s_stream)
+        swe_ms = ev0.elapsed_ms(ev1)
+        p.profile(True)
+        p.dispatch(k_swe)
+        p.read_budget(0)
+        sp = p.profile_read()
+        p.profile(False)
+    cells = N_SWE * N_SWE
+    k_ms = sp["k_swe_tile"][0] / sp["k_swe_tile"][1]
+    return {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)",
+            "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
+            "roofline": {"bound": "hbm", "achieved": 24.0 * cells / (k_ms / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "kernel": "k_swe_tile", "bytes_per_cell": 24},
+            "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
 
 
 CNN_FLOPS_PER_CELL = 2 * 25 * (3 * 32 + 32 * 32 + 32 * 6)   # 65.6 kFLOP: the three convolutions, algorithmic
@@ -919,26 +985,32 @@ def run_batch(args, vf, dist: Dist, peak):
     return out
 
 
+EXTRAS = ("swe", "c0", "literal", "batch", "learned", "variants", "next")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water sub-measurement")
-    ap.add_argument("--no-variants", action="store_true", help="skip the comparison of the three P2G schedules")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
+    ap.add_argument("--only", default="",
+                    help="comma-separated sub-measurements to run before the headline: " + ",".join(EXTRAS) +
+                         " (or 'all'); each prints one JSON line, the headline stays the last line")
+    ap.add_argument("--detail", default=None, help="also write the sub-measurements to this JSON file")
     ap.add_argument("--variant-steps", type=int, default=20)
-    ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes sub-measurement")
-    ap.add_argument("--no-literal", action="store_true", help="skip the 12.7M-particle literal-box sub-measurement")
-    ap.add_argument("--no-c0", action="store_true", help="skip the 2D configuration's sub-measurement")
-    ap.add_argument("--no-learned", action="store_true", help="skip the learned shallow-water sub-measurement")
-    ap.add_argument("--no-next", action="store_true",
-                    help="skip the surface-tension and sparse-storage sub-measurements")
     ap.add_argument("--learned-seeds", type=int, default=64, help="held-out seeds of the learned evaluation")
     ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
                     help="the batched step's autotune cache (JSON)")
     args = ap.parse_args()
+    wanted = {w.strip() for w in args.only.split(",") if w.strip()}
+    if "all" in wanted:
+        wanted = set(EXTRAS)
+    unknown = wanted - set(EXTRAS)
+    if unknown:
+        ap.error(f"unknown sub-measurements: {sorted(unknown)}")
+    args.extras = wanted
     dist = Dist()
     try:
         if args.impl == "reference":

@@ -8,7 +8,7 @@
  *   ParticleSimulation3  (vexelray-sim-fluid-gui/.../gui/ParticleSimulation3.java)  -> vf_mpm3_*
  *   PatchSimulation      (vexelray-sim-fluid-gui/.../gui/PatchSimulation.java)      -> vf_swe_*
  * The Java classes keep their public methods and call these through Panama FFM
- * (see INTEGRATION.md for the downcall stubs).
+ * downcalls, one per entry point below.
  *
  * Conventions
  *  - Every function returns int32_t status: VF_OK (0) or a negative VF_E* code. The
@@ -47,6 +47,9 @@ int32_t vf_last_error(char* buf, size_t cap);
 /* Library version, and whether a usable CUDA device is present (1) or not (0). */
 int32_t vf_version(void);
 int32_t vf_device_ok(void);
+/* The architecture the library's kernels were compiled for, as the runtime reports it for one of them
+ * (cudaFuncAttributes.binaryVersion: 100 for sm_100a code). VF_ENODEV without a device. */
+int32_t vf_binary_version(int32_t* out);
 /* Selects the CUDA device the calling thread's next handles use (one process per GPU). */
 int32_t vf_set_device(int32_t device);
 
@@ -158,8 +161,8 @@ int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t
  * is one fixed array in the library (about 7 MB, held on every GPU that loads the library until exit), so
  * it takes at most 262144 particles and 262144 cells ((nx-1)(ny-1)); larger inputs get VF_EINVAL. Every
  * call shares that array: calls that overlap on the GPU race, so a caller with several threads or streams
- * serialises them. The first call on a device looks up the array's device address; make it before any
- * stream capture. Same outputs as vf_sort2. */
+ * serialises them. Each call looks up the array's device address on the current device; the first call on a
+ * device also loads the library there, so make it before any stream capture. Same outputs as vf_sort2. */
 int32_t vf_sort2_noalloc(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm,
                          int32_t* starts);
 
@@ -192,6 +195,12 @@ int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, con
  * Returns when submitted; vf_mpm2_batch_finish waits and reports device errors. */
 int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count);
 int32_t vf_mpm2_batch_finish(vf_mpm2_batch* h);
+/* The polls a CTA of the step kernel makes at a grid barrier before it gives up (0, the default, is about a
+ * second's worth). A barrier that gives up sets the device status: the step's kernel ends, the next blocking call
+ * returns VF_ETIMEOUT, and the batch refuses to step (VF_ESTATE) until it is loaded again, which also restores the
+ * default. A test hook for the bounded wait; the reference's analogue is Stepper's runaway guard
+ * (vexelray-sim-fluid-core/.../stencil/Stepper.java:88-93). */
+int32_t vf_mpm2_batch_set_wait_limit(vf_mpm2_batch* h, int32_t polls);
 /* One scene's particle field (VF2_X..VF2_C11, in the batch's sorted order: by tile and cell, the order within a
  * cell unspecified) or the last step's grid
  * (VF2_GM, VF2_GMU, VF2_GMV; nx*ny floats). Blocking. */

@@ -200,10 +200,12 @@ void or_particle_diagnostics(const float* j, int64_t n, double speed, double sou
     qsort(valid, (size_t)m, sizeof(float), cmp_float);
     int64_t p99 = (int64_t)(0.99 * m); if (p99 > m - 1) p99 = m - 1;
     int64_t p01 = (int64_t)(0.01 * m); if (p01 > m - 1) p01 = m - 1;
-    out->min_density = 1.0 / valid[m - 1];
-    out->max_density = 1.0 / valid[0];
-    out->low_density = 1.0 / valid[p99];
-    out->high_density = 1.0 / valid[p01];
+    /* Java's 1 / valid[k] with valid a float[] is a float division (the int 1 is promoted to float); the
+       record's double field then holds the float quotient */
+    out->min_density = (double)(1.0f / valid[m - 1]);
+    out->max_density = (double)(1.0f / valid[0]);
+    out->low_density = (double)(1.0f / valid[p99]);
+    out->high_density = (double)(1.0f / valid[p01]);
     free(valid);
 }
 

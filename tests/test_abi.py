@@ -39,10 +39,41 @@ def test_library_exports_every_declared_entry_point():
         assert getattr(L, d) is not None
 
 
-def test_library_has_sm100a_code():
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(vexfluid.LIBRARY)], capture_output=True,
-                         text=True)
-    assert "sm_100a" in out.stdout, out.stdout + out.stderr
+def test_binary_version_needs_a_device():
+    """vf_binary_version reports the architecture the runtime sees for the library's kernels; without a device it
+    is VF_ENODEV (the GPU test checks the value)."""
+    L = vexfluid.lib()
+    v = ctypes.c_int32(0)
+    rc = L.vf_binary_version(ctypes.byref(v))
+    if L.vf_device_ok():
+        assert rc == 0 and v.value == 100, (rc, v.value)
+    else:
+        assert rc == vexfluid.VF_ENODEV
+
+
+@pytest.mark.gpu
+def test_library_runs_sm100a_code():
+    """The runtime loads the library's kernels as sm_100 binaries (cudaFuncAttributes.binaryVersion 100)."""
+    L = vexfluid.lib()
+    v = ctypes.c_int32(0)
+    assert L.vf_binary_version(ctypes.byref(v)) == 0, vexfluid.last_error()
+    assert v.value == 100
+
+
+def test_oversized_grids_are_refused_before_the_device():
+    """Cell keys are int32 in the kernels: grids whose keys would overflow are refused with VF_EINVAL, whatever
+    the device."""
+    L = vexfluid.lib()
+    h = ctypes.c_void_p()
+    assert L.vf_mpm2_create(50000, 50000, 10, 0, ctypes.byref(h)) == vexfluid.VF_EINVAL
+    assert "2^31" in vexfluid.last_error()
+    assert L.vf_mpm3_prepare(2048, 2048, 1024, 10, 0, ctypes.byref(h)) == vexfluid.VF_EINVAL
+    assert "int32" in vexfluid.last_error()
+    f = (ctypes.c_float * 1)(0.5)
+    i = (ctypes.c_int32 * 1)(0)
+    one = ctypes.c_int64(1)
+    assert L.vf_sort2(50000, 50000, f, f, one, i, i) == vexfluid.VF_EINVAL
+    assert L.vf_sort2_noalloc(50000, 50000, f, f, one, i, i) == vexfluid.VF_EINVAL
 
 
 def test_argument_checks_come_before_the_device():

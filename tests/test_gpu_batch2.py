@@ -179,3 +179,35 @@ def test_refusals():
             b.advance(1)   # nothing loaded
         with pytest.raises(vf.IllegalArgumentException):
             b.load(*[[p[f][:50] for p in parts] for f in range(5)])
+
+
+def test_a_grid_barrier_that_gives_up_reports_a_timeout():
+    """The bounded wait of the step kernel's grid barrier, made to run out: with the poll limit at one, CTAs that
+    arrive before the last one give up, set the timeout bit and end the kernel. The next blocking call returns
+    VF_ETIMEOUT, the batch refuses to step until it is loaded again, and a reload steps within the oracle's
+    one-step bar. (The reference's analogue: Stepper's runaway guard, Stepper.java:88-93.)"""
+    scenes, parts = make_batch(13, "config", shapes=SHAPES[:3])
+    with vf.BatchSimulation(scenes, **flags_of("config")) as b:
+        load(b, parts)
+        b.set_wait_limit(1)
+        b.advance(1)
+        with pytest.raises(vf.VfError) as err:
+            b.finish()
+        assert err.value.code == vf.VF_ETIMEOUT, err.value
+        assert "grid barrier timed out" in str(err.value)
+        with pytest.raises(vf.IllegalStateException):
+            b.advance(1)
+        load(b, parts)   # resets the barrier, the status and the poll limit
+        b.advance(1)
+        b.finish()
+        for k, (sc, p) in enumerate(zip(scenes, parts)):
+            o = oracle_scene(sc, p)
+            o.step(np.array(p[5], F), oracle_physics("config"))
+            for name in ("gm", "gmu", "gmv"):
+                got, want = b.read(k, name), o.g[name]
+                assert np.all(np.abs(got - want) <= 1e-5 * np.maximum(1, np.abs(want))), (k, name)
+    # a fresh batch after the timed-out one was destroyed steps normally
+    with vf.BatchSimulation(scenes, **flags_of("config")) as b:
+        load(b, parts)
+        b.advance(2)
+        b.finish()

@@ -274,3 +274,34 @@ def test_the_nominal_mass_is_measured_at_load():
         vf.check(vf.lib().vf_mpm3_nominal_mass(s._h, got.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         assert got[0] == np.finfo(F).max
         assert len(s.compression()) == 0
+
+
+def _diag_equal(got, want):
+    w = (want.min_density, want.max_density, want.low_density, want.high_density, want.mach, want.courant,
+         float(want.non_finite))
+    assert tuple(got) == w, (got, w)
+
+
+def test_particle_diagnostics_on_the_device_match_the_oracle():
+    """ParticleDiagnostics.of (ParticleDiagnostics.java:126-148) computed on the device by radix selection over
+    J, against the oracle's sort of the same J read back: every field equal. Covers J after a dam-break slab's
+    steps, then J rewritten with the values the reference refuses (NaN, infinities, zero, negatives), denormals,
+    ties and a spread of magnitudes."""
+    from _oracle import particle_diagnostics
+    fall = math.sqrt(2 * 200 * 12)
+    bulk = (5 * fall) ** 2
+    dt = stable_step(bulk, 1.0, fall, 0.3)
+    x, y, z, m = slab3(71, 24)
+    with vf.ParticleSimulation3(24, 24, 24, len(x)) as s:
+        s.load([x, y, z], [np.zeros_like(x)] * 3, m, vf.flip3_params(dt, 0.0, -200.0, 0.0, bulk, 1.0))
+        s.advance(30)
+        j = s.read("j")
+        _diag_equal(s.particle_diagnostics(fall, 5 * fall, dt), particle_diagnostics(j, fall, 5 * fall, dt))
+        rng = np.random.default_rng(4)
+        k = np.exp(rng.normal(0, 2, len(x))).astype(F)
+        k[:9] = [np.nan, np.inf, -np.inf, 0.0, -0.0, -1.0, 1e-42, 1e-40, 3e38]
+        k[9:40] = np.float32(1.25)   # ties
+        s.write("j", k)
+        _diag_equal(s.particle_diagnostics(1.0, 2.0, 0.5), particle_diagnostics(k, 1.0, 2.0, 0.5))
+        s.write("j", np.full(len(x), np.nan, F))   # nothing valid
+        _diag_equal(s.particle_diagnostics(1.0, 2.0, 0.5), particle_diagnostics(np.full(len(x), np.nan, F), 1.0, 2.0, 0.5))

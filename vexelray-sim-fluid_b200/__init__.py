@@ -97,6 +97,7 @@ def lib() -> ctypes.CDLL:
         "vf_last_error": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int32),
         "vf_version": ([], ctypes.c_int32),
         "vf_device_ok": ([], ctypes.c_int32),
+        "vf_binary_version": ([ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
         "vf_set_device": ([ctypes.c_int32], ctypes.c_int32),
         "vf_event_create": ([ctypes.POINTER(_vp)], ctypes.c_int32),
         "vf_event_record": ([_vp, _vp], ctypes.c_int32),
@@ -165,6 +166,7 @@ def lib() -> ctypes.CDLL:
         "vf_mpm2_batch_load": ([_vp] + [_f32p] * 5, ctypes.c_int32),
         "vf_mpm2_batch_advance": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_batch_finish": ([_vp], ctypes.c_int32),
+        "vf_mpm2_batch_set_wait_limit": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm2_batch_read": ([_vp, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_int64], ctypes.c_int32),
         "vf_mpm2_batch_config": ([_vp, ctypes.c_int32] + [_i32p] * 4, ctypes.c_int32),
         "vf_mpm2_batch_phases": ([_vp, ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int32),
@@ -559,6 +561,11 @@ class BatchSimulation:
 
     def finish(self) -> None:
         check(lib().vf_mpm2_batch_finish(self._h))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls a CTA makes at a grid barrier before it gives up (0: the default, about a second). A load restores
+        the default."""
+        check(lib().vf_mpm2_batch_set_wait_limit(self._h, polls))
 
     def read(self, scene: int, name: str) -> np.ndarray:
         f = FIELDS2[name]

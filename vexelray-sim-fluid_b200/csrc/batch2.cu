@@ -147,6 +147,11 @@ __device__ __forceinline__ void batch_key(const Scene2& sc, float x, float y, in
 __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_step(Batch2 B) {
     extern __shared__ __align__(16) float dyn[];
     __shared__ int scan_smem[33];
+    // a step after one whose grid barrier gave up does nothing: the barrier's count is no longer consistent
+    __shared__ int dead;
+    if (threadIdx.x == 0) dead = (*(volatile uint32_t*)B.status & ST_TIMEOUT) != 0;
+    __syncthreads();
+    if (dead) return;
     const unsigned par = *B.step & 1u;   // read before the first barrier; CTA 0 advances it after
     const float* __restrict__ in = B.part[par];
     float* __restrict__ out = B.part[par ^ 1u];
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             if (carry != sc.np) set_status(B.status, ST_RANK);
         }
     }
-    grid_barrier(B.bar, B.status);
+    if (!grid_barrier(B.bar, B.status)) return;
     phase_done(0);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(B.step, 1u);
 
@@ -243,7 +248,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
         }
         if (lane == 31 && run != te) set_status(B.status, ST_RANK);
     }
-    grid_barrier(B.bar, B.status);
+    if (!grid_barrier(B.bar, B.status)) return;
     phase_done(1);
 
     // ---- 3. permute: perm[cursor[key]++] = slot, four slots per thread, one cursor bump per distinct key of a
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             if (gi < sc.nx && gj < sc.ny) g_next[sc.g0 + (int64_t)gj * sc.nx + gi] = make_float4(0, 0, 0, 0);
         }
     }
-    grid_barrier(B.bar, B.status);
+    if (!grid_barrier(B.bar, B.status)) return;
     phase_done(2);
     const int items = min(B.scene_chunk_start[B.nscenes], B.item_cap);
 
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
         }
         __syncwarp();   // the window is free for the next chunk
     }
-    grid_barrier(B.bar, B.status);
+    if (!grid_barrier(B.bar, B.status)) return;
     phase_done(3);
     if (blockIdx.x == 0 && threadIdx.x == 0) B.work[0] = 0;
 
@@ -602,6 +607,7 @@ struct vf_mpm2_batch {
     int wmax = 0;
     int64_t steps = 0, launches = 0;
     bool loaded = false;
+    bool timed_out = false;   // a grid barrier gave up: no step runs again until the next load
     cudaGraphExec_t graph = nullptr;
 };
 
@@ -667,8 +673,9 @@ int32_t batch_status(vf_mpm2_batch* h) {
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     if (st) {
         VF_TRY_CUDA(cudaMemsetAsync(h->status.ptr, 0, 4, h->stream));
+        if (st & ST_TIMEOUT) h->timed_out = true;
         set_error("a batch kernel flagged device status 0x%x%s", st,
-                  (st & ST_TIMEOUT) ? " (a grid barrier timed out)" : "");
+                  (st & ST_TIMEOUT) ? " (a grid barrier timed out; load the batch again before stepping it)" : "");
         return (st & ST_TIMEOUT) ? VF_ETIMEOUT : VF_EDEVICE;
     }
     return VF_OK;
@@ -855,6 +862,7 @@ int32_t vf_mpm2_batch_load(vf_mpm2_batch* h, const float* x, const float* y, con
     VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     h->steps = 0;
     h->loaded = true;
+    h->timed_out = false;
     return batch_status(h);
 }
 
@@ -862,6 +870,7 @@ int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
     VF_REQUIRE(count >= 0, VF_EINVAL, "count >= 0, got %d", count);
     VF_REQUIRE(h->loaded, VF_ESTATE, "load the batch before stepping it");
+    VF_REQUIRE(!h->timed_out, VF_ESTATE, "a grid barrier of this batch timed out; load it again before stepping it");
     int32_t rc;
     int left = count;
     if (left >= GRAPH_STEPS) {
@@ -874,6 +883,16 @@ int32_t vf_mpm2_batch_advance(vf_mpm2_batch* h, int32_t count) {
     for (; left > 0; left--)
         if ((rc = launch_step(h))) return rc;
     h->steps += count;
+    return VF_OK;
+}
+
+int32_t vf_mpm2_batch_set_wait_limit(vf_mpm2_batch* h, int32_t polls) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    VF_REQUIRE(polls >= 0, VF_EINVAL, "polls >= 0, got %d", polls);
+    const unsigned v = (unsigned)polls;
+    unsigned* limit = &reinterpret_cast<GridBarrier*>(h->ctl.as<unsigned>() + 4)->limit;
+    VF_TRY_CUDA(cudaMemcpyAsync(limit, &v, 4, cudaMemcpyHostToDevice, h->stream));
+    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
     return VF_OK;
 }
 

@@ -102,6 +102,8 @@ __device__ __forceinline__ float impulse_factor(float dt, float m, float rho0, f
 // ------------------------------------------------------------------ grid-wide barrier (cooperative launches)
 struct GridBarrier {
     unsigned count, gen;
+    unsigned limit;   // polls before a waiter gives up; 0 = BAR_SPINS
+    unsigned pad;
 };
 
 constexpr int BAR_SPINS = 1 << 24;   // x ~64 ns of __nanosleep: about a second
@@ -113,11 +115,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 }
 
 // Grid-wide barrier of a cooperative launch (all CTAs co-resident). The last CTA to arrive resets the
-// count and advances the generation; the others wait for the generation to change, at most BAR_SPINS
-// polls, after which they set ST_TIMEOUT and go on (the host reports the status; the kernel ends).
-__device__ __forceinline__ void grid_barrier(GridBarrier* b, uint32_t* status) {
+// count and advances the generation; the others wait for the generation to change, at most `limit` polls
+// (BAR_SPINS when it is 0), after which they set ST_TIMEOUT. Returns false, to the whole CTA, when this CTA
+// gave up: the caller then returns, so no CTA runs a phase whose inputs another CTA may not have finished.
+// (A CTA that passes the barrier knows every CTA arrived, whatever others did after arriving.)
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t* status) {
+    __shared__ int bar_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
+        int ok = 1;
         const unsigned gen = ld_acquire(&b->gen);
         __threadfence();
         if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
@@ -125,18 +131,23 @@ __device__ __forceinline__ void grid_barrier(GridBarrier* b, uint32_t* status) {
             __threadfence();
             atomicAdd(&b->gen, 1u);
         } else {
-            int spins = 0;
+            const unsigned limit = *(volatile unsigned*)&b->limit;
+            const unsigned cap = limit ? limit : (unsigned)BAR_SPINS;
+            unsigned spins = 0;
             while (ld_acquire(&b->gen) == gen) {
-                if (++spins > BAR_SPINS) {
+                if (++spins > cap) {
                     set_status(status, ST_TIMEOUT);
+                    ok = 0;
                     break;
                 }
                 __nanosleep(64);
             }
         }
         __threadfence();
+        bar_ok = ok;
     }
     __syncthreads();
+    return bar_ok != 0;
 }
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }

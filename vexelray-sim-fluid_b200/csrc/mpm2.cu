@@ -366,7 +366,7 @@ int32_t sort2(vf_mpm2* h) {
     k_scan_single<<<1, 1024, 0, h->stream>>>(h->counts.as<int>(), h->starts.as<int>(), h->cells);
     VF_CHECK_LAUNCH();
     k_permute<<<div_up(h->np, 256), 256, 0, h->stream>>>(h->key.as<int>(), h->rank.as<int>(), h->starts.as<int>(),
-                                                          h->perm.as<int>(), h->np, st);
+                                                          h->perm.as<int>(), h->np, h->cells, st);
     VF_CHECK_LAUNCH();
     k_fixup_cells<<<div_up(h->cells, 256), 256, 0, h->stream>>>(h->perm.as<int>(), h->starts.as<int>(), h->cells);
     VF_CHECK_LAUNCH();
@@ -413,6 +413,8 @@ int32_t vf_mpm2_create(int32_t nx, int32_t ny, int32_t particles, uint32_t flags
     *out = nullptr;
     VF_REQUIRE(particles >= 1, VF_EINVAL, "a step needs particles, got %d", particles);
     VF_REQUIRE(nx >= 3 && ny >= 3, VF_EINVAL, "a grid needs at least three nodes each way, got %d x %d", nx, ny);
+    VF_REQUIRE((int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+               "a grid of %d x %d nodes has more than 2^31-1 nodes: its cell keys would not fit an int32", nx, ny);
     int32_t rc = require_device();
     if (rc) return rc;
     vf_mpm2* h = new vf_mpm2();
@@ -612,6 +614,8 @@ int32_t vf_scatter2(int32_t mode, int32_t nx, int32_t ny, const float* x, const 
                     const float* v, const float* m, int64_t np, float* gm, float* gmu, float* gmv) {
     VF_REQUIRE(x && y && u && v && m && gm && gmu && gmv, VF_EINVAL, "null argument");
     VF_REQUIRE(nx >= 2 && ny >= 2, VF_EINVAL, "a grid needs at least two nodes each way, got %d x %d", nx, ny);
+    VF_REQUIRE((int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+               "a grid of %d x %d nodes has more than 2^31-1 nodes: its cell keys would not fit an int32", nx, ny);
     VF_REQUIRE(mode >= VF_SCATTER_GRID && mode <= VF_SCATTER_SEGMENTED, VF_EINVAL, "no schedule %d", mode);
     VF_REQUIRE(np >= 0 && np < (1LL << 31), VF_EINVAL, "particle count %lld out of range", (long long)np);
     int32_t rc = require_device();
@@ -669,6 +673,8 @@ int32_t vf_fixed_scatter2(int32_t nx, int32_t ny, const float* x, const float* y
                           int32_t* gmu, int32_t* gmv) {
     VF_REQUIRE(x && y && u && v && m && gm && gmu && gmv, VF_EINVAL, "null argument");
     VF_REQUIRE(nx >= 2 && ny >= 2, VF_EINVAL, "a grid needs at least two nodes each way");
+    VF_REQUIRE((int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+               "a grid of %d x %d nodes has more than 2^31-1 nodes: its cell keys would not fit an int32", nx, ny);
     // FixedPoint (FixedScatter.java:96-101)
     VF_REQUIRE(mass_bits >= 0 && velocity_bits >= 0 && mass_bits <= 30 && velocity_bits <= 30, VF_EINVAL,
                "bits out of range: %d, %d", mass_bits, velocity_bits);
@@ -697,6 +703,8 @@ int32_t vf_fixed_scatter2(int32_t nx, int32_t ny, const float* x, const float* y
 int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t np, int32_t* perm, int32_t* starts) {
     VF_REQUIRE(x && y && perm && starts, VF_EINVAL, "null argument");
     VF_REQUIRE(nx >= 2 && ny >= 2, VF_EINVAL, "a grid needs at least two nodes each way");
+    VF_REQUIRE((int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+               "a grid of %d x %d nodes has more than 2^31-1 nodes: its cell keys would not fit an int32", nx, ny);
     VF_REQUIRE(np >= 1 && np < (1LL << 31), VF_EINVAL, "particle count %lld out of range", (long long)np);
     int32_t rc = require_device();
     if (rc) return rc;
@@ -714,7 +722,7 @@ int32_t vf_sort2(int32_t nx, int32_t ny, const float* x, const float* y, int64_t
                                                  key.as<int>(), rank.as<int>(), cells, status.as<uint32_t>());
     k_scan_single<<<1, 1024, 0, s>>>(counts.as<int>(), dstarts.as<int>(), cells);
     k_permute<<<div_up(n, 256), 256, 0, s>>>(key.as<int>(), rank.as<int>(), dstarts.as<int>(), dperm.as<int>(), n,
-                                             status.as<uint32_t>());
+                                             cells, status.as<uint32_t>());
     k_fixup_cells<<<div_up(cells, 256), 256, 0, s>>>(dperm.as<int>(), dstarts.as<int>(), cells);
     VF_CHECK_LAUNCH();
     VF_TRY_CUDA(cudaMemcpyAsync(perm, dperm.ptr, (size_t)np * 4, cudaMemcpyDeviceToHost, s));

@@ -46,6 +46,7 @@ struct vf_mpm3 {
     DeviceBuffer params;
     DeviceBuffer status;
     DeviceBuffer scratch;     // readouts
+    DeviceBuffer pdiag;       // the particle diagnostics' histograms, made on first use
     DeviceBuffer nominal;     // the smallest positive mass loaded, as float bits (ParticleSimulation3.java:248-253)
     DeviceBuffer fixed;       // the exact schedule's grid: int64 [4][nodes], FIXED3_BITS fractional bits
     bool tension = false;     // VF_TENSION: Tension3's passes between the scatter and the grid
@@ -445,6 +446,13 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
     VF_REQUIRE(particles >= 1, VF_EINVAL, "a step needs particles, got %d", particles);
     VF_REQUIRE(nx >= 3 && ny >= 3 && nz >= 3, VF_EINVAL, "a 3D grid needs at least three nodes each way, got %d x %d x %d",
                nx, ny, nz);
+    {
+        // brick-major cell keys (bricks of 8^3 stencil cells) and node indices are int32 in the kernels
+        const int64_t bricks = (int64_t)((nx - 2 + 7) / 8) * ((ny - 2 + 7) / 8) * ((nz - 2 + 7) / 8);
+        VF_REQUIRE(bricks * 512 <= INT32_MAX && (int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+                   "a %d x %d x %d grid is too large: its cell keys (%lld) would not fit an int32", nx, ny, nz,
+                   (long long)(bricks * 512));
+    }
     int p2g = (int)((flags & VF_P2G_MASK) >> VF_P2G_SHIFT);
     VF_REQUIRE(p2g <= VF_P2G_AUTO, VF_EINVAL, "no scatter schedule %d", p2g);
     p2g = resolve_p2g(p2g, particles, (int64_t)nx * ny * nz, pool_bricks > 0);
@@ -823,15 +831,14 @@ int32_t vf_mpm3_touched_nodes(vf_mpm3* h, int64_t* out) {
 // reads J back and reduces on the host; so does this (percentiles need the sorted values).
 int32_t vf_mpm3_particle_diagnostics(vf_mpm3* h, double speed, double sound, double dt, double out[7]) {
     VF_REQUIRE(h && out, VF_EINVAL, "null argument");
-    std::vector<float> j((size_t)h->np);
-    VF_TRY_CUDA(cudaMemcpyAsync(j.data(), h->part[h->cur].as<float>() + (int64_t)J * h->stride, (size_t)h->np * 4,
-                                cudaMemcpyDeviceToHost, h->stream));
-    VF_TRY_CUDA(cudaStreamSynchronize(h->stream));
-    std::vector<float> valid;
-    valid.reserve(j.size());
-    for (float v : j)
-        if (std::isfinite(v) && v > 0) valid.push_back(v);
-    const int64_t n = (int64_t)valid.size();
+    if (!h->pdiag.ptr) {
+        int32_t rc = h->pdiag.alloc(pdiag_scratch_bytes());
+        if (rc) return rc;
+    }
+    unsigned r[5];
+    int32_t rc = pdiag_run(h->part[h->cur].as<float>() + (int64_t)J * h->stride, h->np, h->pdiag.ptr, h->stream, r);
+    if (rc) return rc;
+    const int64_t n = r[0];
     out[4] = speed / sound;
     out[5] = (speed + sound) * dt;
     out[6] = (double)(h->np - n);
@@ -839,12 +846,11 @@ int32_t vf_mpm3_particle_diagnostics(vf_mpm3* h, double speed, double sound, dou
         out[0] = out[1] = out[2] = out[3] = 0;
         return VF_OK;
     }
-    std::sort(valid.begin(), valid.end());
-    auto pct = [&](double p) { int64_t k = (int64_t)(p * n); return k < n - 1 ? k : n - 1; };
-    out[0] = 1.0 / valid[n - 1];
-    out[1] = 1.0 / valid[0];
-    out[2] = 1.0 / valid[pct(0.99)];
-    out[3] = 1.0 / valid[pct(0.01)];
+    // Java's 1 / valid[k] on a float[] is a float division; the record's double holds the float quotient
+    out[0] = (double)(1.0f / bits_to_float((int32_t)r[2]));
+    out[1] = (double)(1.0f / bits_to_float((int32_t)r[1]));
+    out[2] = (double)(1.0f / bits_to_float((int32_t)r[3]));
+    out[3] = (double)(1.0f / bits_to_float((int32_t)r[4]));
     return VF_OK;
 }
 

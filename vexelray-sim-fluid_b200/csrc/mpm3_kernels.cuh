@@ -211,4 +211,9 @@ __global__ void k_touched3(const float4* grid, int64_t nodes, unsigned long long
 __global__ void k_min_positive3(const float* m, int n, unsigned* out);
 __global__ void k_unpack_grid3(const float4* grid, float* out, int64_t nodes, int comp);
 
+// ParticleDiagnostics.of's order statistics of a device J (pdiag.cu): out = {valid count, min bits, max bits,
+// bits at the 99th percentile rank, bits at the 1st}; scratch of pdiag_scratch_bytes().
+size_t pdiag_scratch_bytes();
+int32_t pdiag_run(const float* j, int64_t n, void* scratch, cudaStream_t s, unsigned out[5]);
+
 }  // namespace vf

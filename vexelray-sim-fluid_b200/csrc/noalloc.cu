@@ -14,9 +14,9 @@
 //  * every call uses the same array and leaves its contents behind; the counts are cleared at the
 //    start of each call. Calls that overlap on the GPU (from several host threads, or several
 //    streams) race on the array and must be serialised by the caller;
-//  * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//    that device current, once per device; make that first call before any stream capture.
-#include <mutex>
+//  * each call looks up the array's device address on the current device (cudaGetSymbolAddress, a
+//    host-side lookup); the first call on a device also loads the library's module there, so make
+//    that first call before any stream capture.
 
 #include "sort.cuh"
 
@@ -31,10 +31,6 @@ constexpr int64_t WORDS = 5 * MAX_P + 2 * MAX_C + 1 + 64;   // x y key rank perm
 // The scratch. In host code its name is only a host-side stand-in: kernels get the device address
 // found by cudaGetSymbolAddress, never the symbol itself.
 static __device__ __align__(256) int32_t g_sort2_scratch[WORDS];
-
-constexpr int MAX_DEVICES = 64;
-int32_t* g_addr[MAX_DEVICES] = {};
-std::mutex g_lock;
 
 // Scatter.cell (Scatter.java:473-477), counted with warp-aggregated atomics: the sort's first pass.
 __global__ void __launch_bounds__(256) k_count_cells(const float* x, const float* y, int np, int nx, int ny,
@@ -55,23 +51,18 @@ __global__ void __launch_bounds__(256) k_count_cells(const float* x, const float
     }
 }
 
-// The device address of the scratch on the current device, looked up once per device.
+// The device address of the scratch on the current device. It is looked up on every call (a host-side table
+// lookup, no allocation), so a module reloaded after cudaDeviceReset is found at its new address.
 int32_t scratch_address(int32_t** out) {
     int dev = 0;
     VF_TRY_CUDA(cudaGetDevice(&dev));
-    VF_REQUIRE(dev >= 0 && dev < MAX_DEVICES, VF_ENODEV, "device %d is beyond the %d this entry point tracks", dev,
-               MAX_DEVICES);
-    std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_sort2_scratch);
-        if (e != cudaSuccess || !p) {
-            set_error("cudaGetSymbolAddress of the sort scratch failed on device %d: %s", dev, cudaGetErrorString(e));
-            return VF_ECUDA;
-        }
-        g_addr[dev] = (int32_t*)p;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_sort2_scratch);
+    if (e != cudaSuccess || !p) {
+        set_error("cudaGetSymbolAddress of the sort scratch failed on device %d: %s", dev, cudaGetErrorString(e));
+        return VF_ECUDA;
     }
-    *out = g_addr[dev];
+    *out = (int32_t*)p;
     return VF_OK;
 }
 
@@ -81,6 +72,8 @@ extern "C" int32_t vf_sort2_noalloc(int32_t nx, int32_t ny, const float* x, cons
                                     int32_t* perm, int32_t* starts) {
     VF_REQUIRE(x && y && perm && starts, VF_EINVAL, "null argument");
     VF_REQUIRE(nx >= 2 && ny >= 2, VF_EINVAL, "a grid needs at least two nodes each way, got %d x %d", nx, ny);
+    VF_REQUIRE((int64_t)nx * ny <= INT32_MAX, VF_EINVAL,
+               "a grid of %d x %d nodes has more than 2^31-1 nodes: its cell keys would not fit an int32", nx, ny);
     const int64_t cells = (int64_t)(nx - 1) * (ny - 1);
     VF_REQUIRE(np >= 1 && np <= MAX_P, VF_EINVAL,
                "vf_sort2_noalloc takes 1 to %lld particles, got %lld (its scratch is a fixed array; use vf_sort2)",
@@ -109,7 +102,7 @@ extern "C" int32_t vf_sort2_noalloc(int32_t nx, int32_t ny, const float* x, cons
     VF_TRY_CUDA(cudaMemcpyAsync(dy, y, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     k_count_cells<<<div_up(n, 256), 256, 0, s>>>(dx, dy, n, nx, ny, counts, key, rank, cells, status);
     k_scan_single<<<1, 1024, 0, s>>>(counts, dstarts, cells);
-    k_permute<<<div_up(n, 256), 256, 0, s>>>(key, rank, dstarts, dperm, n, status);
+    k_permute<<<div_up(n, 256), 256, 0, s>>>(key, rank, dstarts, dperm, n, cells, status);
     k_fixup_cells<<<div_up(cells, 256), 256, 0, s>>>(dperm, dstarts, cells);
     VF_CHECK_LAUNCH();
     VF_TRY_CUDA(cudaMemcpyAsync(perm, dperm, (size_t)n * 4, cudaMemcpyDeviceToHost, s));

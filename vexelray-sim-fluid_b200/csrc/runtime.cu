@@ -165,6 +165,16 @@ extern "C" int32_t vf_version(void) { return 1; }
 
 extern "C" int32_t vf_device_ok(void) { return vf::require_device() == VF_OK ? 1 : 0; }
 
+extern "C" int32_t vf_binary_version(int32_t* out) {
+    VF_REQUIRE(out, VF_EINVAL, "null argument");
+    int32_t rc = vf::require_device();
+    if (rc) return rc;
+    cudaFuncAttributes attr{};
+    VF_TRY_CUDA(cudaFuncGetAttributes(&attr, vf::k_fill_f32));
+    *out = attr.binaryVersion;
+    return VF_OK;
+}
+
 extern "C" int32_t vf_set_device(int32_t device) {
     VF_TRY_CUDA(cudaSetDevice(device));
     return vf::require_device();

@@ -90,10 +90,15 @@ __global__ void __launch_bounds__(512) k_cell_scan(int* __restrict__ cell_count,
 }
 
 __global__ void k_permute(const int* __restrict__ key, const int* __restrict__ rank, const int* __restrict__ starts,
-                          int* __restrict__ perm, int n, uint32_t* status) {
+                          int* __restrict__ perm, int n, int64_t cells, uint32_t* status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int d = starts[key[i]] + rank[i];
+    const int k = key[i];
+    if (k < 0 || (int64_t)k >= cells) {
+        set_status(status, ST_OOB);
+        return;
+    }
+    int d = starts[k] + rank[i];
     if (d < 0 || d >= n) {
         set_status(status, ST_RANK);
         return;

@@ -117,7 +117,8 @@ __device__ __forceinline__ void insertion_sort_run(int* a, int n) {
 
 // perm[starts[key[i]] + rank[i]] = i.
 __global__ void k_permute(const int* __restrict__ key, const int* __restrict__ rank,
-                          const int* __restrict__ starts, int* __restrict__ perm, int n, uint32_t* status);
+                          const int* __restrict__ starts, int* __restrict__ perm, int n, int64_t cells,
+                          uint32_t* status);
 
 // Sorts each cell's run of perm ascending, one thread per cell (2D: cells small, runs short).
 __global__ void k_fixup_cells(int* __restrict__ perm, const int* __restrict__ starts, int64_t cells);
