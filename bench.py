@@ -405,11 +405,9 @@ def run_literal(args, vf):
         prof = sim.profile_read()
         sim.profile(False)
         touched = sim.touched_nodes()
-    pg = sum(prof.get(k, (0.0, 1))[0] for k in ("k_p2g3_tile", "k_g2p3_tile")) / steps
     return {"workload": "3D dam break, the config's literal box [0.05,0.45]x[0.05,0.65]x[0.05,0.45] at 8 per cell",
             "particles": np3, "steps": steps, "ms_per_step": ms / steps,
-            "particle_steps_per_s": np3 * steps / (ms / 1e3), "p2g_g2p_ms_per_step": pg,
-            "p2g_g2p_hbm_frac": (152.0 * np3 + 28.0 * touched) / (pg / 1e3) / 1e9 / measured_peaks()[0]}
+            "particle_steps_per_s": np3 * steps / (ms / 1e3), "roofline": roofline3(prof, steps, np3, touched)}
 
 
 def cpu_step_rate(x, y, z, m, params, budget_s=10.0, min_steps=10, max_steps=40, warmup=1):
@@ -573,19 +571,34 @@ def run_ours(args, dist: Dist):
 
 
 def roofline3(prof, steps, np3, touched):
-    """The P2G+G2P roofline from a profiled run: algorithmic bytes 152 Np + 28 N_t per step over the two kernels'
-    event-timed device time."""
-    t_p2g = prof.get("k_p2g3_tile", (0.0, 1))
-    t_g2p = prof.get("k_g2p3_tile", (0.0, 1))
-    per_step_ms = (t_p2g[0] + t_g2p[0]) / steps
-    alg_bytes = 152.0 * np3 + 28.0 * touched
-    achieved = alg_bytes / (per_step_ms / 1e3) / 1e9
+    """The roofline of the step's dominant kernel from a profiled run (CUDA events around every launch).
+
+    Fused step (the default): k_g2p2g3 gathers each particle from grid k and scatters it into grid k+1, so the
+    P2G+G2P pair is one kernel. Its algorithmic bytes a launch: read x, y, z, m, j (20 B) and write the 16 advected
+    fields (64 B) a particle, read grid k's four floats and write grid k+1's four floats a touched node (32 B):
+    84 Np + 32 N_t. `pair_target_ms` is the time the separate passes' bytes (152 Np + 28 N_t) take at 70% of the
+    peak: the north-star bar for P2G+G2P, which the fused kernel's time is compared with.
+    Separate passes: k_p2g3_tile + k_g2p3_tile at 152 Np + 28 N_t."""
     peak, peak_kind = measured_peaks()
-    tr_p2g, tr_g2p = profiled_traffic("k_p2g3_tile"), profiled_traffic("k_g2p3_tile")
-    traffic = (tr_p2g + tr_g2p) if (tr_p2g is not None and tr_g2p is not None) else None
-    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic, "kernel": "k_p2g3_tile + k_g2p3_tile", "peak_kind": peak_kind,
-            "algorithmic_bytes_per_step": alg_bytes, "touched_nodes": touched, "kernels_ms_per_step": round(per_step_ms, 4)}
+    sep_bytes = 152.0 * np3 + 28.0 * touched
+    if "k_g2p2g3" in prof:
+        t, n = prof["k_g2p2g3"]
+        per_ms = t / n
+        alg = 84.0 * np3 + 32.0 * touched
+        kernel, tr = "k_g2p2g3 (fused G2P of step k + P2G of step k+1)", profiled_traffic("k_g2p2g3")
+    else:
+        t_p2g = prof.get("k_p2g3_tile", (0.0, 1))
+        t_g2p = prof.get("k_g2p3_tile", (0.0, 1))
+        per_ms = (t_p2g[0] + t_g2p[0]) / steps
+        alg = sep_bytes
+        tr_p2g, tr_g2p = profiled_traffic("k_p2g3_tile"), profiled_traffic("k_g2p3_tile")
+        tr = (tr_p2g + tr_g2p) if (tr_p2g is not None and tr_g2p is not None) else None
+        kernel = "k_p2g3_tile + k_g2p3_tile"
+    achieved = alg / (per_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": tr, "kernel": kernel, "peak_kind": peak_kind,
+            "algorithmic_bytes": alg, "touched_nodes": touched, "pair_ms": round(per_ms, 4),
+            "pair_target_ms": round(sep_bytes / (0.7 * peak * 1e9) * 1e3, 4)}
 
 
 def run_variants(args, vf, sim):
@@ -594,9 +607,10 @@ def run_variants(args, vf, sim):
     stream = sim.stream()
     variants = {}
     names = {vf.VF_P2G_ATOMIC: "global_atomic", vf.VF_P2G_WARP: "warp_aggregated", vf.VF_P2G_TILE: "sorted_smem_tile",
-             vf.VF_P2G_FIXED: "exact_fixed_point"}
-    for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_FIXED, vf.VF_P2G_TILE):
-        sim.set_schedule(sched)
+             vf.VF_P2G_FIXED: "exact_fixed_point", -1: "sorted_smem_tile_fused"}
+    for sched in (vf.VF_P2G_ATOMIC, vf.VF_P2G_WARP, vf.VF_P2G_FIXED, vf.VF_P2G_TILE, -1):
+        sim.set_schedule(vf.VF_P2G_TILE if sched < 0 else sched)
+        sim.set_fused(sched < 0)
         sim.advance(2)
         sim.finish()
         sim.profile(True)
@@ -612,38 +626,45 @@ def run_variants(args, vf, sim):
             "p2g_ms_per_step": sum(vp[k][0] for k in p2g) / args.variant_steps,
             "kernels_ms_per_step": {k: v[0] / args.variant_steps for k, v in vp.items()}}
     sim.set_schedule(vf.VF_P2G_TILE)
+    sim.set_fused(True)
     return {"workload": WORKLOAD3, "steps": args.variant_steps, "schedules": variants}
 
 
 def run_swe(args, vf, dist, peak):
-    """Shallow water, 4096^2 HLL: cell-updates/s, the k_swe_tile roofline at 24 B a cell, the oracle on one core."""
+    """Shallow water, 4096^2 HLL: cell-updates/s and the tile kernel's roofline at 24 B a cell, in the exact
+    arithmetic (bit for bit the reference's) and in the fast mode; the oracle on one core as the CPU baseline."""
     h = swe_bumps()
     zero2 = np.zeros_like(h)
     ev0, ev1 = vf.Event(), vf.Event()
-    with vf.PatchSimulation(N_SWE, N_SWE) as p:
-        p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
-        p.write_budget(0, 2 ** 31 - 1)
-        p.dispatch(3)
-        p.read_budget(0)
-        k_swe = max(10, args.steps)
-        s_stream = p.stream()
-        ev0.record(s_stream)
-        p.dispatch(k_swe)
-        ev1.record(s_stream)
-        swe_ms = ev0.elapsed_ms(ev1)
-        p.profile(True)
-        p.dispatch(k_swe)
-        p.read_budget(0)
-        sp = p.profile_read()
-        p.profile(False)
     cells = N_SWE * N_SWE
-    k_ms = sp["k_swe_tile"][0] / sp["k_swe_tile"][1]
-    return {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)",
+    out = {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)"}
+    for exact in (True, False):
+        with vf.PatchSimulation(N_SWE, N_SWE) as p:
+            p.set_exact(exact)
+            p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
+            p.write_budget(0, 2 ** 31 - 1)
+            p.dispatch(3)
+            p.read_budget(0)
+            k_swe = max(10, args.steps)
+            s_stream = p.stream()
+            ev0.record(s_stream)
+            p.dispatch(k_swe)
+            ev1.record(s_stream)
+            swe_ms = ev0.elapsed_ms(ev1)
+            p.profile(True)
+            p.dispatch(k_swe)
+            p.read_budget(0)
+            sp = p.profile_read()
+            p.profile(False)
+        name = "k_swe_tile" if exact else "k_swe_tile_fast"
+        k_ms = sp[name][0] / sp[name][1]
+        achieved = 24.0 * cells / (k_ms / 1e3) / 1e9
+        out["exact" if exact else "fast"] = {
             "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
-            "roofline": {"bound": "hbm", "achieved": 24.0 * cells / (k_ms / 1e3) / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": 24.0 * cells / (k_ms / 1e3) / 1e9 / peak, "traffic": None,
-                         "kernel": "k_swe_tile", "bytes_per_cell": 24},
-            "cpu_baseline": None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)}
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": name, "bytes_per_cell": 24}}
+    out["cpu_baseline"] = None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)
+    return out
 
 
 CNN_FLOPS_PER_CELL = 2 * 25 * (3 * 32 + 32 * 32 + 32 * 6)   # 65.6 kFLOP: the three convolutions, algorithmic

@@ -296,6 +296,16 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
 void* vf_mpm3_stream(vf_mpm3* h);
 /* Change the scatter schedule (VF_P2G_*) between steps. */
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
+/* The fused step: with the sorted tiled schedule on dense storage without tension (the default there), a step is
+ * the sort and ONE kernel that gathers each particle's velocity and affine matrix from the last grid (Flip3.advect),
+ * moves it, and scatters its new state into the next grid (Flip3.scatter of the next step), so a particle's
+ * velocity and affine matrix are written once and not read back. The next step's scatter is then made at the end
+ * of this one; grid(), the snapshot and the device pointers still show the last step's grid, and anything that
+ * changes the particles, the params or the schedule discards the early scatter. on = 0 runs Flip3Step's passes
+ * one kernel each (the tiled scatter, then the tiled gather). No counterpart in the reference. */
+int32_t vf_mpm3_set_fused(vf_mpm3* h, int32_t on);
+/* 1 when the steps run fused. */
+int32_t vf_mpm3_fused(const vf_mpm3* h);
 /* The schedule the steps run (VF_P2G_AUTO resolved). */
 int32_t vf_mpm3_schedule(const vf_mpm3* h);
 /* The smallest positive mass of the last load (or restore), FLT_MAX if none: ParticleSimulation3's nominalMass
@@ -364,6 +374,14 @@ int32_t vf_swe_tile_width(const vf_swe* h);
  * previous step's last wave and wait on the device for its completion): 1 (the default) or 0 (plain stream
  * order). Bit-identical either way. */
 int32_t vf_swe_set_overlap(vf_swe* h, int32_t on);
+/* The step's arithmetic. on = 1 (the default): every operation rounded as the reference's strict f32 does, so
+ * the state, clock and clamp count equal the reference's CPU step bit for bit. on = 0: the fast mode, the same
+ * tile and flux form with fused multiply-adds, one approximate reciprocal of each cell's depth and of each face's
+ * wave span, and an approximate wave-speed square root: within a stated tolerance of the reference (about 1e-5
+ * relative per cell over tens of steps of smooth flow), the water moving only between neighbours as before. No
+ * counterpart in the reference, whose Vulkan path has no correctly rounded division either. */
+int32_t vf_swe_set_exact(vf_swe* h, int32_t on);
+int32_t vf_swe_exact(const vf_swe* h);
 /* A versioned binary snapshot of the patch (kind 2, the same 64-byte header with the edges in flags, 8 bits each):
  * the 16-word device block (speed words in their rotation, budget words, clamp count, params), clock, dispatch
  * count, steps and the last step's ticks (int64 each), then h, hu, hv. Resumes bit for bit, clock included.

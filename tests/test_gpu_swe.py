@@ -17,9 +17,10 @@ pytestmark = pytest.mark.gpu
 class GpuSweBackend:
     """PatchSimulation's raw rotation as a Stepper backend (Stepper.Gpu, Stepper.java:224-311)."""
 
-    def __init__(self, nx, ny, edges, tile_width=0):
+    def __init__(self, nx, ny, edges, tile_width=0, exact=True):
         self.p = vf.PatchSimulation(nx, ny, edges)
         self.p.set_tile_width(tile_width)
+        self.p.set_exact(exact)
         self.k = 0
 
     def load(self, h, hu, hv, params, first_speed):
@@ -237,3 +238,48 @@ def test_overlapped_and_stream_ordered_launches_agree_to_the_bit():
         for f in range(3):
             assert np.array_equal(out[0][0][f].view(np.int32), out[1][0][f].view(np.int32)), (width, f)
         assert out[0][1:] == out[1][1:], width
+
+
+# ---------------------------------------------------------------------------------- the fast mode
+# Tolerance (written here): after 1 and 60 steps of smooth flow every cell's h, hu and hv within
+# 2e-5 * max(1, |oracle|) of the exact arithmetic (the oracle), and the clock within one tick a step.
+
+
+def fast_backend(nx, ny, edges):
+    return GpuSweBackend(nx, ny, edges, exact=False)
+
+
+@pytest.mark.parametrize("nx,ny,edges", [(512, 384, (0, 0, 0, 0)), (300, 130, (0, 1, 1, 0))])
+def test_fast_mode_stays_within_its_tolerance_of_the_oracle(nx, ny, edges):
+    h = bumps(max(nx, ny), 3, count=10)[: nx * ny]
+    z = np.zeros(nx * ny, F)
+    params = swe_params(9.81, 0.45, 1, 1, 1e-6)
+    a = Stepper(OracleSweBackend(nx, ny, edges), nx, ny)
+    b = Stepper(fast_backend(nx, ny, edges), nx, ny)
+    for s in (a, b):
+        s.set(h, z, z, params, 1e9)
+    for steps in (1, 59):
+        a.step(steps)
+        b.step(steps)
+        sa, sb = a.read(), b.read()
+        for f in range(3):
+            e = sa[f].astype(np.float64)
+            err = np.abs(sb[f] - e)
+            assert np.all(err <= 2e-5 * np.maximum(1, np.abs(e))), (steps, f, float(err.max()))
+        assert abs(a.ticks() - b.ticks()) <= (1 if steps == 1 else 60), (a.ticks(), b.ticks())
+    assert not b.b.p.exact()
+
+
+def test_fast_mode_closed_box_holds_its_water():
+    """ShallowWaterTest.aClosedBoxHoldsItsWater (ShallowWaterTest.java:166-195) in the fast mode: the flux form
+    still moves water only between neighbours, so 300 steps keep the volume within 1e-5 and clamp nothing."""
+    check_closed_box_holds_its_water(fast_backend)
+
+
+def test_fast_mode_lake_at_rest_stays_at_rest():
+    check_lake_at_rest(fast_backend)
+
+
+def test_fast_mode_ritter_dam_break_converges():
+    coarse, fine = check_ritter_converges(fast_backend)
+    assert abs(coarse - 0.0128) < 0.002 and abs(fine - 0.0080) < 0.002

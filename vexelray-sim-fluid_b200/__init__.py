@@ -137,6 +137,8 @@ def lib() -> ctypes.CDLL:
         "vf_mpm3_pool_capacity": ([_vp], ctypes.c_int32),
         "vf_mpm3_set_graph": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_mpm3_schedule": ([_vp], ctypes.c_int32),
+        "vf_mpm3_set_fused": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_mpm3_fused": ([_vp], ctypes.c_int32),
         "vf_mpm3_nominal_mass": ([_vp, _f32p], ctypes.c_int32),
         "vf_mpm3_prepared_close": ([_vp], None),
         "vf_mpm3_create": ([_vp, ctypes.POINTER(_vp)], ctypes.c_int32),
@@ -228,6 +230,8 @@ def lib() -> ctypes.CDLL:
         "vf_swe_set_tile_width": ([_vp, ctypes.c_int32], ctypes.c_int32),
         "vf_swe_tile_width": ([_vp], ctypes.c_int32),
         "vf_swe_set_overlap": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_set_exact": ([_vp, ctypes.c_int32], ctypes.c_int32),
+        "vf_swe_exact": ([_vp], ctypes.c_int32),
         "vf_swe_snapshot": ([_vp, _vp, ctypes.c_int64, _i64p], ctypes.c_int32),
         "vf_swe_restore": ([_vp, _vp, ctypes.c_int64], ctypes.c_int32),
         "vf_swe_write_budget": ([_vp, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
@@ -949,6 +953,14 @@ class ParticleSimulation3:
         """The scatter schedule the steps run (VF_P2G_AUTO resolved for this size)."""
         return int(lib().vf_mpm3_schedule(self._h))
 
+    def set_fused(self, on: bool) -> None:
+        """The fused step (the gather and the next step's scatter in one kernel), the default where it applies;
+        off runs the separate tiled scatter and gather."""
+        check(lib().vf_mpm3_set_fused(self._h, 1 if on else 0))
+
+    def fused(self) -> bool:
+        return bool(lib().vf_mpm3_fused(self._h))
+
     def set_graph(self, on: bool) -> None:
         """advance() replays its steps two at a time from a captured CUDA graph (off by default)."""
         check(lib().vf_mpm3_set_graph(self._h, 1 if on else 0))
@@ -1171,6 +1183,14 @@ class PatchSimulation:
     def set_overlap(self, on: bool) -> None:
         """Steps launched as programmatic dependents of the previous step (default) or in plain stream order."""
         check(lib().vf_swe_set_overlap(self._h, 1 if on else 0))
+
+    def set_exact(self, on: bool) -> None:
+        """The reference's strict f32 arithmetic, bit for bit (default), or the fast mode (fused multiply-adds and
+        approximate reciprocals, within a stated tolerance)."""
+        check(lib().vf_swe_set_exact(self._h, 1 if on else 0))
+
+    def exact(self) -> bool:
+        return bool(lib().vf_swe_exact(self._h))
 
     def snapshot(self) -> bytes:
         """The patch's state as a versioned, checksummed blob (cells, speed and budget words, clock, steps)."""

@@ -71,6 +71,13 @@ struct vf_mpm3 {
     // windows of active[g]), 2 dense (memset)
     int grid_dirty[2] = {0, 0};
     bool counted = false;     // cell/brick counts and key/rank hold the current positions' keys
+    // The fused step (k_g2p2g3): the gather of step k and the scatter of step k+1 in one kernel. `fused` selects it
+    // (the default where it applies: the sorted tiled schedule, dense storage, no tension); `ahead` says the grid
+    // buffer grid_last holds the scatter of the CURRENT particles (the next step's), so readouts of the last step's
+    // grid look in the other buffer.
+    bool fused = false;
+    bool fuse_wanted = true;  // vf_mpm3_set_fused
+    bool ahead = false;
     bool sorted_valid = false;
     bool loaded = false;
     Profiler prof;
@@ -142,6 +149,21 @@ Step3 make_step(vf_mpm3* h) {
 }
 
 int persistent_blocks(int per_sm) { return sm_count() * per_sm; }
+
+bool fuse_applies(const vf_mpm3* h) { return h->p2g == VF_P2G_TILE && h->sort && !h->tension && !h->sparse; }
+
+// The grid buffer holding the last step's scatter (what grid(), the snapshot and the device pointers show).
+int ref_grid(const vf_mpm3* h) { return h->ahead ? h->grid_last ^ 1 : h->grid_last; }
+
+// Forgets a scatter made ahead for the current particles (before anything changes them, the params, the schedule,
+// or runs passes on its own): the buffer it went into is cleared densely before its next use.
+void drop_ahead(vf_mpm3* h) {
+    if (!h->ahead) return;
+    h->grid_dirty[h->grid_last] = 2;
+    h->grid_last ^= 1;
+    h->passes_run--;
+    h->ahead = false;
+}
 
 // VF_P2G_AUTO: the schedule measured fastest for the handle's size. Below about 600k particles the tiled scatter,
 // one warp per unit of 8x8x1 cells, leaves much of the GPU idle: the
@@ -339,10 +361,100 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
 uint64_t step_sig(const vf_mpm3* h) {
     return (uint64_t)h->cur | (uint64_t)h->counted << 1 | (uint64_t)(h->passes_run & 1) << 2 |
            (uint64_t)h->grid_dirty[0] << 3 | (uint64_t)h->grid_dirty[1] << 5 | (uint64_t)h->grid_last << 7 |
-           (uint64_t)h->p2g << 8 | (uint64_t)(h->fixed.ptr != nullptr) << 12 | 1ull << 63;
+           (uint64_t)h->p2g << 8 | (uint64_t)(h->fixed.ptr != nullptr) << 12 | (uint64_t)h->fused << 13 |
+           (uint64_t)h->ahead << 14 | 1ull << 63;
 }
 
 constexpr uint32_t STEP_PASSES = VF3_PASS_SORT | VF3_PASS_CLEAR | VF3_PASS_SCATTER | VF3_PASS_GRID | VF3_PASS_ADVECT;
+
+// The fused step's first scatter: the current particles sorted and scattered by the tiled schedule (which also
+// puts each cell's run in order), into the buffer the next scatter takes. Afterwards grid_last holds the scatter
+// of the current particles and the permutation is theirs.
+int32_t fused_prologue(vf_mpm3* h) {
+    const int g = (int)(h->passes_run & 1);
+    int32_t rc = run_sort(h, g, true, true);
+    if (rc) return rc;
+    Step3 s = make_step(h);
+    s.grid = h->grid[g].as<float4>();
+    s.active = h->active[g].as<int>();
+    s.n_active = h->n_active.as<int>() + g;
+    s.perm = h->perm.as<int>();
+    if (h->grid_dirty[g] == 2) VF_TRY_CUDA(cudaMemsetAsync(s.grid, 0, h->grid[g].bytes, h->stream));
+    h->grid_dirty[g] = 0;
+    h->prof.begin("k_p2g3_tile", h->stream);
+    const cudaError_t e = launch_p2g3_tile(persistent_blocks(2), s, h->stream);
+    h->prof.end(h->stream);
+    VF_TRY_CUDA(e);
+    h->grid_dirty[g] = 1;   // its footprint: the windows of active[g]
+    h->grid_last = g;
+    h->view_fresh = false;
+    h->fixed_valid = false;
+    h->passes_run++;
+    h->ahead = true;
+    return VF_OK;
+}
+
+// The sort of the current particles by the keys the last fused kernel counted, in fused mode: the brick list it
+// makes (active[grid_last]) is both the next fused kernel's work and the footprint of the scatter already in
+// grid[grid_last]. No stable fix-up: the fused kernel's sums are atomic, so the order within a cell does not matter.
+int32_t fused_sort(vf_mpm3* h) {
+    const int g = h->grid_last;
+    int* active = h->active[g].as<int>();
+    int* n_active = h->n_active.as<int>() + g;
+    VF_LAUNCH(h->prof, "k_brick_scan", h->stream, k_brick_scan, 1, 1024, 0, h->brick_count.as<int>(),
+              h->brick_start.as<int>(), active, n_active, h->nbricks);
+    VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(),
+              h->cell_start.as<int>(), h->cursor.as<int>(), h->brick_start.as<int>(), active, n_active);
+    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256), 256, 0, h->key.as<int>(),
+              h->cursor.as<int>(), h->perm.as<int>(), h->np, h->nkeys, h->status.as<uint32_t>());
+    h->counted = false;
+    h->sorted_valid = true;
+    return VF_OK;
+}
+
+// One fused step: [the prologue scatter, or the sort] then k_g2p2g3, which gathers from grid[grid_last], writes the
+// advected particles to their sorted slots in the other set, scatters them into the other grid buffer (cleared
+// here over its last footprint) and counts their keys.
+int32_t fused_step(vf_mpm3* h) {
+    int32_t rc = h->ahead ? fused_sort(h) : fused_prologue(h);
+    if (rc) return rc;
+    const int gi = h->grid_last, go = gi ^ 1;
+    Step3 s = make_step(h);
+    if (h->grid_dirty[go] == 1) {
+        s.grid = h->grid[go].as<float4>();
+        s.active = h->active[go].as<int>();
+        s.n_active = h->n_active.as<int>() + go;
+        VF_LAUNCH(h->prof, "k_clear_bricks3", h->stream, k_clear_bricks3, persistent_blocks(8), 256, 0, s);
+    } else if (h->grid_dirty[go] == 2) {
+        VF_TRY_CUDA(cudaMemsetAsync(h->grid[go].ptr, 0, h->grid[go].bytes, h->stream));
+    }
+    h->grid_dirty[go] = 0;
+    s.grid = h->grid[gi].as<float4>();
+    s.active = h->active[gi].as<int>();
+    s.n_active = h->n_active.as<int>() + gi;
+    s.perm = h->perm.as<int>();
+    s.out = h->part[h->cur ^ 1].as<float>();
+    s.count_next = 1;
+    h->prof.begin("k_g2p2g3", h->stream);
+    const cudaError_t e = launch_g2p2g3(persistent_blocks(2), s, h->grid[go].as<float4>(), h->stream);
+    h->prof.end(h->stream);
+    VF_TRY_CUDA(e);
+    h->cur ^= 1;
+    h->grid_last = go;
+    h->grid_dirty[go] = 1;   // its footprint list is made by the next fused sort, into active[go]
+    h->passes_run++;
+    h->counted = true;
+    h->view_fresh = false;
+    h->fixed_valid = false;
+    return VF_OK;
+}
+
+// One step of advance(): fused where it applies, else Flip3Step's passes.
+int32_t step_once(vf_mpm3* h) {
+    if (h->fused) return fused_step(h);
+    drop_ahead(h);
+    return run_passes(h, STEP_PASSES, h->sort);
+}
 
 // Two steps into h->pair by stream capture, then launched once. The host state the capture advanced is put back
 // if the capture fails, and the steps are left to run uncaptured.
@@ -354,8 +466,9 @@ int32_t capture_pair(vf_mpm3* h, uint64_t sig) {
         cudaGetLastError();
         return VF_ECUDA;
     }
-    int32_t rc = run_passes(h, STEP_PASSES, h->sort);
-    if (!rc) rc = run_passes(h, STEP_PASSES, h->sort);
+    const bool ahead = h->ahead;
+    int32_t rc = step_once(h);
+    if (!rc) rc = step_once(h);
     cudaGraph_t graph = nullptr;
     const cudaError_t end = cudaStreamEndCapture(h->stream, &graph);
     cudaGraphExec_t exec = nullptr;
@@ -375,6 +488,7 @@ int32_t capture_pair(vf_mpm3* h, uint64_t sig) {
     h->grid_dirty[0] = dirty0;
     h->grid_dirty[1] = dirty1;
     h->grid_last = last;
+    h->ahead = ahead;
     h->counted = counted;
     h->sorted_valid = sorted;
     h->view_fresh = fresh;
@@ -401,7 +515,7 @@ int32_t check_status(vf_mpm3* h) {
 // page into `view` (allocated on first use, unpacked once per scatter).
 int32_t last_grid(vf_mpm3* h, float4** out) {
     if (!h->sparse) {
-        *out = h->grid[h->grid_last].as<float4>();
+        *out = h->grid[ref_grid(h)].as<float4>();
         return VF_OK;
     }
     if (!h->view.ptr) {
@@ -511,6 +625,7 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
                       (rc = h->mark.alloc((size_t)h->npages * 4)) || (rc = h->n_used.alloc(2 * sizeof(int)))))
         return fail(rc);
     h->tension = (flags & VF_TENSION) != 0;
+    h->fused = fuse_applies(h);
     if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
                        (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);
@@ -596,6 +711,7 @@ int32_t vf_mpm3_create(vf_mpm3_prepared* p, vf_mpm3** out) {
 int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z, const float* u, const float* v,
                      const float* w, const float* m, const int32_t* params, int32_t nparams) {
     VF_REQUIRE(h && x && y && z && u && v && w && m, VF_EINVAL, "null argument");
+    drop_ahead(h);
     int32_t rc = upload_params(h, params, nparams);
     if (rc) return rc;
     float* base = h->part[h->cur].as<float>();
@@ -619,6 +735,7 @@ int32_t vf_mpm3_load(vf_mpm3* h, const float* x, const float* y, const float* z,
 
 int32_t vf_mpm3_params(vf_mpm3* h, const int32_t* params, int32_t nparams) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
+    drop_ahead(h);   // the scatter made ahead used the old params
     return upload_params(h, params, nparams);
 }
 
@@ -648,7 +765,7 @@ int32_t vf_mpm3_advance(vf_mpm3* h, int32_t count) {
                 h->use_graph = false;   // this handle's steps do not capture; they run as launches
             }
         }
-        int32_t rc = run_passes(h, STEP_PASSES, h->sort);
+        int32_t rc = step_once(h);
         if (rc) return rc;
         h->steps++;
         k++;
@@ -666,6 +783,7 @@ int32_t vf_mpm3_set_graph(vf_mpm3* h, int32_t on) {
 
 int32_t vf_mpm3_run(vf_mpm3* h, uint32_t passes) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
+    drop_ahead(h);
     int32_t rc = run_passes(h, passes, false);
     if (rc) return rc;
     return check_status(h);
@@ -688,7 +806,7 @@ int32_t vf_mpm3_read(vf_mpm3* h, int32_t field, float* out, int64_t n) {
                 s.grid = last;
                 s.vel = h->vel.as<float4>();
                 VF_LAUNCH(h->prof, "k_grid3_dense", h->stream, k_grid3_dense, div_up(h->nodes, 256), 256, 0, s);
-            } else if ((rc = grid_pass(h, s, h->grid_last))) {
+            } else if ((rc = grid_pass(h, s, ref_grid(h)))) {
                 return rc;
             }
             src = h->vel.as<float4>();
@@ -720,6 +838,7 @@ int32_t vf_mpm3_write(vf_mpm3* h, int32_t field, const float* in, int64_t n) {
     int32_t rc = field_pointer(h, field, &ptr, &len);
     if (rc) return rc;
     VF_REQUIRE(n == len, VF_EINVAL, "particle fields hold %lld floats, got %lld", (long long)len, (long long)n);
+    drop_ahead(h);
     VF_TRY_CUDA(cudaMemcpyAsync(ptr, in, (size_t)len * 4, cudaMemcpyHostToDevice, h->stream));
     if (field <= VF3_Z && h->counted) {
         rc = reset_counts(h);
@@ -798,9 +917,21 @@ int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule) {
         for (int g = 0; g < 2; g++)
             if (h->grid_dirty[g]) h->grid_dirty[g] = 2;
     }
+    drop_ahead(h);
     h->p2g = schedule;
+    h->fused = h->fuse_wanted && fuse_applies(h);
     return VF_OK;
 }
+
+int32_t vf_mpm3_set_fused(vf_mpm3* h, int32_t on) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    drop_ahead(h);
+    h->fuse_wanted = on != 0;
+    h->fused = h->fuse_wanted && fuse_applies(h);
+    return VF_OK;
+}
+
+int32_t vf_mpm3_fused(const vf_mpm3* h) { return h && h->fused ? 1 : 0; }
 
 int32_t vf_mpm3_schedule(const vf_mpm3* h) { return h ? h->p2g : -1; }
 
@@ -914,6 +1045,7 @@ int32_t vf_mpm3_restore(vf_mpm3* h, const void* buf, int64_t size) {
     SnapHeader got;
     int32_t rc = snap_check(buf, size, want, &got);
     if (rc) return rc;
+    drop_ahead(h);
     const char* body = static_cast<const char*>(buf) + sizeof(SnapHeader);
     int32_t words[SNAP3_WORDS];
     memcpy(words, body, sizeof words);

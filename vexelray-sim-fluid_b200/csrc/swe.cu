@@ -6,6 +6,13 @@
 // reference's strict f32 (Java) arithmetic does, so a step's output is bit-identical to the
 // reference's CPU semantics (and to the oracle), and so are the tick counts it derives.
 //
+// A second arithmetic, the fast mode (vf_swe_set_exact(h, 0)), keeps the tile and the flux form but rounds
+// differently: fused multiply-adds (written out as fmaf, since the file forbids contraction), one approximate
+// reciprocal of a cell's depth shared by its two velocities, one approximate reciprocal of each face's wave span
+// shared by its three fluxes, and an approximate square root for the wave speed. About a third of the exact
+// step's instructions; within a stated tolerance of the reference rather than equal to it, and the flux form
+// still moves water only between neighbours. The tick count from the previous step's speed stays IEEE.
+//
 // One CTA per 64 x 16 tile of cells:
 //   1. the tile and a one-cell halo of h, hu, hv land in shared memory by three 2D TMA loads
 //      (the box starts four cells left of the tile so its x coordinate is 16-byte aligned);
@@ -100,6 +107,36 @@ __device__ __forceinline__ Face hll(float g, float dry, float hL, float qnL, flo
 
 __device__ __forceinline__ float velocity(float h, float q, float dry) { return h > dry ? q / h : 0.0f; }
 
+// The fast mode's HLL: the same wave speeds and flux form as hll(), the division by the span done once as an
+// approximate reciprocal, and the products fused.
+__device__ __forceinline__ Face hll_fast(float g, float dry, float hL, float qnL, float qtL, float unL, float utL,
+                                         float cL, float hR, float qnR, float qtR, float unR, float utR, float cR) {
+    float sL = fminf(unL - cL, unR - cR);
+    float sR = fmaxf(unL + cL, unR + cR);
+    if (!(hR > dry)) {
+        sL = unL - cL;
+        sR = __fmaf_rn(2.0f, cL, unL);
+    }
+    if (!(hL > dry)) {
+        sL = __fmaf_rn(-2.0f, cR, unR);
+        sR = unR + cR;
+    }
+    const float lo = fminf(sL, 0.0f);
+    const float hi = fmaxf(sR, 0.0f);
+    const float inv = __fdividef(1.0f, fmaxf(hi - lo, 1e-30f));
+    const float lohi = lo * hi;
+    const float hg = 0.5f * g;
+    const float pL = hg * (hL * hL), pR = hg * (hR * hR);
+    Face f;
+    f.mass = __fmaf_rn(lohi, hR - hL, __fmaf_rn(hi, qnL, -lo * qnR)) * inv;
+    f.normal = __fmaf_rn(lohi, qnR - qnL, __fmaf_rn(hi, __fmaf_rn(qnL, unL, pL), -lo * __fmaf_rn(qnR, unR, pR))) * inv;
+    f.tangent = __fmaf_rn(lohi, qtR - qtL, __fmaf_rn(hi * qnL, utL, -(lo * qnR) * utR)) * inv;
+    return f;
+}
+
+// The fast mode's square root (approximate reciprocal square root; zero at zero).
+__device__ __forceinline__ float sqrt_fast(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
 __device__ __forceinline__ bool poll_barrier(uint32_t addr, int phase, int limit) {
     for (int it = 0; it < limit; it++) {
         uint32_t done;
@@ -125,7 +162,7 @@ __device__ __forceinline__ bool wait_barrier(unsigned long long* bar, int phase,
 
 // One tile (tx, ty) of one step. The CTA's mbarrier is initialised; `parity` is the phase its TMA completes.
 // Returns false (status set, nothing written) when the TMA did not land within the bounded wait.
-template <int TX_>
+template <int TX_, bool FAST>
 __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm_h, const CUtensorMap* tm_hu,
                                          const CUtensorMap* tm_hv, SweShared<TX_>& S, int tx, int ty, int parity) {
     using T = Tile<TX_>;
@@ -183,9 +220,16 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
     for (int i = tid; i < PY * PX; i += SWE_THREADS) {
         const int ly = i / PX, lx = i % PX;
         const float h = S.box[0][(ly) * HX + lx + 3];
-        S.pu[ly][lx] = velocity(h, S.box[1][(ly) * HX + lx + 3], dry);
-        S.pv[ly][lx] = velocity(h, S.box[2][(ly) * HX + lx + 3], dry);
-        S.pc[ly][lx] = sqrtf(g * h);
+        if constexpr (FAST) {
+            const float inv = h > dry ? __fdividef(1.0f, h) : 0.0f;
+            S.pu[ly][lx] = S.box[1][(ly) * HX + lx + 3] * inv;
+            S.pv[ly][lx] = S.box[2][(ly) * HX + lx + 3] * inv;
+            S.pc[ly][lx] = sqrt_fast(g * h);
+        } else {
+            S.pu[ly][lx] = velocity(h, S.box[1][(ly) * HX + lx + 3], dry);
+            S.pv[ly][lx] = velocity(h, S.box[2][(ly) * HX + lx + 3], dry);
+            S.pc[ly][lx] = sqrtf(g * h);
+        }
     }
     __syncthreads();
 
@@ -209,8 +253,10 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const float hL = S.box[0][(py) * HX + l + 3], hR = S.box[0][(py) * HX + r + 3];
         const float qnL = sgnL * S.box[1][(py) * HX + l + 3], qtL = S.box[2][(py) * HX + l + 3];
         const float qnR = sgnR * S.box[1][(py) * HX + r + 3], qtR = S.box[2][(py) * HX + r + 3];
-        const Face f = hll(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR, qtR,
-                           sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r]);
+        const Face f = FAST ? hll_fast(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR,
+                                       qtR, sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r])
+                            : hll(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR, qtR,
+                                  sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r]);
         S.fx[0][ly][lf] = f.mass;
         S.fx[1][ly][lf] = f.normal;
         S.fx[2][ly][lf] = f.tangent;
@@ -234,8 +280,10 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const float hB = S.box[0][(b) * HX + px + 3], hT = S.box[0][(t) * HX + px + 3];
         const float qnB = sgnB * S.box[2][(b) * HX + px + 3], qtB = S.box[1][(b) * HX + px + 3];
         const float qnT = sgnT * S.box[2][(t) * HX + px + 3], qtT = S.box[1][(t) * HX + px + 3];
-        const Face f = hll(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT, qtT,
-                           sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px]);
+        const Face f = FAST ? hll_fast(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT,
+                                       qtT, sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px])
+                            : hll(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT, qtT,
+                                  sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px]);
         S.fy[0][lf][lx] = f.mass;
         S.fy[1][lf][lx] = f.normal;
         S.fy[2][lf][lx] = f.tangent;
@@ -249,19 +297,30 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const int gx = x0 + lx, gy = y0 + ly;
         if (gx >= nx || gy >= ny) continue;
         const float h0 = S.box[0][(ly + 1) * HX + lx + 4], hu0 = S.box[1][(ly + 1) * HX + lx + 4], hv0 = S.box[2][(ly + 1) * HX + lx + 4];
-        const float h = (h0 - rx * (S.fx[0][ly][lx + 1] - S.fx[0][ly][lx])) - ry * (S.fy[0][ly + 1][lx] - S.fy[0][ly][lx]);
-        const float hu =
-            (hu0 - rx * (S.fx[1][ly][lx + 1] - S.fx[1][ly][lx])) - ry * (S.fy[2][ly + 1][lx] - S.fy[2][ly][lx]);
-        const float hv =
-            (hv0 - rx * (S.fx[2][ly][lx + 1] - S.fx[2][ly][lx])) - ry * (S.fy[1][ly + 1][lx] - S.fy[1][ly][lx]);
+        float h, hu, hv;
+        if constexpr (FAST) {
+            h = __fmaf_rn(-ry, S.fy[0][ly + 1][lx] - S.fy[0][ly][lx], __fmaf_rn(-rx, S.fx[0][ly][lx + 1] - S.fx[0][ly][lx], h0));
+            hu = __fmaf_rn(-ry, S.fy[2][ly + 1][lx] - S.fy[2][ly][lx], __fmaf_rn(-rx, S.fx[1][ly][lx + 1] - S.fx[1][ly][lx], hu0));
+            hv = __fmaf_rn(-ry, S.fy[1][ly + 1][lx] - S.fy[1][ly][lx], __fmaf_rn(-rx, S.fx[2][ly][lx + 1] - S.fx[2][ly][lx], hv0));
+        } else {
+            h = (h0 - rx * (S.fx[0][ly][lx + 1] - S.fx[0][ly][lx])) - ry * (S.fy[0][ly + 1][lx] - S.fy[0][ly][lx]);
+            hu = (hu0 - rx * (S.fx[1][ly][lx + 1] - S.fx[1][ly][lx])) - ry * (S.fy[2][ly + 1][lx] - S.fy[2][ly][lx]);
+            hv = (hv0 - rx * (S.fx[2][ly][lx + 1] - S.fx[2][ly][lx])) - ry * (S.fy[1][ly + 1][lx] - S.fy[1][ly][lx]);
+        }
         if (h < 0.0f) clamps++;
         const float nh = fmaxf(h, 0.0f);
         const int64_t c = (int64_t)gy * nx + gx;
         a.out[0][c] = nh;
         a.out[1][c] = hu;
         a.out[2][c] = hv;
-        const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
-        const float speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
+        float speed;
+        if constexpr (FAST) {
+            const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
+            speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
+        } else {
+            const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
+            speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
+        }
         best = max(best, __float_as_int(speed));
         if (c == 0) {
             *a.speed_clear = 0;
@@ -310,7 +369,7 @@ __device__ __forceinline__ void init_tile_barrier(SweShared<TX_>& S, bool tma) {
 // One step, one CTA per tile (grid = tiles). Launched as a programmatic dependent of the previous step: its CTAs
 // may become resident during that step's last wave, set up their barrier, and wait (griddepcontrol.wait: until
 // the previous grid has completed and its stores are visible) before reading anything the previous step wrote.
-template <int TX_>
+template <int TX_, bool FAST>
 __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
                                                           const __grid_constant__ CUtensorMap tm_hu,
                                                           const __grid_constant__ CUtensorMap tm_hv) {
@@ -318,7 +377,7 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
     SweShared<TX_>& S = swe_shared<TX_>();
     init_tile_barrier(S, a.use_tma);
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    swe_tile<TX_>(a, &tm_h, &tm_hu, &tm_hv, S, blockIdx.x, blockIdx.y, 0);
+    swe_tile<TX_, FAST>(a, &tm_h, &tm_hu, &tm_hv, S, blockIdx.x, blockIdx.y, 0);
 }
 
 // ------------------------------------------------------------------ diagnostics (Diagnostics.of)
@@ -473,6 +532,7 @@ struct vf_swe {
     bool tma = false;
     int tile_w = 64;             // the tile width the steps use
     bool pdl = true;             // steps launched as programmatic dependents of the previous step
+    bool exact = true;           // false: the fast mode's arithmetic (vf_swe_set_exact)
     // PatchSimulation.java:52-56
     int64_t clock_now = 0;
     int32_t clock_outstanding = 0;
@@ -536,8 +596,10 @@ int32_t dispatch(vf_swe* h) {
     attr[0].val.programmaticStreamSerializationAllowed = h->pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    h->prof.begin("k_swe_tile", h->stream);
-    const cudaError_t e = cudaLaunchKernelExC(&cfg, wide ? (const void*)k_swe_tile<64> : (const void*)k_swe_tile<32>, args);
+    const void* fn = h->exact ? (wide ? (const void*)k_swe_tile<64, false> : (const void*)k_swe_tile<32, false>)
+                              : (wide ? (const void*)k_swe_tile<64, true> : (const void*)k_swe_tile<32, true>);
+    h->prof.begin(h->exact ? "k_swe_tile" : "k_swe_tile_fast", h->stream);
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
     h->dispatched++;
@@ -625,9 +687,13 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
         return VF_ENOMEM;
     }
     for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status}) cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream);
-    if (cudaFuncSetAttribute(k_swe_tile<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_swe_tile<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
-        cudaFuncSetAttribute(k_swe_tile<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_swe_tile<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(SweShared<32>) + 128) != cudaSuccess ||
+        cudaFuncSetAttribute(k_swe_tile<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
+        cudaFuncSetAttribute(k_swe_tile<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(SweShared<32>) + 128) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared<64>));
@@ -832,6 +898,14 @@ int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
 }
 
 int32_t vf_swe_tile_width(const vf_swe* h) { return h ? h->tile_w : 0; }
+
+int32_t vf_swe_set_exact(vf_swe* h, int32_t on) {
+    VF_REQUIRE(h, VF_EINVAL, "null handle");
+    h->exact = on != 0;
+    return VF_OK;
+}
+
+int32_t vf_swe_exact(const vf_swe* h) { return h && h->exact ? 1 : 0; }
 
 int32_t vf_swe_set_overlap(vf_swe* h, int32_t on) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
