@@ -88,7 +88,7 @@ def dam3(box=BOX3):
     return x, y, z, m, (DT3, 0.0, g, 0.0, bulk, 1.0)
 
 
-def swe_bumps():
+def swe_bumps(n=N_SWE):
     """The shallow-water config: h = 1 + 16 seeded Gaussian bumps (amplitude U(0.1,0.5), sigma U(20,200)
     cells, centres uniform), hu = hv = 0."""
     n = N_SWE
@@ -468,9 +468,36 @@ def emit(name, result, detail):
         detail[name] = result
 
 
+def run_extras(args, vf, dist, sim=None):
+    """The sub-measurements asked for with --only, each one JSON line on stdout."""
+    detail = args.detail_store
+    if "variants" in args.extras and sim is not None:
+        emit("p2g_variants", run_variants(args, vf, sim), detail)
+    peak, _ = measured_peaks()
+    if "literal" in args.extras:
+        emit("literal_box", run_literal(args, vf), detail)
+    if "c0" in args.extras:
+        emit("c0_2d", run_c0(args, vf, dist), detail)
+    if "swe" in args.extras:
+        emit("swe", run_swe(args, vf, dist, peak), detail)
+    if "batch" in args.extras:
+        emit("batch", run_batch(args, vf, dist, peak), detail)
+    if "next" in args.extras:
+        emit("next_rows", run_next_rows(args, vf, peak, cpu=not args.no_cpu and dist.rank == 0), detail)
+    if "learned" in args.extras:
+        emit("learned", run_learned(args, vf), detail)
+    if "cnn" in args.extras:
+        emit("cnn", run_cnn(args, vf), detail)
+    if detail is not None and dist.rank == 0:
+        pathlib.Path(args.detail).write_text(json.dumps(detail, indent=1))
+
+
 def run_ours(args, dist: Dist):
     vf = package()
     vf.set_device(dist.local)
+    if args.no_headline:
+        run_extras(args, vf, dist)
+        return
     x, y, z, m, params = dam3()
     np3 = len(x)
     zeros = np.zeros(np3, np.float32)
@@ -524,26 +551,11 @@ def run_ours(args, dist: Dist):
     e2e = {"value": dist.sum(float(np3) * args.steps) / (e2e_ms / 1e3), "unit": "particle-steps/s",
            "h2d_bytes_per_step": 7 * np3 * 4 / args.steps, "d2h_bytes_per_step": 3 * np3 * 4 / args.steps,
            "job": f"load 7 fields + {args.steps} steps + read x,y,z"}
-    detail = {} if args.detail else None
     if "variants" in args.extras:
-        emit("p2g_variants", run_variants(args, vf, sim), detail)
+        run_extras(args, vf, dist, sim)
+        args.extras = args.extras - {"variants"}
     sim.close()
-
-    peak, _ = measured_peaks()
-    if "literal" in args.extras:
-        emit("literal_box", run_literal(args, vf), detail)
-    if "c0" in args.extras:
-        emit("c0_2d", run_c0(args, vf, dist), detail)
-    if "swe" in args.extras:
-        emit("swe", run_swe(args, vf, dist, peak), detail)
-    if "batch" in args.extras:
-        emit("batch", run_batch(args, vf, dist, peak), detail)
-    if "next" in args.extras:
-        emit("next_rows", run_next_rows(args, vf, peak, cpu=not args.no_cpu and dist.rank == 0), detail)
-    if "learned" in args.extras:
-        emit("learned", run_learned(args, vf), detail)
-    if detail is not None and dist.rank == 0:
-        pathlib.Path(args.detail).write_text(json.dumps(detail, indent=1))
+    run_extras(args, vf, dist)
 
     if dist.rank != 0:
         return
@@ -633,13 +645,14 @@ def run_variants(args, vf, sim):
 def run_swe(args, vf, dist, peak):
     """Shallow water, 4096^2 HLL: cell-updates/s and the tile kernel's roofline at 24 B a cell, in the exact
     arithmetic (bit for bit the reference's) and in the fast mode; the oracle on one core as the CPU baseline."""
-    h = swe_bumps()
+    h = swe_bumps(args.swe_n)
     zero2 = np.zeros_like(h)
     ev0, ev1 = vf.Event(), vf.Event()
-    cells = N_SWE * N_SWE
-    out = {"workload": "HLL shallow water 4096^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2)"}
+    n = args.swe_n
+    cells = n * n
+    out = {"workload": f"HLL shallow water {n}^2, dx=1, 16 seeded bumps, walls, C=0.45 (config 2 at 4096^2)"}
     for exact in (True, False):
-        with vf.PatchSimulation(N_SWE, N_SWE) as p:
+        with vf.PatchSimulation(n, n) as p:
             p.set_exact(exact)
             p.load(h, zero2, zero2, vf.swe_params(9.81, 0.45, 1.0, 1.0, 1e-6))
             p.write_budget(0, 2 ** 31 - 1)
@@ -663,7 +676,7 @@ def run_swe(args, vf, dist, peak):
             "steps": k_swe, "cell_updates_per_s": cells * k_swe / (swe_ms / 1e3), "ms_per_step": swe_ms / k_swe,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": name, "bytes_per_cell": 24}}
-    out["cpu_baseline"] = None if (args.no_cpu or dist.rank != 0) else cpu_swe_rate(h)
+    out["cpu_baseline"] = None if (args.no_cpu or dist.rank != 0 or n != N_SWE) else cpu_swe_rate(h)
     return out
 
 
@@ -917,6 +930,34 @@ def run_learned(args, vf):
     }
 
 
+def run_cnn(args, vf):
+    """The flux network alone: the committed network corrects a 1024^2 coarse patch (a restricted bump state)
+    three times; the per-kernel device times of the corrections and the convolutions' tensor roofline."""
+    from vexfluid import learned as L
+    net, report = L.trained()
+    try:
+        with vf.PatchSimulation(report["coarse"], report["coarse"]) as c:
+            h0 = L.restrict(L.bumps(3, report["fine"]))
+            z = np.zeros_like(h0)
+            c.load(h0.ravel(), z.ravel(), z.ravel(), L.coarse_params())
+            net.correct(c)
+            net.profile(True)
+            for _ in range(3):
+                net.correct(c)
+            prof = net.profile_read()
+            net.profile(False)
+    finally:
+        net.close()
+    conv_ms = sum(prof[k][0] / prof[k][1] for k in ("k_conv1", "k_conv2", "k_conv3"))
+    cells = report["coarse"] ** 2
+    tflops = CNN_FLOPS_PER_CELL * cells / (conv_ms / 1e3) / 1e12
+    tpeak, tkind = measured_tensor_peak()
+    return {"workload": f"flux network corrections of a {report['coarse']}^2 coarse patch",
+            "network_kernels_us": {k: 1e3 * v[0] / v[1] for k, v in prof.items()},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s",
+                         "frac": tflops / tpeak, "peak_kind": tkind, "flops_per_cell": CNN_FLOPS_PER_CELL}}
+
+
 def cpu_batch_rate(scenes, x, y, m, budget_s=10.0):
     """The oracle's 2D step, one scene after another on one host core, over the first scenes of the batch
     until the budget is spent: particle-steps/s."""
@@ -1006,7 +1047,7 @@ def run_batch(args, vf, dist: Dist, peak):
     return out
 
 
-EXTRAS = ("swe", "c0", "literal", "batch", "learned", "variants", "next")
+EXTRAS = ("swe", "c0", "literal", "batch", "learned", "cnn", "variants", "next")
 
 
 def main():
@@ -1020,7 +1061,10 @@ def main():
                     help="comma-separated sub-measurements to run before the headline: " + ",".join(EXTRAS) +
                          " (or 'all'); each prints one JSON line, the headline stays the last line")
     ap.add_argument("--detail", default=None, help="also write the sub-measurements to this JSON file")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="run only the --only sub-measurements (for profiling one of them), no headline line")
     ap.add_argument("--variant-steps", type=int, default=20)
+    ap.add_argument("--swe-n", type=int, default=N_SWE, help="the shallow-water sub-measurement's grid side")
     ap.add_argument("--learned-seeds", type=int, default=64, help="held-out seeds of the learned evaluation")
     ap.add_argument("--tune-cache", default=str(PKG / "batch2_tune.json"),
                     help="the batched step's autotune cache (JSON)")
@@ -1032,6 +1076,7 @@ def main():
     if unknown:
         ap.error(f"unknown sub-measurements: {sorted(unknown)}")
     args.extras = wanted
+    args.detail_store = {} if args.detail else None
     dist = Dist()
     try:
         if args.impl == "reference":

@@ -26,7 +26,8 @@ from typing import Sequence
 import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
-LIBRARY = HERE / "libvexfluid.so"
+# the in-tree build; VEXFLUID_LIBRARY names another build of the same library (a variant built for a comparison)
+LIBRARY = pathlib.Path(os.environ.get("VEXFLUID_LIBRARY", str(HERE / "libvexfluid.so")))
 
 VF_OK, VF_EINVAL, VF_ESTATE, VF_ENOMEM, VF_ECUDA, VF_ETIMEOUT, VF_ENODEV, VF_EDEVICE = 0, -1, -2, -3, -4, -5, -6, -7
 VF_EOS_TAIT = 1

@@ -433,7 +433,10 @@ __global__ void __launch_bounds__(FU_THREADS, 2) k_g2p2g3(Step3 s, float4* __res
     }
 }
 
-constexpr int FU_K = 4;   // particles a chunk
+#ifndef VF_FUSED_CHUNK
+#define VF_FUSED_CHUNK 4
+#endif
+constexpr int FU_K = VF_FUSED_CHUNK;   // particles a chunk (a build may choose another)
 
 cudaError_t launch_g2p2g3(int blocks, const Step3& s, float4* grid_out, cudaStream_t stream) {
     k_g2p2g3<FU_K><<<blocks, FU_THREADS, 0, stream>>>(s, grid_out);

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256) k_permute_cursor(const int* __restrict__ 
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     const int k = valid ? key[i] : 0;
-    const int d = warp_count(cursor, k, valid, nkeys, status);
+    const int d = warp_count_runs(cursor, k, valid, nkeys, status);
     if (!valid) return;
     if (d < 0 || d >= n) {
         set_status(status, ST_RANK);

@@ -40,6 +40,27 @@ __device__ __forceinline__ int warp_count(int* counts, int key, bool valid, int6
     return base + below;
 }
 
+// warp_count for keys that mostly come in runs (particles in slot order, sorted by the last step's keys): one
+// atomic per run of equal consecutive keys instead of a match over the warp. A key that appears in two runs of the
+// warp takes two atomics; the ranks are still distinct, and as provisional as warp_count's.
+__device__ __forceinline__ int warp_count_runs(int* counts, int key, bool valid, int64_t limit, uint32_t* status) {
+    const unsigned all = 0xffffffffu;
+    const int lane = lane_id();
+    const int k = valid ? key : -1;
+    const int prev = __shfl_up_sync(all, k, 1);
+    const unsigned starts = __ballot_sync(all, lane == 0 || prev != k);
+    const int leader = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // the run's first lane
+    const unsigned above = starts & ~(0xffffffffu >> (31 - lane));          // run starts after this lane
+    const int end = above ? __ffs(above) - 1 : 32;
+    int base = 0;
+    if (lane == leader && k >= 0) {
+        if ((int64_t)k < limit) base = atomicAdd(&counts[k], end - leader);
+        else set_status(status, ST_OOB);
+    }
+    base = __shfl_sync(all, base, leader);
+    return base + (lane - leader);
+}
+
 // Adds one to counts[key] for every valid lane, aggregated per distinct key; no rank.
 __device__ __forceinline__ void warp_tally(int* counts, int key, bool valid, int64_t limit, uint32_t* status) {
     const unsigned all = 0xffffffffu;
