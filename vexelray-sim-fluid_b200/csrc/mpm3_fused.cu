@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(FU_THREADS, 2) k_g2p2g3(Step3 s, float4* __res
         // 1. cell starts, clamped into the brick and made non-decreasing; chunks per cell
         const int64_t key0 = (int64_t)b * 512 + lz0 * 64;
         int v = s.cell_start[key0 + tid];
-        int vend = tid == FU_CELLS - 1 ? (lz0 + FU_UZ < BRICK ? s.cell_start[key0 + FU_CELLS] : be) : 0;
+        int vend = be;   // the unit's end: the next unit's first start, or the brick's end
+        if (tid == FU_CELLS - 1 && lz0 + FU_UZ < BRICK) vend = s.cell_start[key0 + FU_CELLS];
         if (v < bs || v > be || vend < bs || vend > be) {
             set_status(s.status, ST_OOB);
             v = min(max(v, bs), be);
