@@ -436,7 +436,7 @@ int32_t fused_step(vf_mpm3* h) {
     s.out = h->part[h->cur ^ 1].as<float>();
     s.count_next = 1;
     h->prof.begin("k_g2p2g3", h->stream);
-    const cudaError_t e = launch_g2p2g3(persistent_blocks(2), s, h->grid[go].as<float4>(), h->stream);
+    const cudaError_t e = launch_g2p2g3(persistent_blocks(fused_blocks_per_sm()), s, h->grid[go].as<float4>(), h->stream);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
     h->cur ^= 1;
@@ -629,6 +629,10 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
     if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
                        (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);
+    if (fused_prepare() != cudaSuccess) {
+        set_error("cannot give the fused step its shared memory");
+        return fail(VF_ECUDA);
+    }
     if (p2g_tile_prepare() != cudaSuccess) {
         set_error("cannot give the tiled scatter %zu bytes of shared memory", p2g_tile_smem());
         return fail(VF_ECUDA);

@@ -202,6 +202,8 @@ cudaError_t launch_p2g3_tile(int blocks, const Step3& s, cudaStream_t stream);
 // The fused step (mpm3_fused.cu): the gather from s.grid of the particles sorted by s.perm, written to their slots
 // in s.out, and their scatter into grid_out; 256 threads a CTA, two CTAs an SM, one CTA per half brick.
 cudaError_t launch_g2p2g3(int blocks, const Step3& s, float4* grid_out, cudaStream_t stream);
+cudaError_t fused_prepare();    // its shared-memory attribute
+int fused_blocks_per_sm();      // the CTAs an SM holds
 size_t p2g_tile_smem();
 cudaError_t p2g_tile_prepare();   // its shared-memory attribute
 __global__ void k_grid3_dense(Step3 s);
