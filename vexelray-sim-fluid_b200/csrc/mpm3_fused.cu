@@ -390,11 +390,14 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, (UZ == 4 ? 2 : 4)) k_g2p2g3(
                                 a23[ox] = __ffma2_rn(x2, q23, a23[ox]);
                             }
                         }
-                        __syncwarp();   // every lane on this row before any lane adds into the window
-                        if (nagg > 0) {
-                            float4* r3 = pwin + fu_node(lx, ly + oy, lz + oz);
+                        // one node at a time, every lane of the warp on the same node offset between barriers: lanes
+                        // hold different cells, so they add into different nodes, and no lane reads a node another
+                        // lane is still writing (a lane's next node may be its neighbour's current one)
+                        float4* r3 = pwin + fu_node(lx, ly + oy, lz + oz);
 #pragma unroll
-                            for (int ox = 0; ox < 3; ox++) {
+                        for (int ox = 0; ox < 3; ox++) {
+                            __syncwarp();
+                            if (nagg > 0) {
                                 float4 t = r3[ox];
                                 t.x += a01[ox].x;
                                 t.y += a01[ox].y;
