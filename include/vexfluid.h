@@ -296,13 +296,13 @@ int32_t vf_mpm3_device_ptr(vf_mpm3* h, const char* name, void** ptr, int32_t* st
 void* vf_mpm3_stream(vf_mpm3* h);
 /* Change the scatter schedule (VF_P2G_*) between steps. */
 int32_t vf_mpm3_set_p2g(vf_mpm3* h, int32_t schedule);
-/* The fused step: with the sorted tiled schedule on dense storage without tension (the default there), a step is
- * the sort and ONE kernel that gathers each particle's velocity and affine matrix from the last grid (Flip3.advect),
- * moves it, and scatters its new state into the next grid (Flip3.scatter of the next step), so a particle's
- * velocity and affine matrix are written once and not read back. The next step's scatter is then made at the end
- * of this one; grid(), the snapshot and the device pointers still show the last step's grid, and anything that
- * changes the particles, the params or the schedule discards the early scatter. on = 0 runs Flip3Step's passes
- * one kernel each (the tiled scatter, then the tiled gather). No counterpart in the reference. */
+/* The fused step, with the sorted tiled schedule on dense storage without tension: a step is the sort and ONE
+ * kernel that gathers each particle's velocity and affine matrix from the last grid (Flip3.advect), moves it, and
+ * scatters its new state into the next grid (Flip3.scatter of the next step), so a particle's velocity and affine
+ * matrix are written once and not read back. The next step's scatter is then made at the end of this one; grid(),
+ * the snapshot and the device pointers still show the last step's grid, and anything that changes the particles,
+ * the params or the schedule discards the early scatter. Off by default (on = 1 turns it on; 0 runs Flip3Step's
+ * passes, the tiled scatter and the tiled gather). No counterpart in the reference. */
 int32_t vf_mpm3_set_fused(vf_mpm3* h, int32_t on);
 /* 1 when the steps run fused. */
 int32_t vf_mpm3_fused(const vf_mpm3* h);

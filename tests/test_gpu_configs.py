@@ -58,11 +58,17 @@ def test_3d_configuration_sort_is_bit_exact():
 
 
 def test_3d_configuration_grid_and_positions_match_the_oracle():
+    """The separate tiled passes (the default) and the fused step."""
     x, y, z, m, params = dam3_tagged()
+    for fused in (False, True):
+        run_3d_configuration(x, y, z, m, params, fused)
+
+
+def run_3d_configuration(x, y, z, m, params, fused):
     n = bench.N3
     o = Flip3State(n, n, n, x, y, z, m)
     with vf.ParticleSimulation3(n, n, n, len(x)) as s:
-        assert s.fused()
+        s.set_fused(fused)
         s.load([x, y, z], [np.zeros_like(x)] * 3, m, vf.flip3_params(*params))
         s.advance(1)
         omp_step(o, params)

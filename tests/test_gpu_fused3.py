@@ -55,9 +55,11 @@ def check_positions(s, o, what):
         assert np.all(err <= 1e-4 * np.abs(e)), (what, key, float((err / np.abs(e)).max()))
 
 
-def test_fused_is_the_default_for_the_sorted_tile():
+def test_fused_is_an_option_of_the_sorted_tile():
     pos, vel, m, p = stirred(count=1000)
     with vf.ParticleSimulation3(40, 40, 40, len(m)) as s:
+        assert not s.fused()
+        s.set_fused(True)
         assert s.fused()
         s.set_fused(False)
         assert not s.fused()
@@ -72,6 +74,7 @@ def test_fused_scatter_matches_the_oracle_per_node(steps):
     pos, vel, m, p = stirred(n)
     o = Flip3State(n, n, n, *pos, m, u=vel[0], v=vel[1], w=vel[2])
     with vf.ParticleSimulation3(n, n, n, len(m)) as s:
+        s.set_fused(True)
         assert s.fused()
         s.load(list(pos), list(vel), m, vf.flip3_params(*p))
         s.advance(steps)
@@ -105,6 +108,7 @@ def test_calls_between_fused_steps_see_and_keep_the_reference_state():
     o = Flip3State(n, n, n, *pos, m, u=vel[0], v=vel[1], w=vel[2])
     p2 = (0.008, 0.0, -20.0, 0.0, 600.0, 1.0)
     with vf.ParticleSimulation3(n, n, n, len(m)) as s:
+        s.set_fused(True)
         s.load(list(pos), list(vel), m, vf.flip3_params(*p))
         s.advance(3)
         for _ in range(3):
@@ -134,6 +138,7 @@ def test_calls_between_fused_steps_see_and_keep_the_reference_state():
         blob = s.snapshot()
         s.advance(3)
         with vf.ParticleSimulation3(n, n, n, len(m)) as t:
+            t.set_fused(True)
             t.restore(blob)
             t.advance(3)
             a, b = s.positions(), t.positions()

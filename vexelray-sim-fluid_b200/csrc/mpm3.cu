@@ -72,11 +72,12 @@ struct vf_mpm3 {
     int grid_dirty[2] = {0, 0};
     bool counted = false;     // cell/brick counts and key/rank hold the current positions' keys
     // The fused step (k_g2p2g3): the gather of step k and the scatter of step k+1 in one kernel. `fused` selects it
-    // (the default where it applies: the sorted tiled schedule, dense storage, no tension); `ahead` says the grid
-    // buffer grid_last holds the scatter of the CURRENT particles (the next step's), so readouts of the last step's
-    // grid look in the other buffer.
+    // (vf_mpm3_set_fused, where it applies: the sorted tiled schedule, dense storage, no tension); `ahead` says the
+    // grid buffer grid_last holds the scatter of the CURRENT particles (the next step's), so readouts of the last
+    // step's grid look in the other buffer. Off by default: at the 3D configuration it measured no faster than the
+    // separate tiled passes.
     bool fused = false;
-    bool fuse_wanted = true;  // vf_mpm3_set_fused
+    bool fuse_wanted = false;
     bool ahead = false;
     bool sorted_valid = false;
     bool loaded = false;
@@ -625,7 +626,7 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
                       (rc = h->mark.alloc((size_t)h->npages * 4)) || (rc = h->n_used.alloc(2 * sizeof(int)))))
         return fail(rc);
     h->tension = (flags & VF_TENSION) != 0;
-    h->fused = fuse_applies(h);
+    h->fused = h->fuse_wanted && fuse_applies(h);
     if (h->tension && ((rc = h->colour[0].alloc((size_t)h->nodes * 4)) || (rc = h->colour[1].alloc((size_t)h->nodes * 4)) ||
                        (rc = h->stress.alloc((size_t)6 * h->nodes * 4))))
         return fail(rc);

@@ -133,15 +133,8 @@ __device__ __forceinline__ void scatter_one(const P2GState& q, float4* grid, con
 }
 
 
-#ifndef VF_FUSED_MINB
-#define VF_FUSED_MINB 0
-#endif
-// CTAs an SM: as many as the shared memory allows (two of 8 x 8 x 4 cells, four of 8 x 8 x 2), or a build's choice
-template <int UZ>
-constexpr int fused_minb() { return VF_FUSED_MINB > 0 ? VF_FUSED_MINB : (UZ == 4 ? 2 : 4); }
-
 template <int UZ, int K>
-__global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(Step3 s, float4* __restrict__ grid_out) {
+__global__ void __launch_bounds__(FusedUnit<UZ>::T, (UZ == 4 ? 2 : 4)) k_g2p2g3(Step3 s, float4* __restrict__ grid_out) {
     using Unit = FusedUnit<UZ>;
     constexpr int T = Unit::T, NW = Unit::NW, CELLS = Unit::CELLS, WN = Unit::WN, CAP = Unit::CAP;
     extern __shared__ __align__(16) float4 fu_smem[];
@@ -208,36 +201,32 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
         }
         for (int i = tid; i < NW * WN; i += T) pwin_all[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         int stayed = 0;   // this thread's particles that stayed in their cell
-        // 3. the chunks, round by round: round r holds chunk r of every cell that has one, in cell order, and a warp
-        // takes 32 consecutive chunks at once. Within a round they belong to 32 different cells, so at one stencil
-        // offset the lanes add into 32 different nodes of the warp's own window (plain loads and stores, no
-        // atomics); where a pass reaches across two rounds and holds a cell twice, the lanes holding it add in turn.
+        // 3. the chunks, round by round: round r holds chunk r of every cell that has one, so the 32 chunks a warp
+        // takes at once (rounds padded to whole warps) belong to 32 different cells, and at one stencil offset the
+        // lanes add into 32 different nodes of the warp's own window: plain loads and stores, no atomics
         for (int r0 = 0; r0 < rounds;) {
             int filled = 0, r = r0;
             while (r < rounds) {
                 const int flag = nch > r ? 1 : 0;
                 int cnt;
                 const int at = fu_scan<NW, false>(flag, tmp, &cnt) - flag;
-                if (filled + cnt > CAP) break;   // CTA-uniform; a round always fits an empty list
+                const int padded = (cnt + 31) & ~31;
+                if (filled + padded > CAP) break;   // CTA-uniform; a round always fits an empty list
                 if (flag) list[filled + at] = tid | (r << 16);
-                filled += cnt;
+                if (tid < padded - cnt) list[filled + cnt + tid] = -1;
+                filled += padded;
                 r++;
             }
             __syncthreads();
-            for (int pass = warp; pass * 32 < filled; pass += NW) {
-                const int slot = pass * 32 + lane;
-                const int entry = slot < filled ? list[slot] : -1;
+            for (int pass = warp; pass < filled / 32; pass += NW) {
+                const int entry = list[pass * 32 + lane];
                 const int c = entry >= 0 ? (entry & 0xffff) : 0;
                 const int p0 = entry >= 0 ? cs[c] + (entry >> 16) * K : 0;
                 const int len = entry >= 0 ? min(K, cs[c + 1] - p0) : 0;
-                // lanes holding the same cell add into the window in turn (rank 0 first)
-                const unsigned peers = __match_any_sync(0xffffffffu, entry >= 0 ? c : -1 - lane);
-                const int rank = __popc(peers & ((1u << lane) - 1u));
-                const int turns = __reduce_max_sync(0xffffffffu, (unsigned)rank) + 1;
                 const int lx = c & 7, ly = (c >> 3) & 7, lz = c >> 6;
                 const int gcx = cx0 + lx, gcy = cy0 + ly, gcz = cz0 + lz;   // the cell: the chunk's stencil base
                 int src[K];
-                float pos[K][3], pm[K], pj[K];
+                float px[K], py[K], pz[K], pm[K], pj[K];
 #pragma unroll
                 for (int i = 0; i < K; i++) {
                     src[i] = -1;
@@ -248,70 +237,11 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
                             sv = 0;
                         }
                         src[i] = sv;
-                        pos[i][0] = in[X * st + sv];
-                        pos[i][1] = in[Y * st + sv];
-                        pos[i][2] = in[Z * st + sv];
+                        px[i] = in[X * st + sv];
+                        py[i] = in[Y * st + sv];
+                        pz[i] = in[Z * st + sv];
                         pm[i] = in[M * st + sv];
                         pj[i] = in[J * st + sv];
-                    }
-                }
-                // the chunk's particles in their cell: stencil offsets and weights; the others keep their state
-                bool live[K];
-                float f[K][3], w[K][3][3];
-#pragma unroll
-                for (int i = 0; i < K; i++) {
-                    live[i] = false;
-                    if (i >= len) continue;
-                    int cl[3];
-#pragma unroll
-                    for (int e = 0; e < 3; e++) {
-                        stencil_axis(pos[i][e], size[e], cl[e], f[i][e]);
-                        bspline_weights(f[i][e], w[i][e]);
-                    }
-                    const bool mine = cl[0] == gcx && cl[1] == gcy && cl[2] == gcz;
-                    live[i] = pm[i] > 0.0f && mine;
-                    if (!live[i]) {
-                        // Flip3.advect skips a particle without mass (Flip3.java:342) and so does the scatter; a
-                        // particle outside its sorted cell is a sort fault. Either keeps its state.
-                        if (pm[i] > 0.0f) set_status(s.status, ST_OOB);
-                        const int d = p0 + i;
-                        for (int fld = 0; fld < NF3; fld++) out[fld * st + d] = in[fld * st + src[i]];
-                        const int key = key3_of(pos[i][0], pos[i][1], pos[i][2], dm);
-                        s.key[d] = key;
-                        tally_one(s, key);
-                    }
-                }
-                // the gather, regrouped per row of three nodes along x; a row's nodes are loaded once for the
-                // chunk's particles, which share the cell
-                float vel[K][3], Sg[K][3][3];
-#pragma unroll
-                for (int i = 0; i < K; i++)
-#pragma unroll
-                    for (int a = 0; a < 3; a++) {
-                        vel[i][a] = 0.0f;
-                        Sg[i][a][0] = Sg[i][a][1] = Sg[i][a][2] = 0.0f;
-                    }
-#pragma unroll
-                for (int oz = 0; oz < 3; oz++) {
-#pragma unroll
-                    for (int oy = 0; oy < 3; oy++) {
-                        const int w0 = fu_node(lx, ly + oy, lz + oz);
-                        const float4 n0 = vwin[w0], n1 = vwin[w0 + 1], n2 = vwin[w0 + 2];
-                        const float v0[3] = {n0.x, n0.y, n0.z}, v1[3] = {n1.x, n1.y, n1.z}, v2[3] = {n2.x, n2.y, n2.z};
-#pragma unroll
-                        for (int i = 0; i < K; i++) {
-                            const float wyz = w[i][1][oy] * w[i][2][oz];
-                            const float wx2x2 = 2.0f * w[i][0][2];
-#pragma unroll
-                            for (int a = 0; a < 3; a++) {
-                                const float r0v = w[i][0][0] * v0[a] + w[i][0][1] * v1[a] + w[i][0][2] * v2[a];
-                                const float rx = w[i][0][1] * v1[a] + wx2x2 * v2[a];
-                                vel[i][a] += wyz * r0v;
-                                Sg[i][a][0] += wyz * rx;
-                                if (oy) Sg[i][a][1] += ((float)oy * wyz) * r0v;
-                                if (oz) Sg[i][a][2] += ((float)oz * wyz) * r0v;
-                            }
-                        }
                     }
                 }
                 P2GState ps[K];
@@ -320,27 +250,71 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
 #pragma unroll
                 for (int i = 0; i < K; i++) {
                     agg[i] = false;
-                    if (!live[i]) continue;
+                    if (i >= len) continue;
                     const int d = p0 + i;
+                    const float at3[3] = {px[i], py[i], pz[i]};
+                    int cl[3];
+                    float f[3];
+                    stencil_axis(at3[0], dm.nx, cl[0], f[0]);
+                    stencil_axis(at3[1], dm.ny, cl[1], f[1]);
+                    stencil_axis(at3[2], dm.nz, cl[2], f[2]);
+                    const bool mine = cl[0] == gcx && cl[1] == gcy && cl[2] == gcz;
+                    if (!(pm[i] > 0.0f) || !mine) {
+                        // Flip3.advect skips a particle without mass (Flip3.java:342) and so does the scatter; a
+                        // particle outside its sorted cell is a sort fault. Either keeps its state.
+                        if (pm[i] > 0.0f) set_status(s.status, ST_OOB);
+                        for (int fld = 0; fld < NF3; fld++) out[fld * st + d] = in[fld * st + src[i]];
+                        const int key = key3_of(at3[0], at3[1], at3[2], dm);
+                        s.key[d] = key;
+                        tally_one(s, key);
+                        continue;
+                    }
+                    // the gather from the velocity window, regrouped per row of three nodes along x
+                    float wx[3], wy[3], wz[3];
+                    bspline_weights(f[0], wx);
+                    bspline_weights(f[1], wy);
+                    bspline_weights(f[2], wz);
+                    const float wx2x2 = 2.0f * wx[2];
+                    float vel[3] = {0, 0, 0}, Sg[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+                    for (int oz = 0; oz < 3; oz++) {
+#pragma unroll
+                        for (int oy = 0; oy < 3; oy++) {
+                            const int w0 = fu_node(lx, ly + oy, lz + oz);
+                            const float4 n0 = vwin[w0], n1 = vwin[w0 + 1], n2 = vwin[w0 + 2];
+                            const float wyz = wy[oy] * wz[oz];
+                            const float v0[3] = {n0.x, n0.y, n0.z}, v1[3] = {n1.x, n1.y, n1.z},
+                                        v2[3] = {n2.x, n2.y, n2.z};
+#pragma unroll
+                            for (int a = 0; a < 3; a++) {
+                                const float r0v = wx[0] * v0[a] + wx[1] * v1[a] + wx[2] * v2[a];
+                                const float rx = wx[1] * v1[a] + wx2x2 * v2[a];
+                                vel[a] += wyz * r0v;
+                                Sg[a][0] += wyz * rx;
+                                if (oy) Sg[a][1] += ((float)oy * wyz) * r0v;
+                                if (oz) Sg[a][2] += ((float)oz * wyz) * r0v;
+                            }
+                        }
+                    }
                     float cm[9];
 #pragma unroll
                     for (int a = 0; a < 3; a++)
 #pragma unroll
-                        for (int e = 0; e < 3; e++) cm[3 * a + e] = 4.0f * (Sg[i][a][e] - f[i][e] * vel[i][a]);
-                    float np3[3], nv[3] = {vel[i][0], vel[i][1], vel[i][2]};
+                        for (int e = 0; e < 3; e++) cm[3 * a + e] = 4.0f * (Sg[a][e] - f[e] * vel[a]);
+                    float pos[3];
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        np3[a] = pos[i][a] + p.dt * nv[a];
-                        keep_inside(np3[a], nv[a], size[a]);
+                        pos[a] = at3[a] + p.dt * vel[a];
+                        keep_inside(pos[a], vel[a], size[a]);
                     }
                     float jn = pj[i] * (1.0f + p.dt * (cm[0] + (cm[4] + cm[8])));
                     jn = clampf(jn, 1.0f / J_BOUND3, J_BOUND3);
-                    out[X * st + d] = np3[0];
-                    out[Y * st + d] = np3[1];
-                    out[Z * st + d] = np3[2];
-                    out[U * st + d] = nv[0];
-                    out[V * st + d] = nv[1];
-                    out[W * st + d] = nv[2];
+                    out[X * st + d] = pos[0];
+                    out[Y * st + d] = pos[1];
+                    out[Z * st + d] = pos[2];
+                    out[U * st + d] = vel[0];
+                    out[V * st + d] = vel[1];
+                    out[W * st + d] = vel[2];
                     out[M * st + d] = pm[i];
                     out[J * st + d] = jn;
 #pragma unroll
@@ -348,9 +322,9 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
                     // the next step's scatter of the new state
                     int ncl[3];
                     float nf[3];
-                    stencil_axis(np3[0], dm.nx, ncl[0], nf[0]);
-                    stencil_axis(np3[1], dm.ny, ncl[1], nf[1]);
-                    stencil_axis(np3[2], dm.nz, ncl[2], nf[2]);
+                    stencil_axis(pos[0], dm.nx, ncl[0], nf[0]);
+                    stencil_axis(pos[1], dm.ny, ncl[1], nf[1]);
+                    stencil_axis(pos[2], dm.nz, ncl[2], nf[2]);
                     float jp;
                     if (p.tait) {
                         const float rj = __frcp_rn(jn), r2 = rj * rj;
@@ -359,7 +333,7 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
                         jp = p.bulk * (1.0f - jn);
                     }
                     const float sp = (k4dt * (pm[i] * vol)) * jp;
-                    p2g_state(ps[i], nf, pm[i], nv, cm, sp);
+                    p2g_state(ps[i], nf, pm[i], vel, cm, sp);
                     const int key = key3_of_cell(ncl[0], ncl[1], ncl[2], dm);
                     s.key[d] = key;
                     if (ncl[0] == gcx && ncl[1] == gcy && ncl[2] == gcz) {
@@ -372,9 +346,8 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
                     }
                 }
                 // the chunk's particles that stayed: their 27 nodes' amounts summed here ((mass, x-momentum) and
-                // (y-, z-momentum) in paired fp32), then added into the warp's window a node at a time, every lane
-                // of the warp on the same node offset between barriers (lanes of one turn hold different cells, so
-                // they add into different nodes, and no lane reads a node another is still writing)
+                // (y-, z-momentum) in paired fp32), then added into the warp's window, a row of three nodes at a
+                // time with every lane of the warp on the same row
 #pragma unroll
                 for (int oz = 0; oz < 3; oz++) {
 #pragma unroll
@@ -417,19 +390,20 @@ __global__ void __launch_bounds__(FusedUnit<UZ>::T, fused_minb<UZ>()) k_g2p2g3(S
                                 a23[ox] = __ffma2_rn(x2, q23, a23[ox]);
                             }
                         }
+                        // one node at a time, every lane of the warp on the same node offset between barriers: lanes
+                        // hold different cells, so they add into different nodes, and no lane reads a node another
+                        // lane is still writing (a lane's next node may be its neighbour's current one)
                         float4* r3 = pwin + fu_node(lx, ly + oy, lz + oz);
-                        for (int turn = 0; turn < turns; turn++) {
 #pragma unroll
-                            for (int ox = 0; ox < 3; ox++) {
-                                __syncwarp();
-                                if (nagg > 0 && rank == turn) {
-                                    float4 t = r3[ox];
-                                    t.x += a01[ox].x;
-                                    t.y += a01[ox].y;
-                                    t.z += a23[ox].x;
-                                    t.w += a23[ox].y;
-                                    r3[ox] = t;
-                                }
+                        for (int ox = 0; ox < 3; ox++) {
+                            __syncwarp();
+                            if (nagg > 0) {
+                                float4 t = r3[ox];
+                                t.x += a01[ox].x;
+                                t.y += a01[ox].y;
+                                t.z += a23[ox].x;
+                                t.w += a23[ox].y;
+                                r3[ox] = t;
                             }
                         }
                     }
@@ -487,7 +461,7 @@ cudaError_t fused_prepare() {
                                 (int)FusedUnit<FU_UZ>::SMEM);
 }
 
-int fused_blocks_per_sm() { return fused_minb<FU_UZ>(); }
+int fused_blocks_per_sm() { return FU_UZ == 4 ? 2 : 4; }
 
 cudaError_t launch_g2p2g3(int blocks, const Step3& s, float4* grid_out, cudaStream_t stream) {
     k_g2p2g3<FU_UZ, FU_K><<<blocks, FusedUnit<FU_UZ>::T, FusedUnit<FU_UZ>::SMEM, stream>>>(s, grid_out);
