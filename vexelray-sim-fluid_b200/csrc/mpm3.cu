@@ -302,7 +302,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
     if (mask & VF3_PASS_SCATTER) {
         if (tile) {
             h->prof.begin("k_p2g3_tile", h->stream);
-            const cudaError_t e = launch_p2g3_tile(persistent_blocks(p2g_tile_blocks_per_sm()), s, h->stream);
+            const cudaError_t e = launch_p2g3_tile(persistent_blocks(2), s, h->stream);
             h->prof.end(h->stream);
             VF_TRY_CUDA(e);
         } else if (h->p2g == VF_P2G_WARP) {
@@ -383,7 +383,7 @@ int32_t fused_prologue(vf_mpm3* h) {
     if (h->grid_dirty[g] == 2) VF_TRY_CUDA(cudaMemsetAsync(s.grid, 0, h->grid[g].bytes, h->stream));
     h->grid_dirty[g] = 0;
     h->prof.begin("k_p2g3_tile", h->stream);
-    const cudaError_t e = launch_p2g3_tile(persistent_blocks(p2g_tile_blocks_per_sm()), s, h->stream);
+    const cudaError_t e = launch_p2g3_tile(persistent_blocks(2), s, h->stream);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
     h->grid_dirty[g] = 1;   // its footprint: the windows of active[g]

@@ -1,7 +1,5 @@
 // mpm3_kernels.cu -- kernels of the 3D MLS-MPM/APIC step. See mpm3_kernels.cuh for the layout.
 // Reference: vexelray-sim-fluid-core/src/main/java/dev/vexelray/sim/fluid/particle/Flip3.java.
-#include <type_traits>
-
 #include "mpm3_kernels.cuh"
 
 namespace vf {
@@ -541,297 +539,17 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
     }
 }
 
-// The fields one half of the split scatter reads: position, mass and J, and the velocity and affine rows of its
-// momentum components (x; or y and z).
-template <int HALF>
-__device__ __forceinline__ void load_pin_half(PIn& q, const float* __restrict__ in, int64_t st, int src) {
-    const float* b = in + src;
-    q.x = b[X * st];
-    q.y = b[Y * st];
-    q.z = b[Z * st];
-    q.m = b[M * st];
-    q.j = b[J * st];
-    if (HALF == 0) {
-        q.u = b[U * st];
-#pragma unroll
-        for (int a = 0; a < 3; a++) q.c[a] = b[(C00 + a) * st];
-    } else {
-        q.v = b[V * st];
-        q.w = b[W * st];
-#pragma unroll
-        for (int a = 3; a < 9; a++) q.c[a] = b[(C00 + a) * st];
-    }
-}
-
-#ifndef VF_P2G_SPLIT_CTAS
-#define VF_P2G_SPLIT_CTAS 4
-#endif
-template <int UZ>
-__global__ void __launch_bounds__(P2G_THREADS, VF_P2G_SPLIT_CTAS) k_p2g3_tile_split(Step3 s) {
-    constexpr int UCELLS = P2GUnit<UZ>::UCELLS, UPB = P2GUnit<UZ>::UPB, WW = P2GUnit<UZ>::WW;
-    extern __shared__ __align__(16) unsigned char p2g_raw[];
-    P2GShared<UZ>& S = *reinterpret_cast<P2GShared<UZ>*>(p2g_raw);
-    const Params3 p = *s.params;
-    const float vol = __fdiv_rn(1.0f, p.rho0);                 // V0 = m / rho0 as m * (1/rho0)
-    const float k4dt = 4.0f * p.dt;
-    const Dims3 dm = s.d;
-    const int64_t st = s.stride;
-    const float* __restrict__ in = s.in;
-    int* __restrict__ perm = s.perm;
-    const unsigned ALL = 0xffffffffu;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float4* ww = S.wwin[warp];
-    int* cstart = S.start[warp];
-    unsigned char* order = S.order[warp];
-    int* bucket = S.bucket[warp];
-    const int units = *s.n_active * UPB;
-    const int total_warps = gridDim.x * P2G_WARPS;
-    for (int u = blockIdx.x * P2G_WARPS + warp; u < units; u += total_warps) {
-        const int b = s.active[u / UPB], lz0 = (u % UPB) * UZ;
-        const int bx = b % dm.nbx, by = (b / dm.nbx) % dm.nby, bz = b / (dm.nbx * dm.nby);
-        const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK + lz0;
-        int bs = s.brick_start[b], be = s.brick_start[b + 1];
-        if (bs < 0 || be > s.np || be < bs) {
-            set_status(s.status, ST_OOB);
-            bs = max(bs, 0);
-            be = min(max(be, bs), s.np);
-        }
-        // the unit's cell starts (clamped into the brick and made non-decreasing)
-        const int64_t key0 = (int64_t)b * 512 + lz0 * 64;
-        for (int c = lane; c <= UCELLS; c += 32) {
-            int v = (c < UCELLS || lz0 + UZ < BRICK) ? s.cell_start[key0 + c] : be;
-            if (v < bs || v > be) {
-                set_status(s.status, ST_OOB);
-                v = min(max(v, bs), be);
-            }
-            cstart[c] = v;
-        }
-        __syncwarp();
-        // a prefix maximum keeps the runs ordered even if the starts were not
-        int carry = bs;
-        for (int c0 = 0; c0 <= UCELLS; c0 += 32) {
-            const int c = c0 + lane;
-            int v = c <= UCELLS ? cstart[c] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(ALL, v, o);
-                if (lane >= o) v = max(v, y);
-            }
-            v = max(v, carry);
-            if (c <= UCELLS) cstart[c] = v;
-            carry = __shfl_sync(ALL, v, 31);
-        }
-        __syncwarp();
-        const int S0 = cstart[0], S1 = cstart[UCELLS];
-        if (S1 == S0) continue;   // an empty unit (warp-uniform)
-
-        // 1. the unit's range staged, each cell's run sorted there, written back
-        const bool staged = S1 - S0 <= RUN_CAP;
-        int* rs = S.run[warp];
-        if (staged) {
-            for (int j = S0 + lane; j < S1; j += 32) rs[j - S0] = perm[j];
-            __syncwarp();
-            for (int c = lane; c < UCELLS; c += 32)
-                if (cstart[c + 1] - cstart[c] > 1) insertion_sort_run(rs + (cstart[c] - S0), cstart[c + 1] - cstart[c]);
-            __syncwarp();
-            for (int j = S0 + lane; j < S1; j += 32) perm[j] = rs[j - S0];
-        } else {
-            for (int c = lane; c < UCELLS; c += 32)
-                if (cstart[c + 1] - cstart[c] > 1) insertion_sort_run(perm + cstart[c], cstart[c + 1] - cstart[c]);
-        }
-        const int* run = staged ? rs : perm + S0;   // the range, indexed from S0
-
-        // the queue: non-empty cells bucketed by count, largest first
-        bucket[lane] = 0;
-        for (int j = lane; j < WW; j += 32) ww[j] = make_float4(0, 0, 0, 0);
-        __syncwarp();
-        for (int c = lane; c < UCELLS; c += 32) {
-            const int n = cstart[c + 1] - cstart[c];
-            if (n > 0) atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1);
-        }
-        __syncwarp();
-        {
-            int v = bucket[lane], x = v;   // exclusive scan over the buckets (largest counts first)
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(ALL, x, o);
-                if (lane >= o) x += y;
-            }
-            bucket[lane] = x - v;
-            if (lane == 31) S.next[warp] = x;   // the number of non-empty cells, for now
-        }
-        __syncwarp();
-        const int ncells = S.next[warp];
-        for (int c = lane; c < UCELLS; c += 32) {
-            const int n = cstart[c + 1] - cstart[c];
-            if (n > 0) order[atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1)] = (unsigned char)c;
-        }
-        __syncwarp();
-        if (lane == 0) S.next[warp] = 32;
-        __syncwarp();
-
-        // 2. cells from the queue, summed in registers, added into the window when done; twice, (mass,
-        // x-momentum) and then (y-, z-momentum), so a lane holds 27 paired sums at a time, not 54, and twice as many
-        // warps fit an SM
-        auto pass = [&](auto tag) {
-            constexpr int HALF = decltype(tag)::value;
-            if (lane == 0) S.next[warp] = 32;
-            __syncwarp();
-            float2 acc[27];
-#pragma unroll
-            for (int k = 0; k < 27; k++) acc[k] = make_float2(0.0f, 0.0f);
-            int cell = lane < ncells ? order[lane] : -1;
-            int i = 0, end = 0;
-            PIn nxt, nxt2;
-            auto open = [&]() {
-                i = cstart[cell];
-                end = cstart[cell + 1];
-                load_pin_half<HALF>(nxt, in, st, checked_src(run, i - S0, s.np, s.status));
-                if (i + 1 < end) load_pin_half<HALF>(nxt2, in, st, checked_src(run, i + 1 - S0, s.np, s.status));
-            };
-            if (cell >= 0) open();
-            while (__any_sync(ALL, cell >= 0)) {
-                if (cell >= 0 && i < end) {
-                    const PIn qq = nxt;
-                    nxt = nxt2;
-                    if (i + 2 < end) load_pin_half<HALF>(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
-                    i++;
-                    int cl[3];
-                    float f[3];
-                    stencil_axis(qq.x, dm.nx, cl[0], f[0]);
-                    stencil_axis(qq.y, dm.ny, cl[1], f[1]);
-                    stencil_axis(qq.z, dm.nz, cl[2], f[2]);
-                    const bool mine = cl[0] == cx0 + (cell & 7) && cl[1] == cy0 + ((cell >> 3) & 7) && cl[2] == cz0 + (cell >> 6);
-                    if (!mine && HALF == 0) set_status(s.status, ST_OOB);
-                    if (mine && qq.m > 0.0f) {
-                        float wx[3], wy[3], wz[3];
-#pragma unroll
-                        for (int e = 0; e < 3; e++) {
-                            float* we = e == 0 ? wx : e == 1 ? wy : wz;
-                            const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
-                            we[0] = 0.5f * (ta * ta);
-                            we[1] = 0.75f - tc * tc;
-                            we[2] = 0.5f * (te * te);
-                        }
-                        float jp;
-                        if (p.tait) {
-                            const float r = __frcp_rn(qq.j), r2 = r * r;
-                            jp = p.bulk * ((r2 * r2) * r2 - qq.j);
-                        } else {
-                            jp = p.bulk * (1.0f - qq.j);
-                        }
-                        const float sp = (k4dt * (qq.m * vol)) * jp;
-                        // the half's momentum rows: A_a = m (v_a - C_a . f) - s f_a, B_ae = m C_ae + s [a == e];
-                        // the first half pairs the mass (coefficients m, 0, 0, 0) with row 0, the second rows 1 and 2
-                        float2 cA, b0, b1, b2;
-                        if (HALF == 0) {
-                            const float c0 = qq.c[0], c1 = qq.c[1], c2 = qq.c[2];
-                            cA = make_float2(qq.m, qq.m * (qq.u - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[0]);
-                            b0 = make_float2(0.0f, qq.m * c0 + sp);
-                            b1 = make_float2(0.0f, qq.m * c1);
-                            b2 = make_float2(0.0f, qq.m * c2);
-                        } else {
-                            const float c3 = qq.c[3], c4 = qq.c[4], c5 = qq.c[5], c6 = qq.c[6], c7 = qq.c[7], c8 = qq.c[8];
-                            cA = make_float2(qq.m * (qq.v - (c3 * f[0] + c4 * f[1] + c5 * f[2])) - sp * f[1],
-                                             qq.m * (qq.w - (c6 * f[0] + c7 * f[1] + c8 * f[2])) - sp * f[2]);
-                            b0 = make_float2(qq.m * c3, qq.m * c6);
-                            b1 = make_float2(qq.m * c4 + sp, qq.m * c7);
-                            b2 = make_float2(qq.m * c5, qq.m * c8 + sp);
-                        }
-#pragma unroll
-                        for (int oz = 0; oz < 3; oz++) {
-#pragma unroll
-                            for (int oy = 0; oy < 3; oy++) {
-                                const float wyz = wy[oy] * wz[oz];
-                                const float2 w2 = make_float2(wyz, wyz);
-                                float2 t = cA;
-                                if (oy) t = __ffma2_rn(make_float2((float)oy, (float)oy), b1, t);
-                                if (oz) t = __ffma2_rn(make_float2((float)oz, (float)oz), b2, t);
-                                const float2 g = __fmul2_rn(w2, t), h = __fmul2_rn(w2, b0);
-#pragma unroll
-                                for (int ox = 0; ox < 3; ox++) {
-                                    const int kk = (oz * 3 + oy) * 3 + ox;
-                                    float2 q = g;
-                                    if (ox == 1) q = __fadd2_rn(q, h);
-                                    else if (ox == 2) q = __ffma2_rn(make_float2(2.0f, 2.0f), h, q);
-                                    acc[kk] = __ffma2_rn(make_float2(wx[ox], wx[ox]), q, acc[kk]);
-                                }
-                            }
-                        }
-                    }
-                }
-                const bool done = cell >= 0 && i >= end;
-                const unsigned fm = __ballot_sync(ALL, done);
-                if (done) {
-                    // into the window's half of each node: lanes flushing together hold distinct cells, so at one
-                    // stencil offset they write distinct nodes
-                    const int wb = ((cell >> 6) * WWY + ((cell >> 3) & 7)) * WWX + (cell & 7);
-#pragma unroll
-                    for (int k = 0; k < 27; k++) {
-                        const int ox = k % 3, oy = (k / 3) % 3, oz = k / 9;
-                        float2* node = reinterpret_cast<float2*>(ww + wb + (oz * WWY + oy) * WWX + ox) + HALF;
-                        float2 v = *node;
-                        v.x += acc[k].x;
-                        v.y += acc[k].y;
-                        *node = v;
-                        acc[k] = make_float2(0.0f, 0.0f);
-                        __syncwarp(fm);
-                    }
-                    const int pos = atomicAdd(&S.next[warp], 1);
-                    cell = pos < ncells ? order[pos] : -1;
-                    if (cell >= 0) open();
-                }
-                __syncwarp();   // this iteration's window writes before the next iteration's reads
-            }
-            __syncwarp();
-        };
-        pass(std::integral_constant<int, 0>{});
-        pass(std::integral_constant<int, 1>{});
-
-        // 3. the window's touched nodes into the grid
-        for (int j = lane; j < WW; j += 32) {
-            const float4 t = ww[j];
-            if (t.x == 0.0f && t.y == 0.0f && t.z == 0.0f && t.w == 0.0f) continue;
-            const int gx = cx0 + j % WWX, gy = cy0 + (j / WWX) % WWY, gz = cz0 + j / (WWX * WWY);
-            if (gx >= dm.nx || gy >= dm.ny || gz >= dm.nz) {
-                set_status(s.status, ST_OOB);
-                continue;
-            }
-            float4* node = node_addr(s, gx, gy, gz);
-            if (!node) {
-                set_status(s.status, ST_POOL);
-                continue;
-            }
-            red_add_v4(node, t.x, t.y, t.z, t.w);
-        }
-        __syncwarp();
-    }
-}
-
 constexpr int P2G_UZ = 1;   // the unit depth the scatter runs
 
 size_t p2g_tile_smem() { return sizeof(P2GShared<P2G_UZ>); }
 
-#ifndef VF_P2G_SPLIT
-#define VF_P2G_SPLIT 1
-#endif
-constexpr bool P2G_SPLIT = VF_P2G_SPLIT != 0;   // the scatter in two halves of the momentum (a build may choose)
-
 cudaError_t p2g_tile_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_p2g3_tile<P2G_UZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p2g_tile_smem());
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_p2g3_tile_split<P2G_UZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_p2g3_tile<P2G_UZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)p2g_tile_smem());
 }
 
-int p2g_tile_blocks_per_sm() { return P2G_SPLIT ? VF_P2G_SPLIT_CTAS : 2; }
-
 cudaError_t launch_p2g3_tile(int blocks, const Step3& s, cudaStream_t stream) {
-    if (P2G_SPLIT)
-        k_p2g3_tile_split<P2G_UZ><<<blocks, P2G_THREADS, p2g_tile_smem(), stream>>>(s);
-    else
-        k_p2g3_tile<P2G_UZ><<<blocks, P2G_THREADS, p2g_tile_smem(), stream>>>(s);
+    k_p2g3_tile<P2G_UZ><<<blocks, P2G_THREADS, p2g_tile_smem(), stream>>>(s);
     return cudaGetLastError();
 }
 

@@ -206,7 +206,6 @@ cudaError_t fused_prepare();    // its shared-memory attribute
 int fused_blocks_per_sm();      // the CTAs an SM holds
 size_t p2g_tile_smem();
 cudaError_t p2g_tile_prepare();   // its shared-memory attribute
-int p2g_tile_blocks_per_sm();     // the CTAs an SM holds
 __global__ void k_grid3_dense(Step3 s);
 __global__ void k_g2p3(Step3 s);
 __global__ void k_g2p3_tile(Step3 s);
