@@ -249,8 +249,11 @@ def fast_backend(nx, ny, edges):
     return GpuSweBackend(nx, ny, edges, exact=False)
 
 
-@pytest.mark.parametrize("nx,ny,edges", [(512, 384, (0, 0, 0, 0)), (300, 130, (0, 1, 1, 0))])
+@pytest.mark.parametrize("nx,ny,edges", [(512, 384, (0, 0, 0, 0)), (300, 130, (0, 1, 1, 0)), (130, 37, (1, 0, 0, 1)),
+                                         (250, 3, (0, 0, 1, 1))])
 def test_fast_mode_stays_within_its_tolerance_of_the_oracle(nx, ny, edges):
+    """Both loaders of the fast mode's tile (TMA where the row pitch allows, plain loads at 130 and 250 columns),
+    walls and open sides, tiles that overrun the domain on both axes."""
     h = bumps(max(nx, ny), 3, count=10)[: nx * ny]
     z = np.zeros(nx * ny, F)
     params = swe_params(9.81, 0.45, 1, 1, 1e-6)

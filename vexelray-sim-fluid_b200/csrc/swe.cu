@@ -6,12 +6,13 @@
 // reference's strict f32 (Java) arithmetic does, so a step's output is bit-identical to the
 // reference's CPU semantics (and to the oracle), and so are the tick counts it derives.
 //
-// A second arithmetic, the fast mode (vf_swe_set_exact(h, 0)), keeps the tile and the flux form but rounds
-// differently: fused multiply-adds (written out as fmaf, since the file forbids contraction), one approximate
-// reciprocal of a cell's depth shared by its two velocities, one approximate reciprocal of each face's wave span
-// shared by its three fluxes, and an approximate square root for the wave speed. About a third of the exact
-// step's instructions; within a stated tolerance of the reference rather than equal to it, and the flux form
-// still moves water only between neighbours. The tick count from the previous step's speed stays IEEE.
+// A second arithmetic, the fast mode (vf_swe_set_exact(h, 0)), keeps the flux form but rounds differently:
+// fused multiply-adds (written out as fmaf, since the file forbids contraction), one approximate reciprocal of a
+// cell's depth shared by its two velocities, one approximate reciprocal of each face's wave span shared by its
+// three fluxes, and an approximate square root for the wave speed; and it runs as a column walk in registers over
+// a TMA-staged tile (k_swe_strip_fast) instead of staging primitives and fluxes in shared memory. It is within a
+// stated tolerance of the reference rather than equal to it, and the water still moves only between neighbours.
+// The tick count from the previous step's speed stays IEEE.
 //
 // One CTA per 64 x 16 tile of cells:
 //   1. the tile and a one-cell halo of h, hu, hv land in shared memory by three 2D TMA loads
@@ -162,7 +163,7 @@ __device__ __forceinline__ bool wait_barrier(unsigned long long* bar, int phase,
 
 // One tile (tx, ty) of one step. The CTA's mbarrier is initialised; `parity` is the phase its TMA completes.
 // Returns false (status set, nothing written) when the TMA did not land within the bounded wait.
-template <int TX_, bool FAST>
+template <int TX_>
 __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm_h, const CUtensorMap* tm_hu,
                                          const CUtensorMap* tm_hv, SweShared<TX_>& S, int tx, int ty, int parity) {
     using T = Tile<TX_>;
@@ -220,16 +221,9 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
     for (int i = tid; i < PY * PX; i += SWE_THREADS) {
         const int ly = i / PX, lx = i % PX;
         const float h = S.box[0][(ly) * HX + lx + 3];
-        if constexpr (FAST) {
-            const float inv = h > dry ? __fdividef(1.0f, h) : 0.0f;
-            S.pu[ly][lx] = S.box[1][(ly) * HX + lx + 3] * inv;
-            S.pv[ly][lx] = S.box[2][(ly) * HX + lx + 3] * inv;
-            S.pc[ly][lx] = sqrt_fast(g * h);
-        } else {
-            S.pu[ly][lx] = velocity(h, S.box[1][(ly) * HX + lx + 3], dry);
-            S.pv[ly][lx] = velocity(h, S.box[2][(ly) * HX + lx + 3], dry);
-            S.pc[ly][lx] = sqrtf(g * h);
-        }
+        S.pu[ly][lx] = velocity(h, S.box[1][(ly) * HX + lx + 3], dry);
+        S.pv[ly][lx] = velocity(h, S.box[2][(ly) * HX + lx + 3], dry);
+        S.pc[ly][lx] = sqrtf(g * h);
     }
     __syncthreads();
 
@@ -253,10 +247,8 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const float hL = S.box[0][(py) * HX + l + 3], hR = S.box[0][(py) * HX + r + 3];
         const float qnL = sgnL * S.box[1][(py) * HX + l + 3], qtL = S.box[2][(py) * HX + l + 3];
         const float qnR = sgnR * S.box[1][(py) * HX + r + 3], qtR = S.box[2][(py) * HX + r + 3];
-        const Face f = FAST ? hll_fast(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR,
-                                       qtR, sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r])
-                            : hll(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR, qtR,
-                                  sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r]);
+        const Face f = hll(g, dry, hL, qnL, qtL, sgnL * S.pu[py][l], S.pv[py][l], S.pc[py][l], hR, qnR, qtR,
+                           sgnR * S.pu[py][r], S.pv[py][r], S.pc[py][r]);
         S.fx[0][ly][lf] = f.mass;
         S.fx[1][ly][lf] = f.normal;
         S.fx[2][ly][lf] = f.tangent;
@@ -280,10 +272,8 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const float hB = S.box[0][(b) * HX + px + 3], hT = S.box[0][(t) * HX + px + 3];
         const float qnB = sgnB * S.box[2][(b) * HX + px + 3], qtB = S.box[1][(b) * HX + px + 3];
         const float qnT = sgnT * S.box[2][(t) * HX + px + 3], qtT = S.box[1][(t) * HX + px + 3];
-        const Face f = FAST ? hll_fast(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT,
-                                       qtT, sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px])
-                            : hll(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT, qtT,
-                                  sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px]);
+        const Face f = hll(g, dry, hB, qnB, qtB, sgnB * S.pv[b][px], S.pu[b][px], S.pc[b][px], hT, qnT, qtT,
+                           sgnT * S.pv[t][px], S.pu[t][px], S.pc[t][px]);
         S.fy[0][lf][lx] = f.mass;
         S.fy[1][lf][lx] = f.normal;
         S.fy[2][lf][lx] = f.tangent;
@@ -297,30 +287,19 @@ __device__ __forceinline__ bool swe_tile(const SweArgs& a, const CUtensorMap* tm
         const int gx = x0 + lx, gy = y0 + ly;
         if (gx >= nx || gy >= ny) continue;
         const float h0 = S.box[0][(ly + 1) * HX + lx + 4], hu0 = S.box[1][(ly + 1) * HX + lx + 4], hv0 = S.box[2][(ly + 1) * HX + lx + 4];
-        float h, hu, hv;
-        if constexpr (FAST) {
-            h = __fmaf_rn(-ry, S.fy[0][ly + 1][lx] - S.fy[0][ly][lx], __fmaf_rn(-rx, S.fx[0][ly][lx + 1] - S.fx[0][ly][lx], h0));
-            hu = __fmaf_rn(-ry, S.fy[2][ly + 1][lx] - S.fy[2][ly][lx], __fmaf_rn(-rx, S.fx[1][ly][lx + 1] - S.fx[1][ly][lx], hu0));
-            hv = __fmaf_rn(-ry, S.fy[1][ly + 1][lx] - S.fy[1][ly][lx], __fmaf_rn(-rx, S.fx[2][ly][lx + 1] - S.fx[2][ly][lx], hv0));
-        } else {
-            h = (h0 - rx * (S.fx[0][ly][lx + 1] - S.fx[0][ly][lx])) - ry * (S.fy[0][ly + 1][lx] - S.fy[0][ly][lx]);
-            hu = (hu0 - rx * (S.fx[1][ly][lx + 1] - S.fx[1][ly][lx])) - ry * (S.fy[2][ly + 1][lx] - S.fy[2][ly][lx]);
-            hv = (hv0 - rx * (S.fx[2][ly][lx + 1] - S.fx[2][ly][lx])) - ry * (S.fy[1][ly + 1][lx] - S.fy[1][ly][lx]);
-        }
+        const float h = (h0 - rx * (S.fx[0][ly][lx + 1] - S.fx[0][ly][lx])) - ry * (S.fy[0][ly + 1][lx] - S.fy[0][ly][lx]);
+        const float hu =
+            (hu0 - rx * (S.fx[1][ly][lx + 1] - S.fx[1][ly][lx])) - ry * (S.fy[2][ly + 1][lx] - S.fy[2][ly][lx]);
+        const float hv =
+            (hv0 - rx * (S.fx[2][ly][lx + 1] - S.fx[2][ly][lx])) - ry * (S.fy[1][ly + 1][lx] - S.fy[1][ly][lx]);
         if (h < 0.0f) clamps++;
         const float nh = fmaxf(h, 0.0f);
         const int64_t c = (int64_t)gy * nx + gx;
         a.out[0][c] = nh;
         a.out[1][c] = hu;
         a.out[2][c] = hv;
-        float speed;
-        if constexpr (FAST) {
-            const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
-            speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
-        } else {
-            const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
-            speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
-        }
+        const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
+        const float speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
         best = max(best, __float_as_int(speed));
         if (c == 0) {
             *a.speed_clear = 0;
@@ -369,7 +348,7 @@ __device__ __forceinline__ void init_tile_barrier(SweShared<TX_>& S, bool tma) {
 // One step, one CTA per tile (grid = tiles). Launched as a programmatic dependent of the previous step: its CTAs
 // may become resident during that step's last wave, set up their barrier, and wait (griddepcontrol.wait: until
 // the previous grid has completed and its stores are visible) before reading anything the previous step wrote.
-template <int TX_, bool FAST>
+template <int TX_>
 __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
                                                           const __grid_constant__ CUtensorMap tm_hu,
                                                           const __grid_constant__ CUtensorMap tm_hv) {
@@ -377,7 +356,210 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
     SweShared<TX_>& S = swe_shared<TX_>();
     init_tile_barrier(S, a.use_tma);
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    swe_tile<TX_, FAST>(a, &tm_h, &tm_hu, &tm_hv, S, blockIdx.x, blockIdx.y, 0);
+    swe_tile<TX_>(a, &tm_h, &tm_hu, &tm_hv, S, blockIdx.x, blockIdx.y, 0);
+}
+
+// ------------------------------------------------------------------ the fast mode's strip kernel
+// One CTA of four warps per tile of 120 columns x 32 rows. The tile and a halo (columns x0-4 .. x0+123, rows
+// y0-1 .. y0+32) land in shared memory by three 2D TMA loads; then every lane walks one column up the tile in
+// registers: lane L of warp w holds column x0 + 30 w + L - 1, lanes 1..30 update their cell, lanes 0 and 31 only
+// lend their state to their neighbours. A cell's west face is computed by its lane from its left neighbour's state
+// (a shuffle), its east face is the right neighbour's west face (a shuffle), its south face was computed one row
+// below and its north face is computed from the next row: every face once (twice where two warps meet, from the
+// same inputs), the state read from shared memory once, and no shared-memory traffic for primitives or fluxes.
+constexpr int STRIP_WARPS = 4;
+constexpr int STRIP_COLS = 30 * STRIP_WARPS;   // columns a tile updates (a multiple of 4: the box's x stays aligned)
+constexpr int STRIP_ROWS = 32;
+constexpr int STRIP_BW = 128;                  // box width: columns x0-4 .. x0+123
+constexpr int STRIP_BH = STRIP_ROWS + 2;       // box height: rows y0-1 .. y0+ROWS
+
+struct StripShared {
+    float box[3][STRIP_BH * STRIP_BW];
+    unsigned long long bar;
+    int red[STRIP_WARPS];
+    int clamps;
+};
+
+struct CellState {
+    float h, qx, qy, u, v, c;   // depth, momenta, velocities, wave speed
+};
+
+__device__ __forceinline__ CellState cell_fast(float h, float qx, float qy, float g, float dry) {
+    CellState q;
+    q.h = h;
+    q.qx = qx;
+    q.qy = qy;
+    const float inv = h > dry ? __fdividef(1.0f, h) : 0.0f;
+    q.u = qx * inv;
+    q.v = qy * inv;
+    q.c = sqrt_fast(g * h);
+    return q;
+}
+
+__device__ __forceinline__ CellState shfl_up_cell(const CellState& a) {
+    const unsigned all = 0xffffffffu;
+    CellState q;
+    q.h = __shfl_up_sync(all, a.h, 1);
+    q.qx = __shfl_up_sync(all, a.qx, 1);
+    q.qy = __shfl_up_sync(all, a.qy, 1);
+    q.u = __shfl_up_sync(all, a.u, 1);
+    q.v = __shfl_up_sync(all, a.v, 1);
+    q.c = __shfl_up_sync(all, a.c, 1);
+    return q;
+}
+
+// The ghost of a cell across a side (ShallowWater.neighbour, ShallowWater.java:316-326): a wall negates the normal
+// momentum (and so the normal velocity), an open side copies the cell.
+__device__ __forceinline__ CellState ghost_x(CellState q, bool wall) {
+    if (wall) {
+        q.qx = -q.qx;
+        q.u = -q.u;
+    }
+    return q;
+}
+
+__device__ __forceinline__ CellState ghost_y(CellState q, bool wall) {
+    if (wall) {
+        q.qy = -q.qy;
+        q.v = -q.v;
+    }
+    return q;
+}
+
+__global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip_fast(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
+                                                                    const __grid_constant__ CUtensorMap tm_hu,
+                                                                    const __grid_constant__ CUtensorMap tm_hv) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    extern __shared__ __align__(128) unsigned char strip_raw[];
+    const uint32_t mis = (uint32_t)__cvta_generic_to_shared(strip_raw) & 127u;
+    StripShared& S = *reinterpret_cast<StripShared*>(strip_raw + ((128u - mis) & 127u));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0 && a.use_tma) {
+        const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int x0 = blockIdx.x * STRIP_COLS, y0 = blockIdx.y * STRIP_ROWS;
+    const int nx = a.nx, ny = a.ny;
+    // ShallowWater.java:184-192: the step from the fastest wave, in whole ticks, within the budget
+    const float g = a.params[0], courant = a.params[1], dx = a.params[2], dy = a.params[3], dry = a.params[4];
+    const float fastest = __int_as_float(__ldcg(a.speed_in));
+    const float allowed = fminf((courant * fminf(dx, dy)) / fmaxf(fastest, 1e-30f), 2000.0f);
+    int ticks = (int)(allowed * 1000000.0f);
+    const int budget = __ldcg(a.budget_in);
+    if (budget < ticks) ticks = budget;
+    const float dt = (float)ticks * (float)(1.0 / 1000000.0);
+    const float rx = dt / dx;
+    const float ry = dt / dy;
+    // 1. stage the tile and its halo
+    bool loaded = true;
+    if (tid == 0) S.clamps = 0;
+    if (a.use_tma) {
+        if (tid == 0) {
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+            const uint32_t bytes = 3u * STRIP_BH * STRIP_BW * 4u;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+            const CUtensorMap* maps[3] = {&tm_h, &tm_hu, &tm_hv};
+            const int bx = x0 - 4, by = y0 - 1;   // bx is a multiple of 4: 16-byte aligned
+            for (int f = 0; f < 3; f++) {
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&S.box[f][0]);
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                    "[%4];" ::"r"(dst),
+                    "l"(maps[f]), "r"(bx), "r"(by), "r"(bar)
+                    : "memory");
+            }
+        }
+        loaded = wait_barrier(&S.bar, 0, a.status);
+    } else {
+        for (int i = tid; i < STRIP_BH * STRIP_BW; i += STRIP_WARPS * 32) {
+            const int ly = i / STRIP_BW, lx = i % STRIP_BW;
+            const int gx = x0 - 4 + lx, gy = y0 - 1 + ly;
+            const bool in = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+            const int64_t c = (int64_t)gy * nx + gx;
+            for (int f = 0; f < 3; f++) S.box[f][i] = in ? __ldcg(a.in[f] + c) : 0.0f;
+        }
+    }
+    if (!__syncthreads_and(loaded)) return;   // a TMA that never landed: the status says so, nothing is written
+
+    // 2. the column walk
+    const int cx = x0 + 30 * warp + lane - 1;        // this lane's column
+    const int bc = 30 * warp + lane + 3;             // its column in the box
+    const bool own = lane >= 1 && lane <= 30 && cx < nx;
+    const bool wall_w = a.edge[0] == VF_EDGE_WALL, wall_e = a.edge[1] == VF_EDGE_WALL;
+    const bool wall_s = a.edge[2] == VF_EDGE_WALL, wall_n = a.edge[3] == VF_EDGE_WALL;
+    auto load = [&](int r) {
+        const int i = r * STRIP_BW + bc;
+        return cell_fast(S.box[0][i], S.box[1][i], S.box[2][i], g, dry);
+    };
+    CellState prev = load(0);
+    Face gs = {0.0f, 0.0f, 0.0f}, fw = {0.0f, 0.0f, 0.0f}, fe = {0.0f, 0.0f, 0.0f};
+    int best = 0, clamps = 0;
+    for (int r = 1; r <= STRIP_ROWS + 1; r++) {
+        const int y = y0 - 1 + r;   // this box row's row of the domain
+        const CellState cur = load(r);
+        // the face between rows y-1 and y (cur's south face, prev's north face)
+        CellState bot = prev, top = cur;
+        if (y == 0) bot = ghost_y(cur, wall_s);
+        if (y == ny) top = ghost_y(prev, wall_n);
+        const Face gn = hll_fast(g, dry, bot.h, bot.qy, bot.qx, bot.v, bot.u, bot.c, top.h, top.qy, top.qx, top.v,
+                                 top.u, top.c);
+        if (r >= 2) {
+            // the update of row y-1 (ShallowWater.java:206-235) from its four faces
+            const int yu = y - 1;
+            if (own && yu < ny) {
+                const float h = __fmaf_rn(-ry, gn.mass - gs.mass, __fmaf_rn(-rx, fe.mass - fw.mass, prev.h));
+                const float hu = __fmaf_rn(-ry, gn.tangent - gs.tangent, __fmaf_rn(-rx, fe.normal - fw.normal, prev.qx));
+                const float hv = __fmaf_rn(-ry, gn.normal - gs.normal, __fmaf_rn(-rx, fe.tangent - fw.tangent, prev.qy));
+                if (h < 0.0f) clamps++;
+                const float nh = fmaxf(h, 0.0f);
+                const int64_t c = (int64_t)yu * nx + cx;
+                a.out[0][c] = nh;
+                a.out[1][c] = hu;
+                a.out[2][c] = hv;
+                const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
+                const float speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
+                best = max(best, __float_as_int(speed));
+                if (c == 0) {
+                    *a.speed_clear = 0;
+                    *a.budget_out = budget - ticks;
+                }
+            }
+        }
+        gs = gn;
+        if (r <= STRIP_ROWS) {
+            // this row's x-faces, for its update at the next row: the west face from the left neighbour, the east
+            // face the right neighbour's west face
+            CellState left = shfl_up_cell(cur), right = cur;
+            if (cx == 0) left = ghost_x(cur, wall_w);
+            if (cx == nx) right = ghost_x(left, wall_e);
+            fw = hll_fast(g, dry, left.h, left.qx, left.qy, left.u, left.v, left.c, right.h, right.qx, right.qy,
+                          right.u, right.v, right.c);
+            fe.mass = __shfl_down_sync(0xffffffffu, fw.mass, 1);
+            fe.normal = __shfl_down_sync(0xffffffffu, fw.normal, 1);
+            fe.tangent = __shfl_down_sync(0xffffffffu, fw.tangent, 1);
+        }
+        prev = cur;
+    }
+    // 3. the CTA's fastest wave and clamp count, one atomic each
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+        clamps += __shfl_xor_sync(0xffffffffu, clamps, o);
+    }
+    if (lane == 0) {
+        S.red[warp] = best;
+        if (clamps) atomicAdd(&S.clamps, clamps);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int m = 0;
+        for (int w = 0; w < STRIP_WARPS; w++) m = max(m, S.red[w]);
+        if (m > *(volatile int*)a.speed_out) atomicMax(a.speed_out, m);
+        if (S.clamps) atomicAdd(a.clamped, S.clamps);
+    }
 }
 
 // ------------------------------------------------------------------ diagnostics (Diagnostics.of)
@@ -529,6 +711,7 @@ struct vf_swe {
     DeviceBuffer status, diag;
     int32_t* host_words = nullptr;   // pinned: the budget and the status word read back together
     CUtensorMap maps[2][2][3];   // [tile width 64, 32][state][field]
+    CUtensorMap smaps[2][3];     // the fast mode's strip boxes: [state][field]
     bool tma = false;
     int tile_w = 64;             // the tile width the steps use
     bool pdl = true;             // steps launched as programmatic dependents of the previous step
@@ -584,21 +767,27 @@ int32_t dispatch(vf_swe* h) {
     for (int e = 0; e < 4; e++) a.edge[e] = h->edges[e];
     a.use_tma = h->tma ? 1 : 0;
     const int wide = h->tile_w == 64;
-    CUtensorMap* m = h->maps[wide ? 0 : 1][si];
+    CUtensorMap* m = h->exact ? h->maps[wide ? 0 : 1][si] : h->smaps[si];
     void* args[] = {&a, &m[0], &m[1], &m[2]};
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
-    cfg.blockDim = dim3(SWE_THREADS);
-    cfg.dynamicSmemBytes = wide ? sizeof(SweShared<64>) + 128 : sizeof(SweShared<32>) + 128;
+    if (h->exact) {
+        cfg.gridDim = dim3(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
+        cfg.blockDim = dim3(SWE_THREADS);
+        cfg.dynamicSmemBytes = wide ? sizeof(SweShared<64>) + 128 : sizeof(SweShared<32>) + 128;
+    } else {
+        cfg.gridDim = dim3(div_up(h->nx, STRIP_COLS), div_up(h->ny, STRIP_ROWS));
+        cfg.blockDim = dim3(STRIP_WARPS * 32);
+        cfg.dynamicSmemBytes = sizeof(StripShared) + 128;
+    }
     cfg.stream = h->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = h->pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void* fn = h->exact ? (wide ? (const void*)k_swe_tile<64, false> : (const void*)k_swe_tile<32, false>)
-                              : (wide ? (const void*)k_swe_tile<64, true> : (const void*)k_swe_tile<32, true>);
-    h->prof.begin(h->exact ? "k_swe_tile" : "k_swe_tile_fast", h->stream);
+    const void* fn = h->exact ? (wide ? (const void*)k_swe_tile<64> : (const void*)k_swe_tile<32>)
+                              : (const void*)k_swe_strip_fast;
+    h->prof.begin(h->exact ? "k_swe_tile" : "k_swe_strip_fast", h->stream);
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
@@ -687,14 +876,12 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
         return VF_ENOMEM;
     }
     for (DeviceBuffer* b : {&h->state[0], &h->state[1], &h->small, &h->status}) cudaMemsetAsync(b->ptr, 0, b->bytes, h->stream);
-    if (cudaFuncSetAttribute(k_swe_tile<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_swe_tile<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
-        cudaFuncSetAttribute(k_swe_tile<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_swe_tile<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(SweShared<32>) + 128) != cudaSuccess ||
-        cudaFuncSetAttribute(k_swe_tile<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
-        cudaFuncSetAttribute(k_swe_tile<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(SweShared<32>) + 128) != cudaSuccess) {
+        cudaFuncSetAttribute(k_swe_strip_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(StripShared) + 128) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared<64>));
         return VF_ECUDA;
@@ -703,9 +890,13 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
     for (int s = 0; s < 2; s++)
         for (int f = 0; f < 3; f++)
             tma = tma && make_map(&h->maps[0][s][f], field(h, s, f), nx, ny, Tile<64>::HX, Tile<64>::HY) &&
-                  make_map(&h->maps[1][s][f], field(h, s, f), nx, ny, Tile<32>::HX, Tile<32>::HY);
+                  make_map(&h->maps[1][s][f], field(h, s, f), nx, ny, Tile<32>::HX, Tile<32>::HY) &&
+                  make_map(&h->smaps[s][f], field(h, s, f), nx, ny, STRIP_BW, STRIP_BH);
     h->tma = tma;
-    if (!tma) memset(h->maps, 0, sizeof h->maps);
+    if (!tma) {
+        memset(h->maps, 0, sizeof h->maps);
+        memset(h->smaps, 0, sizeof h->smaps);
+    }
     h->tile_w = auto_tile_width(nx, ny);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
         vf_swe_destroy(h);
