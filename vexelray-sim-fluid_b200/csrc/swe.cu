@@ -135,6 +135,46 @@ __device__ __forceinline__ Face hll_fast(float g, float dry, float hL, float qnL
     return f;
 }
 
+// Two faces of the fast mode's HLL at once, one in each half of paired fp32 (FFMA2/FADD2/FMUL2): the column walk's
+// x-face and y-face of a row, which are independent.
+struct Face2 {
+    float2 mass, normal, tangent;
+};
+
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+__device__ __forceinline__ float2 max2(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+
+__device__ __forceinline__ Face2 hll_fast2(float g, float dry, float2 hL, float2 qnL, float2 qtL, float2 unL, float2 utL,
+                                           float2 cL, float2 hR, float2 qnR, float2 qtR, float2 unR, float2 utR,
+                                           float2 cR) {
+    const float2 lm = __fadd2_rn(unL, neg2(cL)), lp = __fadd2_rn(unL, cL);
+    const float2 rm = __fadd2_rn(unR, neg2(cR)), rp = __fadd2_rn(unR, cR);
+    float2 sL = min2(lm, rm), sR = max2(lp, rp);
+    const float2 two = f2(2.0f, 2.0f);
+    const float2 l2 = __ffma2_rn(two, cL, unL), r2 = __ffma2_rn(neg2(two), cR, unR);
+    if (!(hR.x > dry)) { sL.x = lm.x; sR.x = l2.x; }
+    if (!(hR.y > dry)) { sL.y = lm.y; sR.y = l2.y; }
+    if (!(hL.x > dry)) { sL.x = r2.x; sR.x = rp.x; }
+    if (!(hL.y > dry)) { sL.y = r2.y; sR.y = rp.y; }
+    const float2 zero = f2(0.0f, 0.0f);
+    const float2 lo = min2(sL, zero), hi = max2(sR, zero);
+    const float2 span = max2(__fadd2_rn(hi, neg2(lo)), f2(1e-30f, 1e-30f));
+    const float2 inv = f2(__fdividef(1.0f, span.x), __fdividef(1.0f, span.y));
+    const float2 lohi = __fmul2_rn(lo, hi);
+    const float2 hg = f2(0.5f * g, 0.5f * g);
+    const float2 pL = __fmul2_rn(hg, __fmul2_rn(hL, hL)), pR = __fmul2_rn(hg, __fmul2_rn(hR, hR));
+    const float2 loqR = __fmul2_rn(lo, qnR), hiqL = __fmul2_rn(hi, qnL);
+    Face2 f;
+    f.mass = __fmul2_rn(__ffma2_rn(lohi, __fadd2_rn(hR, neg2(hL)), __fadd2_rn(hiqL, neg2(loqR))), inv);
+    const float2 fl = __ffma2_rn(qnL, unL, pL), fr = __ffma2_rn(qnR, unR, pR);
+    f.normal = __fmul2_rn(__ffma2_rn(lohi, __fadd2_rn(qnR, neg2(qnL)), __ffma2_rn(hi, fl, neg2(__fmul2_rn(lo, fr)))), inv);
+    f.tangent =
+        __fmul2_rn(__ffma2_rn(lohi, __fadd2_rn(qtR, neg2(qtL)), __ffma2_rn(hiqL, utL, neg2(__fmul2_rn(loqR, utR)))), inv);
+    return f;
+}
+
 // The fast mode's square root (approximate reciprocal square root; zero at zero).
 __device__ __forceinline__ float sqrt_fast(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
@@ -426,6 +466,75 @@ __device__ __forceinline__ CellState ghost_y(CellState q, bool wall) {
     return q;
 }
 
+// One CTA's column walk (k_swe_strip_fast, step 2). INTERIOR: the tile and its halo lie inside the domain.
+template <bool INTERIOR>
+__device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int x0, int y0, float g, float dry, float rx,
+                                           float ry, int budget, int ticks, int& best, int& clamps) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nx = a.nx, ny = a.ny;
+    const int cx = x0 + 30 * warp + lane - 1;        // this lane's column
+    const int bc = 30 * warp + lane + 3;             // its column in the box
+    const bool own = lane >= 1 && lane <= 30 && (INTERIOR || cx < nx);
+    const bool wall_w = a.edge[0] == VF_EDGE_WALL, wall_e = a.edge[1] == VF_EDGE_WALL;
+    const bool wall_s = a.edge[2] == VF_EDGE_WALL, wall_n = a.edge[3] == VF_EDGE_WALL;
+    auto load = [&](int r) {
+        const int i = r * STRIP_BW + bc;
+        return cell_fast(S.box[0][i], S.box[1][i], S.box[2][i], g, dry);
+    };
+    CellState prev = load(0);
+    Face gs = {0.0f, 0.0f, 0.0f}, fw = {0.0f, 0.0f, 0.0f}, fe = {0.0f, 0.0f, 0.0f};
+    for (int r = 1; r <= STRIP_ROWS + 1; r++) {
+        const int y = y0 - 1 + r;   // this box row's row of the domain
+        const CellState cur = load(r);
+        // the face between rows y-1 and y (cur's south face, prev's north face), and this row's west face from the
+        // left neighbour, together in paired fp32
+        CellState bot = prev, top = cur;
+        CellState left = shfl_up_cell(cur), right = cur;
+        if (!INTERIOR) {
+            if (y == 0) bot = ghost_y(cur, wall_s);
+            if (y == ny) top = ghost_y(prev, wall_n);
+            if (cx == 0) left = ghost_x(cur, wall_w);
+            if (cx == nx) right = ghost_x(left, wall_e);
+        }
+        // .x the y-face (normal y), .y the x-face (normal x)
+        const Face2 ff = hll_fast2(g, dry, f2(bot.h, left.h), f2(bot.qy, left.qx), f2(bot.qx, left.qy),
+                                   f2(bot.v, left.u), f2(bot.u, left.v), f2(bot.c, left.c), f2(top.h, right.h),
+                                   f2(top.qy, right.qx), f2(top.qx, right.qy), f2(top.v, right.u), f2(top.u, right.v),
+                                   f2(top.c, right.c));
+        const Face gn = {ff.mass.x, ff.normal.x, ff.tangent.x};
+        if (r >= 2) {
+            // the update of row y-1 (ShallowWater.java:206-235) from its four faces
+            const int yu = y - 1;
+            if (own && (INTERIOR || yu < ny)) {
+                const float h = __fmaf_rn(-ry, gn.mass - gs.mass, __fmaf_rn(-rx, fe.mass - fw.mass, prev.h));
+                const float hu = __fmaf_rn(-ry, gn.tangent - gs.tangent, __fmaf_rn(-rx, fe.normal - fw.normal, prev.qx));
+                const float hv = __fmaf_rn(-ry, gn.normal - gs.normal, __fmaf_rn(-rx, fe.tangent - fw.tangent, prev.qy));
+                if (h < 0.0f) clamps++;
+                const float nh = fmaxf(h, 0.0f);
+                const int64_t c = (int64_t)yu * nx + cx;
+                a.out[0][c] = nh;
+                a.out[1][c] = hu;
+                a.out[2][c] = hv;
+                const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
+                const float speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
+                best = max(best, __float_as_int(speed));
+                if (!INTERIOR && c == 0) {
+                    *a.speed_clear = 0;
+                    *a.budget_out = budget - ticks;
+                }
+            }
+        }
+        gs = gn;
+        // this row's x-faces for its update at the next row: its own west face, and the right neighbour's west face
+        // as its east face
+        fw = Face{ff.mass.y, ff.normal.y, ff.tangent.y};
+        fe.mass = __shfl_down_sync(0xffffffffu, fw.mass, 1);
+        fe.normal = __shfl_down_sync(0xffffffffu, fw.normal, 1);
+        fe.tangent = __shfl_down_sync(0xffffffffu, fw.tangent, 1);
+        prev = cur;
+    }
+}
+
 __global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip_fast(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
                                                                     const __grid_constant__ CUtensorMap tm_hu,
                                                                     const __grid_constant__ CUtensorMap tm_hv) {
@@ -484,65 +593,13 @@ __global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip_fast(SweArgs a, 
     }
     if (!__syncthreads_and(loaded)) return;   // a TMA that never landed: the status says so, nothing is written
 
-    // 2. the column walk
-    const int cx = x0 + 30 * warp + lane - 1;        // this lane's column
-    const int bc = 30 * warp + lane + 3;             // its column in the box
-    const bool own = lane >= 1 && lane <= 30 && cx < nx;
-    const bool wall_w = a.edge[0] == VF_EDGE_WALL, wall_e = a.edge[1] == VF_EDGE_WALL;
-    const bool wall_s = a.edge[2] == VF_EDGE_WALL, wall_n = a.edge[3] == VF_EDGE_WALL;
-    auto load = [&](int r) {
-        const int i = r * STRIP_BW + bc;
-        return cell_fast(S.box[0][i], S.box[1][i], S.box[2][i], g, dry);
-    };
-    CellState prev = load(0);
-    Face gs = {0.0f, 0.0f, 0.0f}, fw = {0.0f, 0.0f, 0.0f}, fe = {0.0f, 0.0f, 0.0f};
+    // 2. the column walk: tiles that touch no side of the domain skip every ghost and bounds test
     int best = 0, clamps = 0;
-    for (int r = 1; r <= STRIP_ROWS + 1; r++) {
-        const int y = y0 - 1 + r;   // this box row's row of the domain
-        const CellState cur = load(r);
-        // the face between rows y-1 and y (cur's south face, prev's north face)
-        CellState bot = prev, top = cur;
-        if (y == 0) bot = ghost_y(cur, wall_s);
-        if (y == ny) top = ghost_y(prev, wall_n);
-        const Face gn = hll_fast(g, dry, bot.h, bot.qy, bot.qx, bot.v, bot.u, bot.c, top.h, top.qy, top.qx, top.v,
-                                 top.u, top.c);
-        if (r >= 2) {
-            // the update of row y-1 (ShallowWater.java:206-235) from its four faces
-            const int yu = y - 1;
-            if (own && yu < ny) {
-                const float h = __fmaf_rn(-ry, gn.mass - gs.mass, __fmaf_rn(-rx, fe.mass - fw.mass, prev.h));
-                const float hu = __fmaf_rn(-ry, gn.tangent - gs.tangent, __fmaf_rn(-rx, fe.normal - fw.normal, prev.qx));
-                const float hv = __fmaf_rn(-ry, gn.normal - gs.normal, __fmaf_rn(-rx, fe.tangent - fw.tangent, prev.qy));
-                if (h < 0.0f) clamps++;
-                const float nh = fmaxf(h, 0.0f);
-                const int64_t c = (int64_t)yu * nx + cx;
-                a.out[0][c] = nh;
-                a.out[1][c] = hu;
-                a.out[2][c] = hv;
-                const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
-                const float speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
-                best = max(best, __float_as_int(speed));
-                if (c == 0) {
-                    *a.speed_clear = 0;
-                    *a.budget_out = budget - ticks;
-                }
-            }
-        }
-        gs = gn;
-        if (r <= STRIP_ROWS) {
-            // this row's x-faces, for its update at the next row: the west face from the left neighbour, the east
-            // face the right neighbour's west face
-            CellState left = shfl_up_cell(cur), right = cur;
-            if (cx == 0) left = ghost_x(cur, wall_w);
-            if (cx == nx) right = ghost_x(left, wall_e);
-            fw = hll_fast(g, dry, left.h, left.qx, left.qy, left.u, left.v, left.c, right.h, right.qx, right.qy,
-                          right.u, right.v, right.c);
-            fe.mass = __shfl_down_sync(0xffffffffu, fw.mass, 1);
-            fe.normal = __shfl_down_sync(0xffffffffu, fw.normal, 1);
-            fe.tangent = __shfl_down_sync(0xffffffffu, fw.tangent, 1);
-        }
-        prev = cur;
-    }
+    const bool interior = x0 >= 1 && x0 + STRIP_COLS + 1 <= nx && y0 >= 1 && y0 + STRIP_ROWS + 1 <= ny;
+    if (interior)
+        strip_walk<true>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
+    else
+        strip_walk<false>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
     // 3. the CTA's fastest wave and clamp count, one atomic each
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
