@@ -365,9 +365,10 @@ int32_t vf_swe_dispatch(vf_swe* h, int32_t n);
 int64_t vf_swe_dispatched(const vf_swe* h);
 int32_t vf_swe_write_budget(vf_swe* h, int32_t slot, int32_t ticks);
 int32_t vf_swe_read_budget(vf_swe* h, int32_t slot, int32_t* ticks);
-/* The step kernel's tile width: 64 or 32 cells (16 rows either way); 0 picks by grid size (32 when 64-wide tiles
- * would give fewer than four per resident CTA slot, e.g. 1024^2). No counterpart in the reference: results are
- * bit-identical for both widths, only the speed differs. */
+/* The step kernel: 0 (the default) walks columns of 120 x 32-cell strips in registers (k_swe_strip); 64 or 32
+ * stage primitives and fluxes of 64- or 32-cell-wide tiles in shared memory (k_swe_tile, 16 rows). No counterpart
+ * in the reference: results are bit-identical for all three, only the speed differs. The fast mode
+ * (vf_swe_set_exact(h, 0)) always walks strips. */
 int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width);
 int32_t vf_swe_tile_width(const vf_swe* h);
 /* Each step launched as a programmatic dependent of the previous one (its CTAs may become resident during the

@@ -57,12 +57,13 @@ def bumps(n, seed, count=6):
     return h.astype(F).ravel()
 
 
-@pytest.mark.parametrize("tile_width", [32, 64])
+@pytest.mark.parametrize("tile_width", [0, 32, 64])
 @pytest.mark.parametrize("nx,ny,edges", [(128, 96, (0, 0, 0, 0)), (130, 37, (0, 1, 1, 0)), (64, 64, (1, 1, 1, 1)),
                                          (200, 1, (0, 0, 0, 0))])
 def test_steps_are_bit_exact_against_the_oracle(nx, ny, edges, tile_width):
     """Every word of state, and the clock, equal the oracle's after each of 60 steps (TMA tiles when the row
-    pitch allows, plain loads otherwise; walls, open edges and a 1-D strip; both tile widths)."""
+    pitch allows, plain loads otherwise; walls, open edges and a 1-D strip; the column walk over strips (0) and
+    both widths of the staged tile kernel)."""
     h = bumps(max(nx, ny), 5)[: nx * ny] if ny > 1 else np.where(np.arange(nx) < nx // 2, 1.0, 0.0).astype(F)
     hu = np.zeros(nx * ny, F)
     hv = np.zeros(nx * ny, F)
@@ -167,28 +168,28 @@ def test_device_diagnostics_match_the_host_readout():
         assert d[6:] == [e.non_finite, e.negative, e.wet]
 
 
-def test_both_tile_widths_give_the_same_bits_on_a_large_grid():
-    """1024 x 1024 (the learned solver's coarse grid, where the width is chosen as 32): 20 steps at each width,
-    equal to the last bit, and the automatic choice is the narrow one there and the wide one at 2048 x 2048."""
+def test_every_step_kernel_gives_the_same_bits_on_a_large_grid():
+    """1024 x 1024 (the learned solver's coarse grid): 20 steps with the column walk over strips (the default) and
+    the staged tile kernel at both widths, equal to the last bit, with the same clock and fastest wave."""
     n = 1024
     h = bumps(n, 9, count=12)
     z = np.zeros(n * n, F)
     params = swe_params(9.81, 0.45, 1, 1, 1e-6).view(np.int32)
     out = []
-    for width in (64, 32):
+    for width in (0, 64, 32):
         with vf.PatchSimulation(n, n) as p:
-            assert p.tile_width() == 32
+            assert p.tile_width() == 0
             p.set_tile_width(width)
             assert p.tile_width() == width
             p.load(h, z, z, params)
             a = p.advance(2 ** 31 - 1, 20)
             assert a.steps == 20
             out.append((p.read(), p.fastest_wave(), p.now()))
-    for f in range(3):
-        assert np.array_equal(out[0][0][f].view(np.int32), out[1][0][f].view(np.int32)), f
-    assert out[0][1:] == out[1][1:]
-    with vf.PatchSimulation(2048, 2048) as p:
-        assert p.tile_width() == 64
+    for k in (1, 2):
+        for f in range(3):
+            assert np.array_equal(out[0][0][f].view(np.int32), out[k][0][f].view(np.int32)), (k, f)
+        assert out[0][1:] == out[k][1:]
+    with vf.PatchSimulation(64, 64) as p:
         with pytest.raises(vf.IllegalArgumentException):
             p.set_tile_width(48)
 
@@ -225,7 +226,7 @@ def test_overlapped_and_stream_ordered_launches_agree_to_the_bit():
     h = bumps(n, 11, count=12)
     z = np.zeros(n * n, F)
     params = swe_params(9.81, 0.45, 1, 1, 1e-6).view(np.int32)
-    for width in (32, 64):
+    for width in (0, 32, 64):
         out = []
         for overlap in (True, False):
             with vf.PatchSimulation(n, n) as p:

@@ -10,7 +10,7 @@
 // fused multiply-adds (written out as fmaf, since the file forbids contraction), one approximate reciprocal of a
 // cell's depth shared by its two velocities, one approximate reciprocal of each face's wave span shared by its
 // three fluxes, and an approximate square root for the wave speed; and it runs as a column walk in registers over
-// a TMA-staged tile (k_swe_strip_fast) instead of staging primitives and fluxes in shared memory. It is within a
+// a TMA-staged tile (k_swe_strip<false>) instead of staging primitives and fluxes in shared memory. It is within a
 // stated tolerance of the reference rather than equal to it, and the water still moves only between neighbours.
 // The tick count from the previous step's speed stays IEEE.
 //
@@ -466,8 +466,21 @@ __device__ __forceinline__ CellState ghost_y(CellState q, bool wall) {
     return q;
 }
 
-// One CTA's column walk (k_swe_strip_fast, step 2). INTERIOR: the tile and its halo lie inside the domain.
-template <bool INTERIOR>
+// A cell's state and primitives in the exact arithmetic (velocity, sqrtf: IEEE division and square root).
+__device__ __forceinline__ CellState cell_exact(float h, float qx, float qy, float g, float dry) {
+    CellState q;
+    q.h = h;
+    q.qx = qx;
+    q.qy = qy;
+    q.u = velocity(h, qx, dry);
+    q.v = velocity(h, qy, dry);
+    q.c = sqrtf(g * h);
+    return q;
+}
+
+// One CTA's column walk (k_swe_strip, step 2). INTERIOR: the tile and its halo lie inside the domain. EXACT: every
+// operation as the tile kernel rounds it (the reference's strict f32); otherwise the fast mode's arithmetic.
+template <bool INTERIOR, bool EXACT>
 __device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int x0, int y0, float g, float dry, float rx,
                                            float ry, int budget, int ticks, int& best, int& clamps) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -479,7 +492,8 @@ __device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int
     const bool wall_s = a.edge[2] == VF_EDGE_WALL, wall_n = a.edge[3] == VF_EDGE_WALL;
     auto load = [&](int r) {
         const int i = r * STRIP_BW + bc;
-        return cell_fast(S.box[0][i], S.box[1][i], S.box[2][i], g, dry);
+        return EXACT ? cell_exact(S.box[0][i], S.box[1][i], S.box[2][i], g, dry)
+                     : cell_fast(S.box[0][i], S.box[1][i], S.box[2][i], g, dry);
     };
     CellState prev = load(0);
     Face gs = {0.0f, 0.0f, 0.0f}, fw = {0.0f, 0.0f, 0.0f}, fe = {0.0f, 0.0f, 0.0f};
@@ -496,27 +510,48 @@ __device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int
             if (cx == 0) left = ghost_x(cur, wall_w);
             if (cx == nx) right = ghost_x(left, wall_e);
         }
-        // .x the y-face (normal y), .y the x-face (normal x)
-        const Face2 ff = hll_fast2(g, dry, f2(bot.h, left.h), f2(bot.qy, left.qx), f2(bot.qx, left.qy),
-                                   f2(bot.v, left.u), f2(bot.u, left.v), f2(bot.c, left.c), f2(top.h, right.h),
-                                   f2(top.qy, right.qx), f2(top.qx, right.qy), f2(top.v, right.u), f2(top.u, right.v),
-                                   f2(top.c, right.c));
-        const Face gn = {ff.mass.x, ff.normal.x, ff.tangent.x};
+        // the y-face (normal y) and the x-face (normal x); the fast mode pairs them, .x and .y
+        Face gn, fwn;
+        if (EXACT) {
+            gn = hll(g, dry, bot.h, bot.qy, bot.qx, bot.v, bot.u, bot.c, top.h, top.qy, top.qx, top.v, top.u, top.c);
+            fwn = hll(g, dry, left.h, left.qx, left.qy, left.u, left.v, left.c, right.h, right.qx, right.qy, right.u,
+                      right.v, right.c);
+        } else {
+            const Face2 ff = hll_fast2(g, dry, f2(bot.h, left.h), f2(bot.qy, left.qx), f2(bot.qx, left.qy),
+                                       f2(bot.v, left.u), f2(bot.u, left.v), f2(bot.c, left.c), f2(top.h, right.h),
+                                       f2(top.qy, right.qx), f2(top.qx, right.qy), f2(top.v, right.u),
+                                       f2(top.u, right.v), f2(top.c, right.c));
+            gn = Face{ff.mass.x, ff.normal.x, ff.tangent.x};
+            fwn = Face{ff.mass.y, ff.normal.y, ff.tangent.y};
+        }
         if (r >= 2) {
             // the update of row y-1 (ShallowWater.java:206-235) from its four faces
             const int yu = y - 1;
             if (own && (INTERIOR || yu < ny)) {
-                const float h = __fmaf_rn(-ry, gn.mass - gs.mass, __fmaf_rn(-rx, fe.mass - fw.mass, prev.h));
-                const float hu = __fmaf_rn(-ry, gn.tangent - gs.tangent, __fmaf_rn(-rx, fe.normal - fw.normal, prev.qx));
-                const float hv = __fmaf_rn(-ry, gn.normal - gs.normal, __fmaf_rn(-rx, fe.tangent - fw.tangent, prev.qy));
+                float h, hu, hv;
+                if (EXACT) {
+                    h = (prev.h - rx * (fe.mass - fw.mass)) - ry * (gn.mass - gs.mass);
+                    hu = (prev.qx - rx * (fe.normal - fw.normal)) - ry * (gn.tangent - gs.tangent);
+                    hv = (prev.qy - rx * (fe.tangent - fw.tangent)) - ry * (gn.normal - gs.normal);
+                } else {
+                    h = __fmaf_rn(-ry, gn.mass - gs.mass, __fmaf_rn(-rx, fe.mass - fw.mass, prev.h));
+                    hu = __fmaf_rn(-ry, gn.tangent - gs.tangent, __fmaf_rn(-rx, fe.normal - fw.normal, prev.qx));
+                    hv = __fmaf_rn(-ry, gn.normal - gs.normal, __fmaf_rn(-rx, fe.tangent - fw.tangent, prev.qy));
+                }
                 if (h < 0.0f) clamps++;
                 const float nh = fmaxf(h, 0.0f);
                 const int64_t c = (int64_t)yu * nx + cx;
                 a.out[0][c] = nh;
                 a.out[1][c] = hu;
                 a.out[2][c] = hv;
-                const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
-                const float speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
+                float speed;
+                if (EXACT) {
+                    const float u = velocity(nh, hu, dry), w = velocity(nh, hv, dry);
+                    speed = fmaxf(fabsf(u), fabsf(w)) + sqrtf(g * nh);
+                } else {
+                    const float inv = nh > dry ? __fdividef(1.0f, nh) : 0.0f;
+                    speed = fmaxf(fabsf(hu * inv), fabsf(hv * inv)) + sqrt_fast(g * nh);
+                }
                 best = max(best, __float_as_int(speed));
                 if (!INTERIOR && c == 0) {
                     *a.speed_clear = 0;
@@ -527,7 +562,7 @@ __device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int
         gs = gn;
         // this row's x-faces for its update at the next row: its own west face, and the right neighbour's west face
         // as its east face
-        fw = Face{ff.mass.y, ff.normal.y, ff.tangent.y};
+        fw = fwn;
         fe.mass = __shfl_down_sync(0xffffffffu, fw.mass, 1);
         fe.normal = __shfl_down_sync(0xffffffffu, fw.normal, 1);
         fe.tangent = __shfl_down_sync(0xffffffffu, fw.tangent, 1);
@@ -535,7 +570,8 @@ __device__ __forceinline__ void strip_walk(const SweArgs& a, StripShared& S, int
     }
 }
 
-__global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip_fast(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
+template <bool EXACT>
+__global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip(SweArgs a, const __grid_constant__ CUtensorMap tm_h,
                                                                     const __grid_constant__ CUtensorMap tm_hu,
                                                                     const __grid_constant__ CUtensorMap tm_hv) {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -597,9 +633,9 @@ __global__ void __launch_bounds__(STRIP_WARPS * 32) k_swe_strip_fast(SweArgs a, 
     int best = 0, clamps = 0;
     const bool interior = x0 >= 1 && x0 + STRIP_COLS + 1 <= nx && y0 >= 1 && y0 + STRIP_ROWS + 1 <= ny;
     if (interior)
-        strip_walk<true>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
+        strip_walk<true, EXACT>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
     else
-        strip_walk<false>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
+        strip_walk<false, EXACT>(a, S, x0, y0, g, dry, rx, ry, budget, ticks, best, clamps);
     // 3. the CTA's fastest wave and clamp count, one atomic each
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -747,13 +783,6 @@ bool make_map(CUtensorMap* m, const float* base, int nx, int ny, int hx, int hy)
     return r == CUDA_SUCCESS;
 }
 
-// 64-wide tiles unless they would give the GPU fewer than four tiles per resident slot (four CTAs of
-// SweShared<64> fit an SM): the last wave's imbalance then costs more than the narrower tile's halo.
-int auto_tile_width(int nx, int ny) {
-    const int64_t tiles = (int64_t)div_up(nx, 64) * div_up(ny, SWE_TY);
-    return tiles < (int64_t)16 * sm_count() ? 32 : 64;
-}
-
 }  // namespace
 
 // ------------------------------------------------------------------ the handle
@@ -770,7 +799,7 @@ struct vf_swe {
     CUtensorMap maps[2][2][3];   // [tile width 64, 32][state][field]
     CUtensorMap smaps[2][3];     // the fast mode's strip boxes: [state][field]
     bool tma = false;
-    int tile_w = 64;             // the tile width the steps use
+    int tile_w = 0;              // 0: the column walk over strips (k_swe_strip); 64 or 32: the staged tile kernel
     bool pdl = true;             // steps launched as programmatic dependents of the previous step
     bool exact = true;           // false: the fast mode's arithmetic (vf_swe_set_exact)
     // PatchSimulation.java:52-56
@@ -824,10 +853,11 @@ int32_t dispatch(vf_swe* h) {
     for (int e = 0; e < 4; e++) a.edge[e] = h->edges[e];
     a.use_tma = h->tma ? 1 : 0;
     const int wide = h->tile_w == 64;
-    CUtensorMap* m = h->exact ? h->maps[wide ? 0 : 1][si] : h->smaps[si];
+    const bool tile = h->exact && h->tile_w != 0;
+    CUtensorMap* m = tile ? h->maps[wide ? 0 : 1][si] : h->smaps[si];
     void* args[] = {&a, &m[0], &m[1], &m[2]};
     cudaLaunchConfig_t cfg = {};
-    if (h->exact) {
+    if (tile) {
         cfg.gridDim = dim3(div_up(h->nx, h->tile_w), div_up(h->ny, SWE_TY));
         cfg.blockDim = dim3(SWE_THREADS);
         cfg.dynamicSmemBytes = wide ? sizeof(SweShared<64>) + 128 : sizeof(SweShared<32>) + 128;
@@ -842,9 +872,9 @@ int32_t dispatch(vf_swe* h) {
     attr[0].val.programmaticStreamSerializationAllowed = h->pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void* fn = h->exact ? (wide ? (const void*)k_swe_tile<64> : (const void*)k_swe_tile<32>)
-                              : (const void*)k_swe_strip_fast;
-    h->prof.begin(h->exact ? "k_swe_tile" : "k_swe_strip_fast", h->stream);
+    const void* fn = tile ? (wide ? (const void*)k_swe_tile<64> : (const void*)k_swe_tile<32>)
+                          : h->exact ? (const void*)k_swe_strip<true> : (const void*)k_swe_strip<false>;
+    h->prof.begin(tile ? "k_swe_tile" : h->exact ? "k_swe_strip" : "k_swe_strip_fast", h->stream);
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     h->prof.end(h->stream);
     VF_TRY_CUDA(e);
@@ -937,7 +967,9 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
                              (int)sizeof(SweShared<64>) + 128) != cudaSuccess ||
         cudaFuncSetAttribute(k_swe_tile<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(SweShared<32>) + 128) != cudaSuccess ||
-        cudaFuncSetAttribute(k_swe_strip_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_swe_strip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(StripShared) + 128) != cudaSuccess ||
+        cudaFuncSetAttribute(k_swe_strip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(StripShared) + 128) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("cannot give the shallow-water kernel %zu bytes of shared memory", sizeof(SweShared<64>));
@@ -954,7 +986,7 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
         memset(h->maps, 0, sizeof h->maps);
         memset(h->smaps, 0, sizeof h->smaps);
     }
-    h->tile_w = auto_tile_width(nx, ny);
+    h->tile_w = 0;
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("clearing buffers failed");
@@ -1141,7 +1173,7 @@ int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
     VF_REQUIRE(width == 0 || width == 32 || width == 64, VF_EINVAL, "a tile is 32 or 64 cells wide (0: by grid size), got %d",
                width);
-    h->tile_w = width ? width : auto_tile_width(h->nx, h->ny);
+    h->tile_w = width;
     return VF_OK;
 }
 
