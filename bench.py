@@ -669,7 +669,7 @@ def run_swe(args, vf, dist, peak):
             p.read_budget(0)
             sp = p.profile_read()
             p.profile(False)
-        name = "k_swe_strip" if exact else "k_swe_strip_fast"
+        name = "k_swe_tile" if exact else "k_swe_strip_fast"
         k_ms = sp[name][0] / sp[name][1]
         achieved = 24.0 * cells / (k_ms / 1e3) / 1e9
         out["exact" if exact else "fast"] = {

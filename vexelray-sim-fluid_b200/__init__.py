@@ -1175,8 +1175,8 @@ class PatchSimulation:
         check(lib().vf_swe_write_budget(self._h, slot, ticks_))
 
     def set_tile_width(self, width: int) -> None:
-        """The step kernel: 0 (the default) the column walk over strips, 32 or 64 the staged tile kernel of that width.
-        Results do not depend on it."""
+        """The exact mode's step kernel: 64 (the default) or 32 the staged tile kernel of that width, 0 the column
+        walk over strips. Results do not depend on it."""
         check(lib().vf_swe_set_tile_width(self._h, width))
 
     def tile_width(self) -> int:

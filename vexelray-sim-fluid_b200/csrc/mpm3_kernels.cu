@@ -220,12 +220,14 @@ __global__ void __launch_bounds__(256) k_p2g3_warp(Step3 s) {
 //  1. A unit's 64 UZ cells are consecutive keys, so their particle runs form one contiguous range of the sort's
 //     permutation. The warp stages it in shared memory, puts each cell's run in ascending order there (the stable
 //     sort's fix-up, fused here: G2P then reads the stable permutation), and writes the range back.
-//  2. Cells are dealt to lanes from a queue ordered by particle count, largest first: a lane sums one whole cell's
-//     27 x 4 deposits in registers (loading two particles ahead), adds them into the warp's 10 x 10 x (UZ + 2) node
-//     window in shared memory when the cell is done, and takes the next cell. A cell's count varies (about
-//     8 +- 2.6 at 8 per cell), so one fixed cell per lane left half the lanes idle behind each warp's fullest cell;
-//     the queue keeps them busy. Lanes that finish together add at the same stencil offset into distinct cells'
-//     distinct nodes, so the window takes plain read-modify-writes, a warp sync between offsets.
+//  2. The unit's non-empty cells, ordered by particle count (largest first), go to the lanes in rounds of 32: a lane
+//     sums one whole cell's 27 x 4 deposits in registers (loading two particles ahead), and when the round's fullest
+//     cell is done all its lanes add their sums into the warp's 10 x 10 x (UZ + 2) node window in shared memory at
+//     once. A cell's count varies (about 8 +- 2.6 at 8 per cell); the ordering puts cells of like counts in one
+//     round, so few lanes wait. A round's lanes hold distinct cells, so at one stencil offset they add into distinct
+//     nodes: plain read-modify-writes, a warp sync between offsets. (Dealing cells from a queue instead, each lane
+//     taking the next cell as soon as its own was done, measured 1.3x slower at 8.2M particles: its lanes added
+//     into the window at scattered times, and that divergent add ran nearly every iteration.)
 //  3. The warp reduces every touched node of its window into the grid with one 16-byte vector
 //     reduction (red.global.add.v4.f32); neighbouring units' windows overlap, and the reductions add.
 //
@@ -237,10 +239,10 @@ constexpr int P2G_THREADS = 128;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
 // A work unit is UZ brick z-layers. One layer (8x8x1 cells, about 500 particles at 8 a cell) measured fastest at
 // every size: 0.54x the time of two layers at 17k particles, 0.91x at 2.9M, 0.95x at 7.2M (more units even out
-// the warps' queues and shorten their tails). Deeper units measured slower (4 layers: 2.6x at 8.2M).
+// the warps' loads and shorten their tails). Deeper units measured slower (4 layers: 2.6x at 8.2M).
 constexpr int WWX = WIN, WWY = WIN;
 constexpr int RUN_CAP = 2048;   // particle slots of one unit staged in shared memory (more: sorted in place)
-constexpr int NBUCKET = 32;     // count buckets of the cell queue (counts of 31 and more share the last)
+constexpr int NBUCKET = 32;     // count buckets of the cell order (counts of 31 and more share the last)
 
 template <int UZ>
 struct P2GUnit {
@@ -256,7 +258,6 @@ struct P2GShared {
     int start[P2G_WARPS][P2GUnit<UZ>::UCELLS + 1];    // cell c's particles: [start[c], start[c + 1])
     unsigned char order[P2G_WARPS][P2GUnit<UZ>::UCELLS];   // non-empty cells by descending count
     int bucket[P2G_WARPS][NBUCKET];
-    int next[P2G_WARPS];                 // the queue's head
 };
 // One particle's fields, as the scatter reads them.
 struct PIn {
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
         }
         const int* run = staged ? rs : perm + S0;   // the range, indexed from S0
 
-        // the queue: non-empty cells bucketed by count, largest first
+        // the order: non-empty cells by count, largest first, ascending cell within a count
         bucket[lane] = 0;
         for (int j = lane; j < WW; j += 32) ww[j] = make_float4(0, 0, 0, 0);
         __syncwarp();
@@ -370,6 +371,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
             if (n > 0) atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1);
         }
         __syncwarp();
+        int ncells;
         {
             int v = bucket[lane], x = v;   // exclusive scan over the buckets (largest counts first)
 #pragma unroll
@@ -378,125 +380,132 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
                 if (lane >= o) x += y;
             }
             bucket[lane] = x - v;
-            if (lane == 31) S.next[warp] = x;   // the number of non-empty cells, for now
+            ncells = __shfl_sync(ALL, x, 31);   // the number of non-empty cells
         }
         __syncwarp();
-        const int ncells = S.next[warp];
-        for (int c = lane; c < UCELLS; c += 32) {
+        for (int c0 = 0; c0 < UCELLS; c0 += 32) {   // UCELLS is a multiple of 32
+            const int c = c0 + lane;
             const int n = cstart[c + 1] - cstart[c];
-            if (n > 0) order[atomicAdd(&bucket[NBUCKET - 1 - min(n, NBUCKET - 1)], 1)] = (unsigned char)c;
+            const int key = n > 0 ? NBUCKET - 1 - min(n, NBUCKET - 1) : -1;
+            const unsigned peers = __match_any_sync(ALL, key);
+            const int base = key >= 0 ? bucket[key] : 0;
+            __syncwarp();
+            if (key >= 0) {
+                order[base + __popc(peers & ((1u << lane) - 1))] = (unsigned char)c;
+                if ((peers & ((1u << lane) - 1)) == 0) bucket[key] = base + __popc(peers);
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        if (lane == 0) S.next[warp] = 32;
-        __syncwarp();
 
-        // 2. cells from the queue, summed in registers, added into the window when done
+        // 2. the cells in rounds of 32 lanes, fullest first: a lane sums one cell's 27 x 4
+        // deposits in registers; a round's cells have similar counts, so its lanes finish together and add into the
+        // window together (distinct cells: distinct nodes at each stencil offset, a warp barrier between offsets)
         float2 acc01[27], acc23[27];   // per node (mass, x-momentum) and (y-, z-momentum)
+        for (int r0 = 0; r0 < ncells; r0 += 32) {
 #pragma unroll
-        for (int k = 0; k < 27; k++) acc01[k] = acc23[k] = make_float2(0.0f, 0.0f);
-        int cell = lane < ncells ? order[lane] : -1;
-        int i = 0, end = 0;
-        PIn nxt, nxt2;
-        auto open = [&]() {   // the lane's new cell: its range and the first two particles in flight
-            i = cstart[cell];
-            end = cstart[cell + 1];
-            load_pin(nxt, in, st, checked_src(run, i - S0, s.np, s.status));
-            if (i + 1 < end) load_pin(nxt2, in, st, checked_src(run, i + 1 - S0, s.np, s.status));
-        };
-        if (cell >= 0) open();
-        while (__any_sync(ALL, cell >= 0)) {
-            if (cell >= 0 && i < end) {
-                const PIn qq = nxt;
-                nxt = nxt2;
-                if (i + 2 < end) load_pin(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
-                i++;
-                int cl[3];
-                float f[3];
-                stencil_axis(qq.x, dm.nx, cl[0], f[0]);
-                stencil_axis(qq.y, dm.ny, cl[1], f[1]);
-                stencil_axis(qq.z, dm.nz, cl[2], f[2]);
-                const bool mine = cl[0] == cx0 + (cell & 7) && cl[1] == cy0 + ((cell >> 3) & 7) && cl[2] == cz0 + (cell >> 6);
-                if (!mine) set_status(s.status, ST_OOB);
-                if (mine && qq.m > 0.0f) {
-                    float wx[3], wy[3], wz[3];
-#pragma unroll
-                    for (int e = 0; e < 3; e++) {
-                        float* we = e == 0 ? wx : e == 1 ? wy : wz;
-                        const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
-                        we[0] = 0.5f * (ta * ta);
-                        we[1] = 0.75f - tc * tc;
-                        we[2] = 0.5f * (te * te);
-                    }
-                    float jp;
-                    if (p.tait) {
-                        const float r = __frcp_rn(qq.j), r2 = r * r;
-                        jp = p.bulk * ((r2 * r2) * r2 - qq.j);
-                    } else {
-                        jp = p.bulk * (1.0f - qq.j);
-                    }
-                    const float sp = (k4dt * (qq.m * vol)) * jp;
-                    const float vel[3] = {qq.u, qq.v, qq.w};
-                    float A[3], B[3][3];
-#pragma unroll
-                    for (int r = 0; r < 3; r++) {
-                        const float c0 = qq.c[3 * r], c1 = qq.c[3 * r + 1], c2 = qq.c[3 * r + 2];
-                        A[r] = qq.m * (vel[r] - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[r];
-                        B[r][0] = qq.m * c0;
-                        B[r][1] = qq.m * c1;
-                        B[r][2] = qq.m * c2;
-                        B[r][r] += sp;
-                    }
-                    // paired fp32 (FFMA2): a node's (mass, x-momentum) += wx (m wyz, wyz M_x) and (y-, z-momentum)
-                    // += wx (wyz M_y, wyz M_z), M_a = T_a + ox B_a0, T_a = A_a + oy B_a1 + oz B_a2; the mass lane
-                    // rides along with zero coefficients
-                    const float2 c01 = make_float2(qq.m, A[0]), c23 = make_float2(A[1], A[2]);
-                    const float2 b0_01 = make_float2(0.0f, B[0][0]), b0_23 = make_float2(B[1][0], B[2][0]);
-                    const float2 b1_01 = make_float2(0.0f, B[0][1]), b1_23 = make_float2(B[1][1], B[2][1]);
-                    const float2 b2_01 = make_float2(0.0f, B[0][2]), b2_23 = make_float2(B[1][2], B[2][2]);
-#pragma unroll
-                    for (int oz = 0; oz < 3; oz++) {
-#pragma unroll
-                        for (int oy = 0; oy < 3; oy++) {
-                            const float wyz = wy[oy] * wz[oz];
-                            const float2 w2 = make_float2(wyz, wyz);
-                            float2 t01 = c01, t23 = c23;
-                            if (oy) {
-                                const float2 f2 = make_float2((float)oy, (float)oy);
-                                t01 = __ffma2_rn(f2, b1_01, t01);
-                                t23 = __ffma2_rn(f2, b1_23, t23);
-                            }
-                            if (oz) {
-                                const float2 f2 = make_float2((float)oz, (float)oz);
-                                t01 = __ffma2_rn(f2, b2_01, t01);
-                                t23 = __ffma2_rn(f2, b2_23, t23);
-                            }
-                            const float2 g01 = __fmul2_rn(w2, t01), g23 = __fmul2_rn(w2, t23);
-                            const float2 h01 = __fmul2_rn(w2, b0_01), h23 = __fmul2_rn(w2, b0_23);
-#pragma unroll
-                            for (int ox = 0; ox < 3; ox++) {
-                                const int kk = (oz * 3 + oy) * 3 + ox;
-                                float2 q01 = g01, q23 = g23;
-                                if (ox == 1) {
-                                    q01 = __fadd2_rn(q01, h01);
-                                    q23 = __fadd2_rn(q23, h23);
-                                } else if (ox == 2) {
-                                    const float2 two = make_float2(2.0f, 2.0f);
-                                    q01 = __ffma2_rn(two, h01, q01);
-                                    q23 = __ffma2_rn(two, h23, q23);
+            for (int k = 0; k < 27; k++) acc01[k] = acc23[k] = make_float2(0.0f, 0.0f);
+            const int cell = r0 + lane < ncells ? order[r0 + lane] : -1;
+            int i = 0, end = 0;
+            PIn nxt, nxt2;
+            if (cell >= 0) {
+                i = cstart[cell];
+                end = cstart[cell + 1];
+                load_pin(nxt, in, st, checked_src(run, i - S0, s.np, s.status));
+                if (i + 1 < end) load_pin(nxt2, in, st, checked_src(run, i + 1 - S0, s.np, s.status));
+            }
+            const int steps = (int)__reduce_max_sync(ALL, (unsigned)(end - i));
+            for (int t = 0; t < steps; t++) {
+                if (i < end) {
+                    const PIn qq = nxt;
+                    nxt = nxt2;
+                    if (i + 2 < end) load_pin(nxt2, in, st, checked_src(run, i + 2 - S0, s.np, s.status));
+                    i++;
+                    int cl[3];
+                    float f[3];
+                    stencil_axis(qq.x, dm.nx, cl[0], f[0]);
+                    stencil_axis(qq.y, dm.ny, cl[1], f[1]);
+                    stencil_axis(qq.z, dm.nz, cl[2], f[2]);
+                    const bool mine = cl[0] == cx0 + (cell & 7) && cl[1] == cy0 + ((cell >> 3) & 7) && cl[2] == cz0 + (cell >> 6);
+                    if (!mine) set_status(s.status, ST_OOB);
+                    if (mine && qq.m > 0.0f) {
+                        float wx[3], wy[3], wz[3];
+    #pragma unroll
+                        for (int e = 0; e < 3; e++) {
+                            float* we = e == 0 ? wx : e == 1 ? wy : wz;
+                            const float ta = 1.5f - f[e], tc = f[e] - 1.0f, te = f[e] - 0.5f;
+                            we[0] = 0.5f * (ta * ta);
+                            we[1] = 0.75f - tc * tc;
+                            we[2] = 0.5f * (te * te);
+                        }
+                        float jp;
+                        if (p.tait) {
+                            const float r = __frcp_rn(qq.j), r2 = r * r;
+                            jp = p.bulk * ((r2 * r2) * r2 - qq.j);
+                        } else {
+                            jp = p.bulk * (1.0f - qq.j);
+                        }
+                        const float sp = (k4dt * (qq.m * vol)) * jp;
+                        const float vel[3] = {qq.u, qq.v, qq.w};
+                        float A[3], B[3][3];
+    #pragma unroll
+                        for (int r = 0; r < 3; r++) {
+                            const float c0 = qq.c[3 * r], c1 = qq.c[3 * r + 1], c2 = qq.c[3 * r + 2];
+                            A[r] = qq.m * (vel[r] - (c0 * f[0] + c1 * f[1] + c2 * f[2])) - sp * f[r];
+                            B[r][0] = qq.m * c0;
+                            B[r][1] = qq.m * c1;
+                            B[r][2] = qq.m * c2;
+                            B[r][r] += sp;
+                        }
+                        // paired fp32 (FFMA2): a node's (mass, x-momentum) += wx (m wyz, wyz M_x) and (y-, z-momentum)
+                        // += wx (wyz M_y, wyz M_z), M_a = T_a + ox B_a0, T_a = A_a + oy B_a1 + oz B_a2; the mass lane
+                        // rides along with zero coefficients
+                        const float2 c01 = make_float2(qq.m, A[0]), c23 = make_float2(A[1], A[2]);
+                        const float2 b0_01 = make_float2(0.0f, B[0][0]), b0_23 = make_float2(B[1][0], B[2][0]);
+                        const float2 b1_01 = make_float2(0.0f, B[0][1]), b1_23 = make_float2(B[1][1], B[2][1]);
+                        const float2 b2_01 = make_float2(0.0f, B[0][2]), b2_23 = make_float2(B[1][2], B[2][2]);
+    #pragma unroll
+                        for (int oz = 0; oz < 3; oz++) {
+    #pragma unroll
+                            for (int oy = 0; oy < 3; oy++) {
+                                const float wyz = wy[oy] * wz[oz];
+                                const float2 w2 = make_float2(wyz, wyz);
+                                float2 t01 = c01, t23 = c23;
+                                if (oy) {
+                                    const float2 f2 = make_float2((float)oy, (float)oy);
+                                    t01 = __ffma2_rn(f2, b1_01, t01);
+                                    t23 = __ffma2_rn(f2, b1_23, t23);
                                 }
-                                const float2 x2 = make_float2(wx[ox], wx[ox]);
-                                acc01[kk] = __ffma2_rn(x2, q01, acc01[kk]);
-                                acc23[kk] = __ffma2_rn(x2, q23, acc23[kk]);
+                                if (oz) {
+                                    const float2 f2 = make_float2((float)oz, (float)oz);
+                                    t01 = __ffma2_rn(f2, b2_01, t01);
+                                    t23 = __ffma2_rn(f2, b2_23, t23);
+                                }
+                                const float2 g01 = __fmul2_rn(w2, t01), g23 = __fmul2_rn(w2, t23);
+                                const float2 h01 = __fmul2_rn(w2, b0_01), h23 = __fmul2_rn(w2, b0_23);
+    #pragma unroll
+                                for (int ox = 0; ox < 3; ox++) {
+                                    const int kk = (oz * 3 + oy) * 3 + ox;
+                                    float2 q01 = g01, q23 = g23;
+                                    if (ox == 1) {
+                                        q01 = __fadd2_rn(q01, h01);
+                                        q23 = __fadd2_rn(q23, h23);
+                                    } else if (ox == 2) {
+                                        const float2 two = make_float2(2.0f, 2.0f);
+                                        q01 = __ffma2_rn(two, h01, q01);
+                                        q23 = __ffma2_rn(two, h23, q23);
+                                    }
+                                    const float2 x2 = make_float2(wx[ox], wx[ox]);
+                                    acc01[kk] = __ffma2_rn(x2, q01, acc01[kk]);
+                                    acc23[kk] = __ffma2_rn(x2, q23, acc23[kk]);
+                                }
                             }
                         }
                     }
+
                 }
             }
-            const bool done = cell >= 0 && i >= end;
-            const unsigned fm = __ballot_sync(ALL, done);
-            if (done) {
-                // into the window: lanes flushing together hold distinct cells, so at one stencil offset they
-                // write distinct nodes
+            const unsigned fm = __ballot_sync(ALL, cell >= 0);
+            if (cell >= 0) {
                 const int wb = ((cell >> 6) * WWY + ((cell >> 3) & 7)) * WWX + (cell & 7);
 #pragma unroll
                 for (int k = 0; k < 27; k++) {
@@ -508,17 +517,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g3_tile(Step3 s) {
                     v.z += acc23[k].x;
                     v.w += acc23[k].y;
                     ww[wi] = v;
-                    acc01[k] = acc23[k] = make_float2(0.0f, 0.0f);
                     __syncwarp(fm);
                 }
-                const int pos = atomicAdd(&S.next[warp], 1);
-                cell = pos < ncells ? order[pos] : -1;
-                if (cell >= 0) open();
             }
-            __syncwarp();   // this iteration's window writes before the next iteration's reads
+            __syncwarp();
         }
         __syncwarp();
-
         // 3. the window's touched nodes into the grid
         for (int j = lane; j < WW; j += 32) {
             const float4 t = ww[j];

@@ -12,9 +12,10 @@
 // three fluxes, and an approximate square root for the wave speed; and it runs as a column walk in registers over
 // a TMA-staged tile (k_swe_strip<false>) instead of staging primitives and fluxes in shared memory. It is within a
 // stated tolerance of the reference rather than equal to it, and the water still moves only between neighbours.
-// The tick count from the previous step's speed stays IEEE.
+// The tick count from the previous step's speed stays IEEE. The exact mode can walk strips too
+// (vf_swe_set_tile_width(h, 0), k_swe_strip<true>): bit-identical, and measured slower than the tile below.
 //
-// One CTA per 64 x 16 tile of cells:
+// One CTA per 64 x 16 tile of cells (k_swe_tile):
 //   1. the tile and a one-cell halo of h, hu, hv land in shared memory by three 2D TMA loads
 //      (the box starts four cells left of the tile so its x coordinate is 16-byte aligned);
 //   2. per cell of tile+halo: u = hu/h, v = hv/h (0 when dry) and c = sqrt(g h), once;
@@ -35,7 +36,7 @@ using namespace vf;
 
 namespace {
 
-// A tile is TX x 16 cells, TX = 64, or 32 on grids too small to fill the GPU with 64-wide tiles.
+// A tile is TX x 16 cells, TX = 64 (the default) or 32 (vf_swe_set_tile_width).
 template <int TX_>
 struct Tile {
     static constexpr int TX = TX_, TY = 16;
@@ -109,34 +110,8 @@ __device__ __forceinline__ Face hll(float g, float dry, float hL, float qnL, flo
 __device__ __forceinline__ float velocity(float h, float q, float dry) { return h > dry ? q / h : 0.0f; }
 
 // The fast mode's HLL: the same wave speeds and flux form as hll(), the division by the span done once as an
-// approximate reciprocal, and the products fused.
-__device__ __forceinline__ Face hll_fast(float g, float dry, float hL, float qnL, float qtL, float unL, float utL,
-                                         float cL, float hR, float qnR, float qtR, float unR, float utR, float cR) {
-    float sL = fminf(unL - cL, unR - cR);
-    float sR = fmaxf(unL + cL, unR + cR);
-    if (!(hR > dry)) {
-        sL = unL - cL;
-        sR = __fmaf_rn(2.0f, cL, unL);
-    }
-    if (!(hL > dry)) {
-        sL = __fmaf_rn(-2.0f, cR, unR);
-        sR = unR + cR;
-    }
-    const float lo = fminf(sL, 0.0f);
-    const float hi = fmaxf(sR, 0.0f);
-    const float inv = __fdividef(1.0f, fmaxf(hi - lo, 1e-30f));
-    const float lohi = lo * hi;
-    const float hg = 0.5f * g;
-    const float pL = hg * (hL * hL), pR = hg * (hR * hR);
-    Face f;
-    f.mass = __fmaf_rn(lohi, hR - hL, __fmaf_rn(hi, qnL, -lo * qnR)) * inv;
-    f.normal = __fmaf_rn(lohi, qnR - qnL, __fmaf_rn(hi, __fmaf_rn(qnL, unL, pL), -lo * __fmaf_rn(qnR, unR, pR))) * inv;
-    f.tangent = __fmaf_rn(lohi, qtR - qtL, __fmaf_rn(hi * qnL, utL, -(lo * qnR) * utR)) * inv;
-    return f;
-}
-
-// Two faces of the fast mode's HLL at once, one in each half of paired fp32 (FFMA2/FADD2/FMUL2): the column walk's
-// x-face and y-face of a row, which are independent.
+// approximate reciprocal and the products fused; two faces at once, one in each half of paired fp32
+// (FFMA2/FADD2/FMUL2): the column walk's x-face and y-face of a row, which are independent.
 struct Face2 {
     float2 mass, normal, tangent;
 };
@@ -799,7 +774,7 @@ struct vf_swe {
     CUtensorMap maps[2][2][3];   // [tile width 64, 32][state][field]
     CUtensorMap smaps[2][3];     // the fast mode's strip boxes: [state][field]
     bool tma = false;
-    int tile_w = 0;              // 0: the column walk over strips (k_swe_strip); 64 or 32: the staged tile kernel
+    int tile_w = 64;             // 64 or 32: the staged tile kernel; 0: the column walk over strips (k_swe_strip)
     bool pdl = true;             // steps launched as programmatic dependents of the previous step
     bool exact = true;           // false: the fast mode's arithmetic (vf_swe_set_exact)
     // PatchSimulation.java:52-56
@@ -986,7 +961,7 @@ int32_t vf_swe_create(int32_t nx, int32_t ny, const int32_t edges[4], vf_swe** o
         memset(h->maps, 0, sizeof h->maps);
         memset(h->smaps, 0, sizeof h->smaps);
     }
-    h->tile_w = 0;
+    h->tile_w = 64;
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
         vf_swe_destroy(h);
         set_error("clearing buffers failed");
@@ -1171,7 +1146,7 @@ int32_t vf_swe_restore(vf_swe* h, const void* buf, int64_t size) {
 
 int32_t vf_swe_set_tile_width(vf_swe* h, int32_t width) {
     VF_REQUIRE(h, VF_EINVAL, "null handle");
-    VF_REQUIRE(width == 0 || width == 32 || width == 64, VF_EINVAL, "a tile is 32 or 64 cells wide (0: by grid size), got %d",
+    VF_REQUIRE(width == 0 || width == 32 || width == 64, VF_EINVAL, "a tile is 32 or 64 cells wide (0: strips), got %d",
                width);
     h->tile_w = width;
     return VF_OK;
