@@ -91,7 +91,6 @@ def dam3(box=BOX3):
 def swe_bumps(n=N_SWE):
     """The shallow-water config: h = 1 + 16 seeded Gaussian bumps (amplitude U(0.1,0.5), sigma U(20,200)
     cells, centres uniform), hu = hv = 0."""
-    n = N_SWE
     rng = np.random.default_rng(SEED_SWE)
     h = np.ones((n, n), np.float32)
     y = np.arange(n, dtype=np.float32)[:, None]
