@@ -40,7 +40,7 @@ struct vf_mpm3 {
     DeviceBuffer cell_count, cell_start, cursor;
     DeviceBuffer brick_count, brick_start;
     DeviceBuffer active[2];   // the non-empty bricks of the step that scattered into grid[g]
-    DeviceBuffer n_active;    // int[2]
+    DeviceBuffer n_active;    // int[4]: the non-empty bricks of each list, then each list's gather item counter
     DeviceBuffer grid[2];
     DeviceBuffer vel;
     DeviceBuffer params;
@@ -335,6 +335,7 @@ int32_t run_passes(vf_mpm3* h, uint32_t mask, bool count_next) {
                 if ((rc = grid_pass(h, s, g))) return rc;
                 s.vel_ready = 1;
             }
+            s.work = h->n_active.as<int>() + 2 + g;
             VF_LAUNCH(h->prof, "k_g2p3_tile", h->stream, k_g2p3_tile, persistent_blocks(4), 256, 0, s);
         } else {
             if ((rc = grid_pass(h, s, g))) return rc;
@@ -617,7 +618,7 @@ int32_t prepare3(int32_t nx, int32_t ny, int32_t nz, int32_t particles, uint32_t
         (rc = h->brick_count.alloc((size_t)h->nbricks * 4)) ||
         (rc = h->brick_start.alloc((size_t)(h->nbricks + 1) * 4)) ||
         (rc = h->active[0].alloc((size_t)h->nbricks * 4)) || (rc = h->active[1].alloc((size_t)h->nbricks * 4)) ||
-        (rc = h->n_active.alloc(2 * sizeof(int))) || (rc = h->grid[0].alloc(grid_bytes)) ||
+        (rc = h->n_active.alloc(4 * sizeof(int))) || (rc = h->grid[0].alloc(grid_bytes)) ||
         (rc = h->grid[1].alloc(grid_bytes)) || (!h->sparse && (rc = h->vel.alloc((size_t)h->nodes * 16))) ||
         (rc = h->params.alloc(sizeof(Params3))) || (rc = h->status.alloc(64)) || (rc = h->scratch.alloc(64)) ||
         (rc = h->nominal.alloc(16)))

@@ -669,57 +669,101 @@ __global__ void __launch_bounds__(256) k_g2p3(Step3 s) {
 
 // ------------------------------------------------------------------ G2P (brick tile, fused grid update)
 
-// One CTA per non-empty brick. The brick's 10^3 node window is read once from HBM and turned into
-// velocities in shared memory (the grid update, Flip3.grid, fused: no velocity grid in HBM), then
-// each particle of the brick gathers its 27 nodes from shared memory. The gather is regrouped per
-// row of three nodes along x:
+// Work items are bricks (or, in scenes of few bricks, slices of a brick's particles), taken by the CTAs from a
+// counter in device memory (s.work, zeroed by the sort's brick scan): a CTA that finishes a small brick takes the
+// next one, so the kernel ends when the work does rather than when the CTA dealt the most bricks does. A CTA
+// takes its next item while it gathers the current one, and reads that item's brick and particle range then too.
+//
+// Per item the brick's 10^3 node window is read once from HBM and turned into velocities in shared memory (the grid
+// update, Flip3.grid, fused: no velocity grid in HBM); the window's node loads are issued together, and the item's
+// first particles' permutation entries and fields are requested before the window is computed, so the item starts
+// after about two memory round trips. Then each particle of the brick gathers its 27 nodes from shared memory.
+// The gather is regrouped per row of three nodes along x:
 //   r0_a = sum_ox wx v_a,  rx_a = wx1 v_a(1) + 2 wx2 v_a(2),
 //   vel_a = sum wyz r0_a,  S_ax = sum wyz rx_a,  S_ay = sum oy wyz r0_a,  S_az = sum oz wyz r0_a,
 //   C_ae = 4 (S_ae - f_e vel_a)      (= 4 sum w v_a (o_e - f_e), Flip3.java:349-365).
 constexpr int G2P_THREADS = 256;
+constexpr int G2P_WLOADS = (WIN3 + G2P_THREADS - 1) / G2P_THREADS;   // window nodes a thread loads
+
+// An item's brick and particle range, clamped into [0, np].
+struct G2PItem {
+    int b, bs, be;
+};
+
+__device__ __forceinline__ G2PItem g2p_item(const Step3& s, int a, int split) {
+    G2PItem t;
+    t.b = s.active[a / split];
+    int bs = s.brick_start[t.b], be = s.brick_start[t.b + 1];
+    if (bs < 0 || be > s.np || be < bs) {
+        set_status(s.status, ST_OOB);
+        bs = max(bs, 0);
+        be = min(max(be, bs), s.np);
+    }
+    if (split > 1) {   // this item's slice of the brick's particles
+        const int part = a % split;
+        const int64_t len = be - bs;
+        const int e = bs + (int)(len * (part + 1) / split);
+        bs = bs + (int)(len * part / split);
+        be = e;
+    }
+    t.bs = bs;
+    t.be = be;
+    return t;
+}
 
 __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p3_tile(Step3 s) {
     __shared__ float4 vwin[WIN3];
+    __shared__ int4 next_item[2];   // {item, brick, start, end} of a CTA's next item, double-buffered
     const Params3 p = *s.params;
     const Dims3 dm = s.d;
     const int64_t st = s.stride;
-    const int na = *s.n_active;
+    const int tid = threadIdx.x;
     const int split = max(s.g2p_split, 1);
-    for (int a = blockIdx.x; a < na * split; a += gridDim.x) {
-        const int b = s.active[a / split], part = a % split;
+    const int items = *s.n_active * split;
+    if (tid == 0) {
+        const int a = atomicAdd(s.work, 1);
+        int4 v = make_int4(a, 0, 0, 0);
+        if (a < items) {
+            const G2PItem t = g2p_item(s, a, split);
+            v = make_int4(a, t.b, t.bs, t.be);
+        }
+        next_item[0] = v;
+    }
+    __syncthreads();
+    for (int slot = 0;; slot ^= 1) {
+        const int4 cur = next_item[slot];
+        if (cur.x >= items) break;   // uniform: every thread read the same entry after a barrier
+        // the next item, claimed now and read while this one is gathered
+        int nxt = 0;
+        if (tid == 0) nxt = atomicAdd(s.work, 1);
+        const int b = cur.y, bs = cur.z, be = cur.w;
         const int bx = b % dm.nbx, by = (b / dm.nbx) % dm.nby, bz = b / (dm.nbx * dm.nby);
         const int cx0 = bx * BRICK, cy0 = by * BRICK, cz0 = bz * BRICK;
-        for (int wi = threadIdx.x; wi < WIN3; wi += G2P_THREADS) {
+        // the window's node loads, all issued before any is used
+        float4 raw[G2P_WLOADS];
+        bool have[G2P_WLOADS];
+#pragma unroll
+        for (int q = 0; q < G2P_WLOADS; q++) {
+            const int wi = tid + q * G2P_THREADS;
             const int gx = cx0 + wi % WIN, gy = cy0 + (wi / WIN) % WIN, gz = cz0 + wi / (WIN * WIN);
-            float4 v = make_float4(0, 0, 0, 0);
-            if (gx < dm.nx && gy < dm.ny && gz < dm.nz) {
+            raw[q] = make_float4(0, 0, 0, 0);
+            have[q] = false;
+            if (wi < WIN3 && gx < dm.nx && gy < dm.ny && gz < dm.nz) {
                 if (s.vel_ready) {
-                    v = s.vel[((int64_t)gz * dm.ny + gy) * dm.nx + gx];
+                    raw[q] = s.vel[((int64_t)gz * dm.ny + gy) * dm.nx + gx];
+                    have[q] = true;
                 } else if (const float4* node = node_addr(s, gx, gy, gz)) {
-                    const float3 u = grid_velocity(*node, gx, gy, gz, dm, p);
-                    v = make_float4(u.x, u.y, u.z, 0.0f);
+                    raw[q] = *node;
+                    have[q] = true;
                 } else {
                     set_status(s.status, ST_POOL);
                 }
             }
-            vwin[wi] = v;
-        }
-        __syncthreads();
-        int bs = s.brick_start[b], be = s.brick_start[b + 1];
-        if (bs < 0 || be > s.np || be < bs) {
-            set_status(s.status, ST_OOB);
-            bs = max(bs, 0);
-            be = min(max(be, bs), s.np);
-        }
-        if (split > 1) {   // this item's slice of the brick's particles
-            const int64_t len = be - bs;
-            be = bs + (int)(len * (part + 1) / split);
-            bs = bs + (int)(len * part / split);
         }
         // Every thread walks the same number of iterations so the warp-level count is converged. The
         // permutation is read two iterations ahead and the particle one iteration ahead of its use.
         const int iters = (be - bs + G2P_THREADS - 1) / G2P_THREADS;
-        const int d0 = bs + threadIdx.x;
+        const int d0 = bs + tid;
         auto src_of = [&](int d) {
             int v = d < be ? (s.perm ? s.perm[d] : d) : -1;
             if (d < be && (unsigned)v >= (unsigned)s.np) {
@@ -738,6 +782,33 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p3_tile(Step3 s) {
             nm_ = s.in[M * st + src_a];
             nj_ = s.in[J * st + src_a];
         }
+        // the window's velocities
+#pragma unroll
+        for (int q = 0; q < G2P_WLOADS; q++) {
+            const int wi = tid + q * G2P_THREADS;
+            if (wi < WIN3) {
+                float4 v = make_float4(0, 0, 0, 0);
+                if (have[q]) {
+                    if (s.vel_ready) {
+                        v = raw[q];
+                    } else {
+                        const int gx = cx0 + wi % WIN, gy = cy0 + (wi / WIN) % WIN, gz = cz0 + wi / (WIN * WIN);
+                        const float3 u = grid_velocity(raw[q], gx, gy, gz, dm, p);
+                        v = make_float4(u.x, u.y, u.z, 0.0f);
+                    }
+                }
+                vwin[wi] = v;
+            }
+        }
+        if (tid == 0) {   // the next item's brick and range (its claim has had the window loads' time to return)
+            int4 v = make_int4(nxt, 0, 0, 0);
+            if (nxt < items) {
+                const G2PItem t = g2p_item(s, nxt, split);
+                v = make_int4(nxt, t.b, t.bs, t.be);
+            }
+            next_item[slot ^ 1] = v;
+        }
+        __syncthreads();
         for (int it = 0; it < iters; it++) {
             const int d = d0 + it * G2P_THREADS;
             const bool valid = d < be && src_a >= 0;
@@ -813,7 +884,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p3_tile(Step3 s) {
             }
             g2p_count(s, d, valid, pos);
         }
-        __syncthreads();
+        __syncthreads();   // the window is free, and next_item[slot ^ 1] is visible
     }
 }
 

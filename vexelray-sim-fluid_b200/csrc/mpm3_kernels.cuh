@@ -134,6 +134,7 @@ struct Step3 {
     const int* brick_start;
     const int* active;
     const int* n_active;
+    int* work;              // the tiled G2P's item counter (zeroed by the brick scan that made `active`)
     int64_t nkeys;
     int nbricks;
     int count_next;         // G2P also counts keys for the next step's sort

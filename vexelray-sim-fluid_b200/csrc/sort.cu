@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(1024) k_brick_scan(int* __restrict__ brick_cou
     }
     if (threadIdx.x == 0) {
         brick_start[nb] = total;
-        *n_active = total_live;
+        n_active[0] = total_live;
+        n_active[2] = 0;   // the tiled gather's item counter for this list
     }
 }
 

@@ -108,7 +108,8 @@ __device__ __forceinline__ int block_exclusive(int v, int* smem, int* total) {
 __global__ void k_scan_single(int* __restrict__ counts, int* __restrict__ starts, int64_t n);
 
 // The 3D brick level: brick_count[nb] -> brick_start[nb+1], the list of non-empty bricks in
-// index order (active[0..*n_active)), brick_count zeroed. One block of 1024 threads.
+// index order (active[0..*n_active)), brick_count zeroed, and n_active[2] (the tiled gather's item counter for
+// this list) zeroed. One block of 1024 threads.
 __global__ void k_brick_scan(int* __restrict__ brick_count, int* __restrict__ brick_start,
                              int* __restrict__ active, int* __restrict__ n_active, int nb);
 
