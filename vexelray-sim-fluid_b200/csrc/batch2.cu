@@ -22,7 +22,7 @@
 //                    into chunks of at most CHUNK particles, counted per scene
 //   2  cell scan     a warp per non-empty tile: cell counts -> cursors (cell starts), counts zeroed; CTA 0 lays
 //                    the scenes' chunks out one after another
-//   3  permute       per slot: perm[cursor[key]++] = slot, one cursor bump per distinct key of a warp. Within a
+//   3  permute       per slot: perm[cursor[key]++] = slot, one cursor bump per run of equal keys of a warp. Within a
 //                    cell the order is the atomics' (unspecified, as in the reference's CountingSort,
 //                    SortTest.java:121-134); what the scatter needs is each cell's particles contiguous. The
 //                    chunks enter the item list, and the other parity's grid is cleared over the windows of
@@ -251,34 +251,50 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
     if (!grid_barrier(B.bar, B.status)) return;
     phase_done(1);
 
-    // ---- 3. permute: perm[cursor[key]++] = slot, four slots per thread, one cursor bump per distinct key of a
-    // warp (the order within a cell is the atomics' order: unspecified, as in the reference's CountingSort); the
+    // ---- 3. permute: perm[cursor[key]++] = slot, eight slots per thread, one cursor bump per run of equal keys of
+    // a warp (the order within a cell is the atomics' order: unspecified, as in the reference's CountingSort); the
     // tiles' chunks entered in the item list; and the other parity's grid cleared over the windows of the tiles
     // the previous step scattered into
     {
+        // PK slots a thread (a warp's slots consecutive), the next iteration's keys read while this one's atomics
+        // are in flight
+        constexpr int PK = 8;
         const int n32 = (B.np + 31) & ~31;
         const int stride = gridDim.x * blockDim.x;
-        for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n32; i0 += 4 * stride) {
-            int k[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int i = i0 + u * stride;
-                k[u] = i < B.np ? B.key[i] : -1;
-                if (i < B.np && (k[u] < 0 || k[u] >= B.ncells)) {
-                    set_status(B.status, ST_OOB);
-                    k[u] = -1;
-                }
+        auto key_at = [&](int i) {
+            int v = i < B.np ? B.key[i] : -1;
+            if (i < B.np && (v < 0 || v >= B.ncells)) {
+                set_status(B.status, ST_OOB);
+                v = -1;
             }
-            int base[4], rank[4], leader[4];
+            return v;
+        };
+        int kn[PK];
+        const int first = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
-            for (int u = 0; u < 4; u++) {   // the atomics of the four slots in flight together
-                const unsigned peers = __match_any_sync(0xffffffffu, k[u]);
-                leader[u] = __ffs(peers) - 1;
-                rank[u] = __popc(peers & ((1u << lane) - 1u));
-                base[u] = (lane == leader[u] && k[u] >= 0) ? atomicAdd(&B.cursor[k[u]], __popc(peers)) : 0;
+        for (int u = 0; u < PK; u++) kn[u] = key_at(first + u * stride);
+        for (int i0 = first; i0 < n32; i0 += PK * stride) {
+            int k[PK];
+#pragma unroll
+            for (int u = 0; u < PK; u++) {
+                k[u] = kn[u];
+                kn[u] = key_at(i0 + (PK + u) * stride);
+            }
+            // the slots of a warp are consecutive, and in the last step's sorted order their keys come in runs:
+            // one cursor bump per run of equal keys (a key in two runs of the warp takes two, with distinct ranks)
+            int base[PK], rank[PK], leader[PK];
+#pragma unroll
+            for (int u = 0; u < PK; u++) {   // the atomics of the slots in flight together
+                const int prev = __shfl_up_sync(0xffffffffu, k[u], 1);
+                const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != k[u]);
+                leader[u] = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+                const unsigned above = starts & ~(0xffffffffu >> (31 - lane));
+                const int end = above ? __ffs(above) - 1 : 32;
+                rank[u] = lane - leader[u];
+                base[u] = (lane == leader[u] && k[u] >= 0) ? atomicAdd(&B.cursor[k[u]], end - leader[u]) : 0;
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < PK; u++) {
                 const int d = __shfl_sync(0xffffffffu, base[u], leader[u]) + rank[u];
                 if (k[u] >= 0) {
                     if (d >= 0 && d < B.np) B.perm[d] = i0 + u * stride;
@@ -379,11 +395,12 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             if (r.y > r.x) order[atomicAdd(&bucket[QBUCKETS - 1 - min(r.y - r.x, QBUCKETS - 1)], 1)] = (unsigned short)j;
         }
         __syncwarp();
-        if (lane == 0) *head = 32;
-        __syncwarp();
-        // cells dealt to lanes from the queue; a lane sums its cell's 27 amounts (Flip.scatter, Flip.java:269-303)
-        // over the cell's particles in registers and adds them into the window when the cell is done. Lanes that
-        // finish together hold distinct cells, so at one stencil offset they write distinct nodes.
+        // the non-empty cells in synchronous rounds of 32, fullest first: a lane sums its cell's 27 amounts
+        // (Flip.scatter, Flip.java:269-303) over the cell's particles in registers; when the round's fullest cell is
+        // done, all its lanes add their sums into the window at once. A round's cells have like counts, so few lanes
+        // wait, and its lanes hold distinct cells, so at one stencil offset they write distinct nodes. (Dealing
+        // cells from a queue, a lane taking the next cell when its own was done, left the window adds at scattered
+        // times, divergent in nearly every iteration.)
         auto source = [&](int slot) {
             const int src = B.perm[slot];
             if (src < p0 || src >= p1) {
@@ -393,35 +410,39 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             return src;
         };
         float acc[27];
+        for (int r0 = 0; r0 < ncq; r0 += 32) {
 #pragma unroll
-        for (int a = 0; a < 27; a++) acc[a] = 0.0f;
-        int cell = lane < ncq ? order[lane] : -1, i = 0, end = 0;
-        Part2 nxt;   // the lane's next particle in flight
-        auto open = [&]() {
-            const int2 r = crange[cell];
-            i = r.x;
-            end = r.y;
-            load_part2(nxt, in, st, source(i));
-        };
-        if (cell >= 0) open();
-        while (__any_sync(0xffffffffu, cell >= 0)) {
-            if (cell >= 0 && i < end) {
-                const Part2 cur = nxt;
-                if (i + 1 < end) load_part2(nxt, in, st, source(i + 1));
-                i++;
-                if (cur.m > 0.0f) {
-                    const Stencil2 sn = stencil2(cur.x, cur.y, nx, ny);
-                    if (sn.col == x0 + cell % tx && sn.row == y0 + cell / tx) {
-                        const float sp = impulse_factor(prm.dt, cur.m, prm.rho0, prm.bulk, cur.j, prm.tait);
-                        scatter_accumulate2(sn, cur.m, cur.u, cur.v, cur.c00, cur.c01, cur.c10, cur.c11, sp, acc);
-                    } else {
-                        set_status(B.status, ST_OOB);
+            for (int a = 0; a < 27; a++) acc[a] = 0.0f;
+            const int cell = r0 + lane < ncq ? order[r0 + lane] : -1;
+            int i = 0, end = 0;
+            Part2 nxt, nxt2;   // the lane's next two particles in flight
+            if (cell >= 0) {
+                const int2 r = crange[cell];
+                i = r.x;
+                end = r.y;
+                load_part2(nxt, in, st, source(i));
+                if (i + 1 < end) load_part2(nxt2, in, st, source(i + 1));
+            }
+            const int steps = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(end - i, 0));
+            for (int n = 0; n < steps; n++) {
+                if (i < end) {
+                    const Part2 cur = nxt;
+                    nxt = nxt2;
+                    if (i + 2 < end) load_part2(nxt2, in, st, source(i + 2));
+                    i++;
+                    if (cur.m > 0.0f) {
+                        const Stencil2 sn = stencil2(cur.x, cur.y, nx, ny);
+                        if (sn.col == x0 + cell % tx && sn.row == y0 + cell / tx) {
+                            const float sp = impulse_factor(prm.dt, cur.m, prm.rho0, prm.bulk, cur.j, prm.tait);
+                            scatter_accumulate2(sn, cur.m, cur.u, cur.v, cur.c00, cur.c01, cur.c10, cur.c11, sp, acc);
+                        } else {
+                            set_status(B.status, ST_OOB);
+                        }
                     }
                 }
             }
-            const bool done = cell >= 0 && i >= end;
-            const unsigned fm = __ballot_sync(0xffffffffu, done);
-            if (done) {
+            const unsigned fm = __ballot_sync(0xffffffffu, cell >= 0);
+            if (cell >= 0) {
                 const int wb = (cell / tx) * wx + cell % tx;
 #pragma unroll
                 for (int o = 0; o < 9; o++) {
@@ -429,14 +450,10 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
                     ww[wi] += acc[3 * o];
                     ww[wn + wi] += acc[3 * o + 1];
                     ww[2 * wn + wi] += acc[3 * o + 2];
-                    acc[3 * o] = acc[3 * o + 1] = acc[3 * o + 2] = 0.0f;
                     __syncwarp(fm);
                 }
-                const int pos = atomicAdd(head, 1);
-                cell = pos < ncq ? order[pos] : -1;
-                if (cell >= 0) open();
             }
-            __syncwarp();   // this iteration's window writes before the next iteration's reads
+            __syncwarp();   // this round's window writes before the next round's
         }
         __syncwarp();
         for (int j = lane; j < wn; j += 32) {
@@ -487,46 +504,90 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             vw[j] = v;
         }
         __syncwarp();
-        int src_next = c0 + lane < c1 ? B.perm[c0 + lane] : -1;
-        for (int b = c0; b < c1; b += 32) {
-            const int slot = b + lane;
-            int src = src_next;
-            if (slot + 32 < c1) src_next = B.perm[slot + 32];   // the next round's source
-            int nkey = -1, ntile = -1;
-            if (slot < c1) {
-                if (src < p0 || src >= p1) {
-                    set_status(B.status, ST_OOB);
-                    src = slot;
-                }
-                const float px = in[PX * st + src], py = in[PY * st + src];
-                const float pj = in[PJ * st + src], pm = in[PM * st + src];
-                const Stencil2 sn = stencil2(px, py, nx, ny);
-                const int lx = sn.col - x0, ly = sn.row - y0;
-                Advected2 a;
-                if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
-                    const int wb = ly * wx + lx;
-                    a = advect2(sn, px, py, pj, nx, ny, prm, [&](int o) { return vw[wb + (o / 3) * wx + o % 3]; },
-                                [](int) { return 0.0f; });
-                } else {
-                    set_status(B.status, ST_OOB);
-                    a = Advected2{px, py, in[PU * st + src], in[PV * st + src], in[PC00 * st + src],
-                                  in[PC01 * st + src], in[PC10 * st + src], in[PC11 * st + src], pj};
-                }
-                out[PX * st + slot] = a.x;
-                out[PY * st + slot] = a.y;
-                out[PU * st + slot] = a.u;
-                out[PV * st + slot] = a.w;
-                out[PM * st + slot] = pm;
-                out[PJ * st + slot] = a.j;
-                out[PC00 * st + slot] = a.c00;
-                out[PC01 * st + slot] = a.c01;
-                out[PC10 * st + slot] = a.c10;
-                out[PC11 * st + slot] = a.c11;
-                batch_key(sc, a.x, a.y, nkey, ntile);
-                B.key[slot] = nkey;
+        // Groups of GG x 32 particles (GG a lane, 32 apart): a group's permutation entries are read two groups
+        // ahead and its positions, J and masses one group ahead, so a lane has GG particles' loads in flight while
+        // it advects the current group (a particle's arithmetic is far shorter than a load's round trip).
+        constexpr int GG = 4;
+        auto src_at = [&](int slot) {   // a sorted slot's source, checked (its own slot when out of range)
+            if (slot >= c1) return -1;
+            int v = B.perm[slot];
+            if (v < p0 || v >= p1) {
+                set_status(B.status, ST_OOB);
+                v = slot;
             }
-            warp_tally(B.cell_count, nkey, nkey >= 0, B.ncells, B.status);
-            warp_tally(B.tile_count, ntile, ntile >= 0, B.nentries, B.status);
+            return v;
+        };
+        int sa[GG], sb[GG];
+        float qx[GG], qy[GG], qj[GG], qm[GG];
+#pragma unroll
+        for (int u = 0; u < GG; u++) {
+            sa[u] = src_at(c0 + 32 * u + lane);
+            sb[u] = src_at(c0 + 32 * (GG + u) + lane);
+        }
+#pragma unroll
+        for (int u = 0; u < GG; u++) {
+            qx[u] = qy[u] = qj[u] = qm[u] = 0.0f;
+            if (sa[u] >= 0) {
+                qx[u] = in[PX * st + sa[u]];
+                qy[u] = in[PY * st + sa[u]];
+                qj[u] = in[PJ * st + sa[u]];
+                qm[u] = in[PM * st + sa[u]];
+            }
+        }
+        for (int b = c0; b < c1; b += 32 * GG) {
+            int src[GG];
+            float px[GG], py[GG], pj[GG], pm[GG];
+#pragma unroll
+            for (int u = 0; u < GG; u++) {
+                src[u] = sa[u];
+                px[u] = qx[u];
+                py[u] = qy[u];
+                pj[u] = qj[u];
+                pm[u] = qm[u];
+                sa[u] = sb[u];
+                if (sa[u] >= 0) {
+                    qx[u] = in[PX * st + sa[u]];
+                    qy[u] = in[PY * st + sa[u]];
+                    qj[u] = in[PJ * st + sa[u]];
+                    qm[u] = in[PM * st + sa[u]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < GG; u++) sb[u] = src_at(b + 32 * (2 * GG + u) + lane);
+#pragma unroll
+            for (int u = 0; u < GG; u++) {
+                const int slot = b + 32 * u + lane;
+                int nkey = -1, ntile = -1;
+                if (slot < c1) {
+                    const Stencil2 sn = stencil2(px[u], py[u], nx, ny);
+                    const int lx = sn.col - x0, ly = sn.row - y0;
+                    Advected2 a;
+                    if (lx >= 0 && lx < tx && ly >= 0 && ly < ty) {
+                        const int wb = ly * wx + lx;
+                        a = advect2(sn, px[u], py[u], pj[u], nx, ny, prm,
+                                    [&](int o) { return vw[wb + (o / 3) * wx + o % 3]; }, [](int) { return 0.0f; });
+                    } else {
+                        set_status(B.status, ST_OOB);
+                        const int sr = src[u];
+                        a = Advected2{px[u], py[u], in[PU * st + sr], in[PV * st + sr], in[PC00 * st + sr],
+                                      in[PC01 * st + sr], in[PC10 * st + sr], in[PC11 * st + sr], pj[u]};
+                    }
+                    out[PX * st + slot] = a.x;
+                    out[PY * st + slot] = a.y;
+                    out[PU * st + slot] = a.u;
+                    out[PV * st + slot] = a.w;
+                    out[PM * st + slot] = pm[u];
+                    out[PJ * st + slot] = a.j;
+                    out[PC00 * st + slot] = a.c00;
+                    out[PC01 * st + slot] = a.c01;
+                    out[PC10 * st + slot] = a.c10;
+                    out[PC11 * st + slot] = a.c11;
+                    batch_key(sc, a.x, a.y, nkey, ntile);
+                    B.key[slot] = nkey;
+                }
+                warp_tally(B.cell_count, nkey, nkey >= 0, B.ncells, B.status);
+                warp_tally(B.tile_count, ntile, ntile >= 0, B.nentries, B.status);
+            }
         }
         __syncwarp();   // the window is free for the next chunk
     }

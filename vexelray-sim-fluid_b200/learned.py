@@ -158,20 +158,28 @@ def coarse_step_ticks(n_fine: int, hmax: float = 1.5, dx: float = 1.0) -> int:
 
 
 def generate_and_train(net: FluxNet, n_fine: int, seeds, *, pairs: int, spacing: int, interval: int, batch: int,
-                       lr: float, steps_per_pair: int = 1, lr_end: float | None = None, seed: int = 0,
-                       log=None) -> dict:
-    """Fine runs from the seeds (bumps), `pairs` samples each, `spacing` fine steps apart (the first after
-    `spacing` steps); every sample goes into the network's ring and is followed by `steps_per_pair` Adam steps
-    on random batches of the ring. The learning rate decays geometrically from lr to lr_end."""
+                       lr: float, steps_per_pair: float = 1, lr_end: float | None = None, seed: int = 0,
+                       sample_every: int | None = None, log=None) -> dict:
+    """Fine runs from the seeds (bumps), `pairs` samples each; every sample goes into the network's ring and is
+    followed by `steps_per_pair` Adam steps on random batches of the ring (a fraction: one step every so many
+    samples). The learning rate decays geometrically from lr to lr_end.
+
+    Sampling: with `sample_every` the samples' start states are every `sample_every` steps of one fine run (the
+    first after `sample_every` steps), and each target is a second fine solver's state an interval after a copy of
+    the run's state; otherwise the run itself advances through each target, and the next start is `spacing` fine
+    steps after it."""
     rng = np.random.default_rng(seed)
     nc = n_fine // 2
     fine = PatchSimulation(n_fine, n_fine)
+    ahead = PatchSimulation(n_fine, n_fine) if sample_every else None
     coarse = PatchSimulation(nc, nc)
     _empty(coarse, coarse_params())
+    if ahead is not None:
+        _empty(ahead, fine_params())
     cap = net.samples
     filled, slot, losses = 0, 0, []
-    total = len(seeds) * pairs * steps_per_pair
-    done = 0
+    total = int(len(seeds) * pairs * steps_per_pair)
+    done, credit = 0, 0.0
     t0 = time.perf_counter()
     try:
         for s in seeds:
@@ -179,26 +187,36 @@ def generate_and_train(net: FluxNet, n_fine: int, seeds, *, pairs: int, spacing:
             z = np.zeros_like(h0)
             fine.load(h0, z, z, fine_params())
             for _ in range(pairs):
-                fine.advance(NEVER, spacing)
+                fine.advance(NEVER, sample_every or spacing)
                 coarse.restrict_from(fine)
                 net.put_state(slot, 0, coarse)
                 coarse.advance(interval, NEVER)
                 net.put_state(slot, 1, coarse)
-                fine.advance(interval, NEVER)
-                coarse.restrict_from(fine)
+                if ahead is not None:
+                    ahead.copy_from(fine)
+                    ahead.advance(interval, NEVER)
+                    coarse.restrict_from(ahead)
+                else:
+                    fine.advance(interval, NEVER)
+                    coarse.restrict_from(fine)
                 net.put_state(slot, 2, coarse)
                 filled = min(filled + 1, cap)
                 slot = (slot + 1) % cap
-                for _ in range(steps_per_pair):
+                credit += steps_per_pair
+                while credit >= 1.0:
+                    credit -= 1.0
                     frac = done / max(1, total - 1)
-                    rate = lr if lr_end is None else lr * (lr_end / lr) ** frac
+                    rate = lr if lr_end is None else lr * (lr_end / lr) ** min(1.0, frac)
                     pick = rng.choice(filled, size=min(batch, filled), replace=False)
                     losses.append(net.train(pick, rate))
                     done += 1
             if log:
-                log(f"seed {s}: loss {np.mean(losses[-pairs * steps_per_pair:]):.4g}  ({time.perf_counter() - t0:.1f} s)")
+                recent = losses[-max(1, int(pairs * steps_per_pair)):]
+                log(f"seed {s}: loss {np.mean(recent) if recent else float('nan'):.4g}  ({time.perf_counter() - t0:.1f} s)")
     finally:
         fine.close()
+        if ahead is not None:
+            ahead.close()
         coarse.close()
     return {"losses": losses, "seconds": time.perf_counter() - t0}
 

@@ -1,7 +1,11 @@
 """Trains the flux-correction network on the GPU and evaluates it on held-out seeds.
 
   python vexelray-sim-fluid_b200/train_learned.py --out DIR [--fine 2048] [--seeds 128] [--pairs 20]
-         [--spacing 100] [--interval-steps 16] [--eval-seeds 8]
+         [--spacing 100 | --sample-every 10] [--interval-steps 16] [--steps-per-pair 3] [--ring 256]
+         [--eval-seeds 8]
+
+The learned configuration's data (512 runs, pairs every 10 fine steps to 2000) is
+  --seeds 512 --pairs 200 --sample-every 10
 
 Fine runs at --fine^2 (the shallow-water configuration's bump distribution halved in sigma and centres) give the
 samples; the network (coarse grid --fine/2) is trained by the library's own forward and backward kernels with Adam.
@@ -56,7 +60,9 @@ def main(argv=None):
     ap.add_argument("--pairs", type=int, default=20)
     ap.add_argument("--spacing", type=int, default=100)
     ap.add_argument("--interval-steps", type=int, default=16)
-    ap.add_argument("--steps-per-pair", type=int, default=3)
+    ap.add_argument("--sample-every", type=int, default=None,
+                    help="sample every N fine steps of one run, each target from a copy of the run's state")
+    ap.add_argument("--steps-per-pair", type=float, default=3)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--ring", type=int, default=256)
     ap.add_argument("--lr", type=float, default=2e-3)
@@ -78,7 +84,7 @@ def main(argv=None):
     train_seeds = list(range(1000, 1000 + args.seeds))   # held-out seeds are 1 .. eval-seeds
     r = L.generate_and_train(net, n, train_seeds, pairs=args.pairs, spacing=args.spacing, interval=interval,
                              batch=args.batch, lr=args.lr, lr_end=args.lr_end, steps_per_pair=args.steps_per_pair,
-                             log=lambda s: print(s, flush=True))
+                             sample_every=args.sample_every, log=lambda s: print(s, flush=True))
     params = net.params()
     stem = f"learned_{n}_k{args.interval_steps}"
     np.save(out / f"{stem}.npy", params)
@@ -94,7 +100,8 @@ def main(argv=None):
     report = {
         "fine": n, "coarse": n // 2, "interval_ticks": interval, "interval_coarse_steps": args.interval_steps,
         "s_flux": args.s_flux, "s_res": args.s_res, "train_seeds": [train_seeds[0], train_seeds[-1]],
-        "pairs_per_seed": args.pairs, "spacing_fine_steps": args.spacing, "adam_steps": len(losses),
+        "pairs_per_seed": args.pairs, "spacing_fine_steps": args.spacing, "sample_every_fine_steps": args.sample_every,
+        "steps_per_pair": args.steps_per_pair, "ring": args.ring, "adam_steps": len(losses),
         "batch": args.batch, "lr": [args.lr, args.lr_end], "train_seconds": r["seconds"],
         "loss_curve": [float(np.mean(losses[i:i + k])) for i in range(0, len(losses), k)],
         "eval": evals,
