@@ -375,8 +375,8 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
 }
 
 // ------------------------------------------------------------------ the fast mode's strip kernel
-// One CTA of four warps per tile of 120 columns x 32 rows. The tile and a halo (columns x0-4 .. x0+123, rows
-// y0-1 .. y0+32) land in shared memory by three 2D TMA loads; then every lane walks one column up the tile in
+// One CTA of four warps per tile of 120 columns x 16 rows. The tile and a halo (columns x0-4 .. x0+123, rows
+// y0-1 .. y0+16) land in shared memory by three 2D TMA loads; then every lane walks one column up the tile in
 // registers: lane L of warp w holds column x0 + 30 w + L - 1, lanes 1..30 update their cell, lanes 0 and 31 only
 // lend their state to their neighbours. A cell's west face is computed by its lane from its left neighbour's state
 // (a shuffle), its east face is the right neighbour's west face (a shuffle), its south face was computed one row
@@ -384,7 +384,9 @@ __global__ void __launch_bounds__(SWE_THREADS) k_swe_tile(SweArgs a, const __gri
 // same inputs), the state read from shared memory once, and no shared-memory traffic for primitives or fluxes.
 constexpr int STRIP_WARPS = 4;
 constexpr int STRIP_COLS = 30 * STRIP_WARPS;   // columns a tile updates (a multiple of 4: the box's x stays aligned)
-constexpr int STRIP_ROWS = 32;
+// 16 rows: 27.6 KB of tile a CTA, so eight CTAs fit an SM (at 4096^2 the fast step takes 0.124 ms against 0.129
+// with 32 rows, whose 52 KB tiles left room for four)
+constexpr int STRIP_ROWS = 16;
 constexpr int STRIP_BW = 128;                  // box width: columns x0-4 .. x0+123
 constexpr int STRIP_BH = STRIP_ROWS + 2;       // box height: rows y0-1 .. y0+ROWS
 
