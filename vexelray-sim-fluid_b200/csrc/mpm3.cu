@@ -256,7 +256,7 @@ int32_t run_sort(vf_mpm3* h, int g, bool will_scatter, bool fused_fixup) {
     VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(),
               h->cell_start.as<int>(), h->cursor.as<int>(),
                                                           h->brick_start.as<int>(), active, n_active);
-    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256), 256, 0, h->key.as<int>(),
+    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256 * PERMUTE_PER), 256, 0, h->key.as<int>(),
               h->cursor.as<int>(), h->perm.as<int>(), h->np, h->nkeys, h->status.as<uint32_t>());
     // the tiled scatter puts each cell's run in order itself; everything else needs the fix-up pass
     if (!fused_fixup)
@@ -407,7 +407,7 @@ int32_t fused_sort(vf_mpm3* h) {
               h->brick_start.as<int>(), active, n_active, h->nbricks);
     VF_LAUNCH(h->prof, "k_cell_scan", h->stream, k_cell_scan, persistent_blocks(4), 512, 0, h->cell_count.as<int>(),
               h->cell_start.as<int>(), h->cursor.as<int>(), h->brick_start.as<int>(), active, n_active);
-    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256), 256, 0, h->key.as<int>(),
+    VF_LAUNCH(h->prof, "k_permute_cursor", h->stream, k_permute_cursor, div_up(h->np, 256 * PERMUTE_PER), 256, 0, h->key.as<int>(),
               h->cursor.as<int>(), h->perm.as<int>(), h->np, h->nkeys, h->status.as<uint32_t>());
     h->counted = false;
     h->sorted_valid = true;

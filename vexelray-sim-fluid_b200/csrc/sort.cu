@@ -109,16 +109,43 @@ __global__ void k_permute(const int* __restrict__ key, const int* __restrict__ r
 
 __global__ void __launch_bounds__(256) k_permute_cursor(const int* __restrict__ key, int* __restrict__ cursor,
                                                        int* __restrict__ perm, int n, int64_t nkeys, uint32_t* status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const int k = valid ? key[i] : 0;
-    const int d = warp_count_runs(cursor, k, valid, nkeys, status);
-    if (!valid) return;
-    if (d < 0 || d >= n) {
-        set_status(status, ST_RANK);
-        return;
+    // PERMUTE_PER slots a thread, PERMUTE_PER x 256 a block; a warp's slots for one u are consecutive, so in the
+    // last step's sorted order their keys come in runs: one cursor atomic per run, all of a thread's in flight
+    // together before their ranks are read
+    const unsigned all = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int base = blockIdx.x * (256 * PERMUTE_PER) + threadIdx.x;
+    int k[PERMUTE_PER], leader[PERMUTE_PER], rank[PERMUTE_PER], got[PERMUTE_PER];
+#pragma unroll
+    for (int u = 0; u < PERMUTE_PER; u++) {
+        const int i = base + u * 256;
+        k[u] = i < n ? key[i] : -1;
+        if (i < n && (k[u] < 0 || (int64_t)k[u] >= nkeys)) {
+            set_status(status, ST_OOB);
+            k[u] = -1;
+        }
     }
-    perm[d] = i;
+#pragma unroll
+    for (int u = 0; u < PERMUTE_PER; u++) {
+        const int prev = __shfl_up_sync(all, k[u], 1);
+        const unsigned starts = __ballot_sync(all, lane == 0 || prev != k[u]);
+        leader[u] = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // the run's first lane
+        const unsigned above = starts & ~(0xffffffffu >> (31 - lane));    // run starts after this lane
+        const int end = above ? __ffs(above) - 1 : 32;
+        rank[u] = lane - leader[u];
+        got[u] = (lane == leader[u] && k[u] >= 0) ? atomicAdd(&cursor[k[u]], end - leader[u]) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < PERMUTE_PER; u++) {
+        const int d = __shfl_sync(all, got[u], leader[u]) + rank[u];
+        const int i = base + u * 256;
+        if (k[u] < 0) continue;
+        if (d < 0 || d >= n) {
+            set_status(status, ST_RANK);
+            continue;
+        }
+        perm[d] = i;
+    }
 }
 
 // Insertion sort of a short run, ascending.

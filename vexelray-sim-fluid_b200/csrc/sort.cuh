@@ -119,8 +119,10 @@ __global__ void k_cell_scan(int* __restrict__ cell_count, int* __restrict__ cell
                             const int* __restrict__ brick_start, const int* __restrict__ active,
                             const int* __restrict__ n_active);
 
-// perm[cursor[key[i]]++] = i, the cursor bumped once per distinct key in a warp: the permutation with
-// provisional (unstable) order within a cell, for counts that were tallied without ranks.
+// perm[cursor[key[i]]++] = i, the cursor bumped once per run of equal keys in a warp: the permutation with
+// provisional (unstable) order within a cell, for counts that were tallied without ranks. PERMUTE_PER slots a
+// thread, blocks of 256 threads: launch div_up(n, 256 * PERMUTE_PER) blocks.
+constexpr int PERMUTE_PER = 4;
 __global__ void k_permute_cursor(const int* __restrict__ key, int* __restrict__ cursor, int* __restrict__ perm, int n,
                                  int64_t nkeys, uint32_t* status);
 
