@@ -22,6 +22,10 @@ from . import EDGE_OPEN, EDGE_WALL, FluxNet, PatchSimulation, swe_params
 
 G, COURANT, DRY = 9.81, 0.45, 1e-6
 NEVER = 2 ** 31 - 1   # a step budget that does not stop the steps
+# Coarse steps an interval may take before the learned solver gives up on it. An interval is about 16 steps of a
+# still depth of 1.5; a state the correction has driven to near-dry or violent (wave speeds that shrink the step
+# toward one tick) would otherwise spin here. The reference's runaway guard does the same for its stepper.
+INTERVAL_STEP_CAP = 1024
 
 
 def bumps(seed: int, n: int, count: int = 16, scale: float | None = None) -> np.ndarray:
@@ -102,8 +106,11 @@ class LearnedShallowWater:
                     self.start.copy_from(self.coarse)
             if self.net is not None:
                 self.net.predict(self.coarse)   # from the interval's start, as the samples' S
-            a = self.coarse.advance(t, NEVER)
+            a = self.coarse.advance(t, INTERVAL_STEP_CAP)
             self.steps += a.steps
+            if a.spent_ticks < t:
+                raise RuntimeError(f"the corrected coarse state stopped advancing: {a.steps} steps covered "
+                                   f"{a.spent_ticks} of the interval's {t} ticks (correction {self.corrections})")
             if self.net is not None:
                 self.net.apply(self.coarse)     # to the plain interval's end, as the samples' P
                 self.corrections += 1
