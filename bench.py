@@ -922,7 +922,7 @@ def run_learned(args, vf):
                       "speedup": r[1]["speedup"]} for r in rows],
         "network_kernels_us": {k: 1e3 * v[0] / v[1] for k, v in prof.items()},
         "roofline": {"bound": "tensor", "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
-                     "peak_kind": tkind, "traffic": None, "kernel": "k_conv1 (mma.sync) + k_conv2 + k_conv3 (tcgen05), bf16",
+                     "peak_kind": tkind, "traffic": None, "kernel": "k_conv1 + k_conv2 + k_conv3 (tcgen05), bf16",
                      "flops_per_cell": CNN_FLOPS_PER_CELL},
         "training": {"seeds": report["train_seeds"], "pairs_per_seed": report["pairs_per_seed"],
                      "adam_steps": report["adam_steps"], "train_seconds": report["train_seconds"]},

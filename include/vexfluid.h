@@ -487,7 +487,8 @@ typedef struct vf_swe_learned vf_swe_learned;
 int32_t vf_swe_learned_create(int32_t nx, int32_t ny, vf_cnn* net, int64_t interval_ticks, int32_t tile,
                               int32_t fallback, float threshold, int32_t margin, float dx, vf_swe_learned** out);
 int32_t vf_swe_learned_load(vf_swe_learned* h, const float* hcell, const float* hu, const float* hv);
-/* Intervals until `ticks` are spent (the last one shortened to fit). */
+/* Intervals until `ticks` are spent (the last one shortened to fit). VF_ESTATE when an interval takes more than
+ * 1024 coarse steps (a correction drove the state toward dry or violent flow and the step stopped growing). */
 int32_t vf_swe_learned_advance(vf_swe_learned* h, int64_t ticks);
 int32_t vf_swe_learned_read(vf_swe_learned* h, float* hcell, float* hu, float* hv);
 /* out = {coarse steps, corrections applied, fallback tiles stepped}. */

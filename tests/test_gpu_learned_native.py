@@ -4,7 +4,8 @@ steps, corrections and fallback tiles are the same counts.
 
 Cases: the committed network at its configuration (2048^2 fine, 1024^2 coarse); the plain coarse solver with every
 tile falling back to the fine solver; the committed network's parameters on a 256^2 coarse grid with the tiles
-above the median depth jump falling back, over a run that ends inside an interval.
+above the median depth jump falling back, over a run that ends inside an interval; and an interval too long for
+the drivers' step cap, refused by both.
 """
 import pathlib
 
@@ -69,3 +70,26 @@ def test_the_tiles_above_the_median_jump_over_a_partial_interval():
             threshold = float(np.float32(np.median(p.jump_indicator(64))))
         steps, corrections, fallback = both(n, net, interval, 3 * interval + interval // 2, threshold)
     assert corrections == 4 and 0 < fallback < 4 * 16
+
+
+def test_an_interval_that_stops_advancing_is_refused_by_both_drivers():
+    # An interval of about 1,600 coarse steps' ticks (100 ordinary intervals) outruns the drivers' cap of 1,024 steps
+    # an interval: the state is the plain solver's, but the steps look the way they do when a correction has shrunk
+    # them toward a tick, and both drivers stop instead of stepping on.
+    n = 256
+    interval = 100 * 16 * L.coarse_step_ticks(n)
+    h0 = L.bumps(11, n)
+    z = np.zeros_like(h0)
+    py = L.LearnedShallowWater(n // 2, n // 2, None, interval)
+    try:
+        py.load_fine(h0, z, z)
+        with pytest.raises(RuntimeError, match="stopped advancing"):
+            py.advance(interval)
+        assert py.steps == L.INTERVAL_STEP_CAP
+    finally:
+        py.close()
+    with vf.LearnedSimulation(n // 2, n // 2, None, interval) as s:
+        s.load(L.restrict(h0), L.restrict(z), L.restrict(z))
+        with pytest.raises(vf.IllegalStateException, match="stopped advancing"):
+            s.advance(interval)
+        assert s.counts()[0] == L.INTERVAL_STEP_CAP

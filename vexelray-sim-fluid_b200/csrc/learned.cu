@@ -22,6 +22,11 @@ namespace {
 
 constexpr float G = 9.81f, COURANT = 0.45f, DRY = 1e-6f;
 constexpr int32_t NEVER = 2147483647;   // a step budget that does not stop the steps
+// Coarse steps an interval may take before the driver gives up on it (about 64 times the usual 16): a state a
+// correction has driven toward dry or violent flow shrinks the step toward a tick and would otherwise spin. The
+// reference's test stepper stops a run the same way when its steps stop growing
+// (vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/stencil/Stepper.java:90-93).
+constexpr int32_t INTERVAL_STEP_CAP = 1024;
 
 void swe_words(float dx, int32_t out[5]) {
     const float w[5] = {G, COURANT, dx, dx, DRY};
@@ -139,8 +144,12 @@ int32_t vf_swe_learned_advance(vf_swe_learned* h, int64_t ticks) {
             if ((rc = vf_cnn_predict(h->net, sh, su, sv, vf_swe_stream(h->coarse)))) return rc;
         }
         int32_t steps = 0;
-        if ((rc = vf_swe_advance(h->coarse, t, NEVER, &steps, nullptr, nullptr))) return rc;
+        int64_t spent = 0;
+        if ((rc = vf_swe_advance(h->coarse, t, INTERVAL_STEP_CAP, &steps, &spent, nullptr))) return rc;
         h->steps += steps;
+        VF_REQUIRE(spent >= t, VF_ESTATE,
+                   "the corrected coarse state stopped advancing: %d steps covered %lld of the interval's %lld ticks "
+                   "(correction %lld)", steps, (long long)spent, (long long)t, (long long)h->corrections);
         if (h->net) {
             if ((rc = vf_swe_state(h->coarse, &sh, &su, &sv))) return rc;
             if ((rc = vf_cnn_apply(h->net, sh, su, sv, vf_swe_stream(h->coarse)))) return rc;

@@ -24,7 +24,8 @@ G, COURANT, DRY = 9.81, 0.45, 1e-6
 NEVER = 2 ** 31 - 1   # a step budget that does not stop the steps
 # Coarse steps an interval may take before the learned solver gives up on it. An interval is about 16 steps of a
 # still depth of 1.5; a state the correction has driven to near-dry or violent (wave speeds that shrink the step
-# toward one tick) would otherwise spin here. The reference's runaway guard does the same for its stepper.
+# toward one tick) would otherwise spin here. The reference's test stepper stops a run the same way when its
+# steps stop growing (vexelray-sim-fluid-core/src/test/java/dev/vexelray/sim/fluid/stencil/Stepper.java:90-93).
 INTERVAL_STEP_CAP = 1024
 
 
