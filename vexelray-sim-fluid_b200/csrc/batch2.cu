@@ -28,11 +28,11 @@
 //                    chunks enter the item list, and the other parity's grid is cleared over the windows of
 //                    the tiles the previous step scattered into.
 //   4  scatter       a warp per chunk, work-stealing: the tile's cells clipped to the chunk (the cursors hold
-//                    each run's end) are dealt to lanes from a queue ordered by count, largest first; a lane sums
-//                    Flip.scatter's 27 amounts over its cell's particles in registers and adds them into the
-//                    warp's private node window when the cell is done (lanes finishing together hold distinct
-//                    cells, so distinct nodes at each stencil offset: plain read-modify-write); then one 16-byte
-//                    red.global.add.v4.f32 per touched window node
+//                    each run's end) are ordered by count, largest first, and taken in rounds of 32, a lane a cell;
+//                    a lane sums Flip.scatter's 27 amounts over its cell's particles in registers, and when the
+//                    round's fullest cell is done all its lanes add their sums into the warp's private node window
+//                    (a round's lanes hold distinct cells, so distinct nodes at each stencil offset: plain
+//                    read-modify-write); then one 16-byte red.global.add.v4.f32 per touched window node
 //   5  gather        a warp per chunk, work-stealing: the tile window's node velocities (Flip.grid, fused) into
 //                    the warp's shared memory, then per particle Flip.advectBody; the particle is written to its
 //                    sorted slot of the other set, and its next cell key tallied for the next step's sort.
