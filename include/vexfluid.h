@@ -461,9 +461,8 @@ int32_t vf_cnn_correct(vf_cnn* h, float* hcell, float* hu, float* hv, void* stre
  * north face's). */
 int32_t vf_cnn_fluxes(vf_cnn* h, int32_t slot, float* out);
 void* vf_cnn_stream(vf_cnn* h);
-/* The forward and input-gradient convolutions' kernels: 0 (the default) tcgen05.mma for the 32-input-channel layers
- * (TMA-fed ring of input rows in shared memory, accumulators in tensor memory, warp-specialised) and 1's kernels for
- * the 8-channel ones; 1 mma.sync with each warp computing several output rows from every A fragment it loads; 2
+/* The forward and input-gradient convolutions' kernels: 0 (the default) tcgen05.mma for every layer (TMA-fed ring
+ * of input rows in shared memory, accumulators in tensor memory, warp-specialised); 1 mma.sync with each warp computing several output rows from every A fragment it loads; 2
  * mma.sync with one output row per warp. All compute the same network (to fp32 summation order). The weight
  * gradients always run on mma.sync. */
 int32_t vf_cnn_set_path(vf_cnn* h, int32_t path);

@@ -955,8 +955,8 @@ class ParticleSimulation3:
         return int(lib().vf_mpm3_schedule(self._h))
 
     def set_fused(self, on: bool) -> None:
-        """The fused step (the gather and the next step's scatter in one kernel), the default where it applies;
-        off runs the separate tiled scatter and gather."""
+        """The fused step (the gather and the next step's scatter in one kernel) where it applies; off, the default,
+        runs the separate tiled scatter and gather."""
         check(lib().vf_mpm3_set_fused(self._h, 1 if on else 0))
 
     def fused(self) -> bool:
