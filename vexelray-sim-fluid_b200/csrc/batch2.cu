@@ -219,34 +219,52 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
         }
         if (threadIdx.x == 0) B.scene_chunk_start[B.nscenes] = carry;
     }
-    for (int t = gwarp; t < B.nentries; t += nwarps_all) {
-        const int s = B.tile_scene[t];
-        if (s < 0) continue;
-        const int ts = ts_cur[t], te = ts_cur[t + 1];
-        if (te <= ts) continue;
-        if (ts < B.scene[s].p0 || te > B.scene[s].p0 + B.scene[s].np) {   // counts that do not add up
-            if (lane == 0) set_status(B.status, ST_RANK);
-            continue;
-        }
-        const int tc = B.scene[s].tc;                 // 64 .. 512 cells: per = 2 .. 16 per lane
-        const int per = tc >> 5;
-        const int cb = B.scene[s].c0 + (t - B.scene[s].t0) * tc + lane * per;
-        int c[16], sum = 0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            c[k] = k < per ? B.cell_count[cb + k] : 0;
-            sum += c[k];
-        }
-        int run = ts + warp_inclusive(sum) - sum;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            if (k < per) {
-                B.cursor[cb + k] = run;
-                B.cell_count[cb + k] = 0;
-                run += c[k];
+    // The tiles, 32 at a time a warp: a lane reads one tile's run and scene (the reads of the warp's 32 tiles in
+    // flight together); then the warp scans the non-empty ones one at a time, every lane on the tile's cells.
+    for (int t0 = gwarp * 32; t0 < B.nentries; t0 += nwarps_all * 32) {
+        const int tl = t0 + lane;
+        const int sl = tl < B.nentries ? B.tile_scene[tl] : -1;
+        int tsl = 0, tel = 0, tcl = 0, cbl = 0;
+        bool live = false;
+        if (sl >= 0) {
+            tsl = ts_cur[tl];
+            tel = ts_cur[tl + 1];
+            const Scene2& sc = B.scene[sl];
+            if (tel > tsl) {
+                if (tsl < sc.p0 || tel > sc.p0 + sc.np) {   // counts that do not add up
+                    set_status(B.status, ST_RANK);
+                } else {
+                    live = true;
+                    tcl = sc.tc;                           // 64 .. 512 cells: 2 .. 16 per lane
+                    cbl = sc.c0 + (tl - sc.t0) * sc.tc;
+                }
             }
         }
-        if (lane == 31 && run != te) set_status(B.status, ST_RANK);
+        unsigned todo = __ballot_sync(0xffffffffu, live);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int ts = __shfl_sync(0xffffffffu, tsl, l), te = __shfl_sync(0xffffffffu, tel, l);
+            const int tc = __shfl_sync(0xffffffffu, tcl, l);
+            const int per = tc >> 5;
+            const int cb = __shfl_sync(0xffffffffu, cbl, l) + lane * per;
+            int c[16], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                c[k] = k < per ? B.cell_count[cb + k] : 0;
+                sum += c[k];
+            }
+            int run = ts + warp_inclusive(sum) - sum;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                if (k < per) {
+                    B.cursor[cb + k] = run;
+                    B.cell_count[cb + k] = 0;
+                    run += c[k];
+                }
+            }
+            if (lane == 31 && run != te) set_status(B.status, ST_RANK);
+        }
     }
     if (!grid_barrier(B.bar, B.status)) return;
     phase_done(1);
@@ -303,26 +321,54 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             }
         }
     }
-    for (int t = gwarp; t < B.nentries; t += nwarps_all) {
-        const int s = B.tile_scene[t];
-        if (s < 0) continue;
-        const Scene2& sc = B.scene[s];
-        const int ts = ts_cur[t], te = ts_cur[t + 1];
-        if (te > ts && ts >= sc.p0 && te <= sc.p0 + sc.np) {   // the tile's chunks into the item list
-            const int item0 = B.scene_chunk_start[s] + B.chunk_start[t];
-            const int nch = (te - ts + CHUNK - 1) / CHUNK;
-            for (int q = lane; q < nch; q += 32) {
-                if (item0 + q >= 0 && item0 + q < B.item_cap) B.item_tile[item0 + q] = t;
-                else set_status(B.status, ST_OOB);
-            }
+    // The tiles, 32 at a time a warp, a lane a tile: each lane reads its tile's runs and scene (the reads of a warp's
+    // 32 tiles in flight together) and enters the tile's chunks in the item list; then the warp clears, one tile at a
+    // time with every lane on it, the windows of the tiles the previous step scattered into, from the lanes' values.
+    for (int t0 = gwarp * 32; t0 < B.nentries; t0 += nwarps_all * 32) {
+        const int t = t0 + lane;
+        const int s = t < B.nentries ? B.tile_scene[t] : -1;
+        int ts = 0, te = 0;
+        bool clear = false;
+        if (t < B.nentries) {
+            ts = ts_cur[t];
+            te = ts_cur[t + 1];
+            clear = ts_prev[t + 1] > ts_prev[t];
         }
-        if (!(ts_prev[t + 1] > ts_prev[t])) continue;
-        const int lt = t - sc.t0;
-        const int x0 = (lt % sc.ntx) * sc.tx, y0 = (lt / sc.ntx) * sc.ty;
-        const int wx = sc.tx + 2, wn = wx * (sc.ty + 2);
-        for (int j = lane; j < wn; j += 32) {
-            const int gi = x0 + j % wx, gj = y0 + j / wx;
-            if (gi < sc.nx && gj < sc.ny) g_next[sc.g0 + (int64_t)gj * sc.nx + gi] = make_float4(0, 0, 0, 0);
+        int x0 = 0, y0 = 0, wx = 0, wn = 0, nxs = 0, nys = 0;
+        int64_t g0 = 0;
+        if (s >= 0) {
+            const Scene2& sc = B.scene[s];
+            if (te > ts && ts >= sc.p0 && te <= sc.p0 + sc.np) {   // the tile's chunks into the item list
+                const int item0 = B.scene_chunk_start[s] + B.chunk_start[t];
+                const int nch = (te - ts + CHUNK - 1) / CHUNK;
+                for (int q = 0; q < nch; q++) {
+                    if (item0 + q >= 0 && item0 + q < B.item_cap) B.item_tile[item0 + q] = t;
+                    else set_status(B.status, ST_OOB);
+                }
+            }
+            const int lt = t - sc.t0;
+            x0 = (lt % sc.ntx) * sc.tx;
+            y0 = (lt / sc.ntx) * sc.ty;
+            wx = sc.tx + 2;
+            wn = wx * (sc.ty + 2);
+            nxs = sc.nx;
+            nys = sc.ny;
+            g0 = sc.g0;
+        } else {
+            clear = false;
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, clear);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int cx0 = __shfl_sync(0xffffffffu, x0, l), cy0 = __shfl_sync(0xffffffffu, y0, l);
+            const int cwx = __shfl_sync(0xffffffffu, wx, l), cwn = __shfl_sync(0xffffffffu, wn, l);
+            const int cnx = __shfl_sync(0xffffffffu, nxs, l), cny = __shfl_sync(0xffffffffu, nys, l);
+            const int64_t cg0 = __shfl_sync(0xffffffffu, g0, l);
+            for (int j = lane; j < cwn; j += 32) {
+                const int gi = cx0 + j % cwx, gj = cy0 + j / cwx;
+                if (gi < cnx && gj < cny) g_next[cg0 + (int64_t)gj * cnx + gi] = make_float4(0, 0, 0, 0);
+            }
         }
     }
     if (!grid_barrier(B.bar, B.status)) return;
