@@ -80,8 +80,8 @@ struct Batch2 {
     int* chunk_start;          // per tile entry: its first chunk within its scene; the sentinel the scene's chunks
     int* scene_chunks;         // per scene: its chunks
     int* scene_chunk_start;    // per scene (and one past): its first chunk in the item list
-    int* item_tile;            // per chunk: its tile entry
-    int item_cap;              // item_tile's length
+    int4* item;                // per chunk: {tile entry, scene, first slot, end slot}, written by the permute phase
+    int item_cap;              // item's length
     float4* grid[2];
     unsigned* step;            // device step counter (its parity picks the buffers)
     unsigned* work;            // work-stealing counters: [0] scatter, [1] gather
@@ -342,7 +342,8 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
                 const int item0 = B.scene_chunk_start[s] + B.chunk_start[t];
                 const int nch = (te - ts + CHUNK - 1) / CHUNK;
                 for (int q = 0; q < nch; q++) {
-                    if (item0 + q >= 0 && item0 + q < B.item_cap) B.item_tile[item0 + q] = t;
+                    if (item0 + q >= 0 && item0 + q < B.item_cap)
+                        B.item[item0 + q] = make_int4(t, s, ts + q * CHUNK, min(te, ts + (q + 1) * CHUNK));
                     else set_status(B.status, ST_OOB);
                 }
             }
@@ -382,18 +383,15 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
         if (lane == 0) k = (int)atomicAdd(&B.work[0], 1u);
         k = __shfl_sync(0xffffffffu, k, 0);
         if (k >= items) break;
-        const int t = B.item_tile[k];
-        const int s = t >= 0 && t < B.nentries ? B.tile_scene[t] : -1;
-        if (s < 0) {
+        const int4 it = B.item[k];   // the chunk: its tile entry, scene and slots
+        const int t = it.x, s = it.y, c0 = it.z, c1 = it.w;
+        if (t < 0 || t >= B.nentries || s < 0 || s >= B.nscenes) {
             if (lane == 0) set_status(B.status, ST_OOB);
             continue;
         }
         const Scene2& sc = B.scene[s];
-        const int q = k - B.scene_chunk_start[s] - B.chunk_start[t];
-        const int ts = ts_cur[t], te = ts_cur[t + 1];
         const int p0 = sc.p0, p1 = sc.p0 + sc.np;
-        const int c0 = ts + q * CHUNK, c1 = min(te, c0 + CHUNK);
-        if (q < 0 || c0 >= c1 || ts < p0 || te > p1) {
+        if (c0 >= c1 || c0 < p0 || c1 > p1) {
             if (lane == 0) set_status(B.status, ST_OOB);
             continue;
         }
@@ -417,7 +415,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
             continue;
         }
         for (int j = lane; j < tc; j += 32) {
-            const int e = B.cursor[cb + j], b0 = j == 0 ? ts : B.cursor[cb + j - 1];
+            const int e = B.cursor[cb + j], b0 = j == 0 ? c0 : B.cursor[cb + j - 1];   // cell 0 starts at the tile's run start, <= c0
             const int lo = max(b0, c0), hi = min(e, c1);
             crange[j] = make_int2(lo, hi);
             if (hi > lo) atomicAdd(&bucket[QBUCKETS - 1 - min(hi - lo, QBUCKETS - 1)], 1);
@@ -526,15 +524,12 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS, BATCH_MIN_BLOCKS) k_batch2_
         if (lane == 0) k = (int)atomicAdd(&B.work[1], 1u);
         k = __shfl_sync(0xffffffffu, k, 0);
         if (k >= items) break;
-        const int t = B.item_tile[k];
-        const int s = t >= 0 && t < B.nentries ? B.tile_scene[t] : -1;
-        if (s < 0) continue;   // flagged in the scatter
+        const int4 it = B.item[k];   // the chunk: its tile entry, scene and slots
+        const int t = it.x, s = it.y, c0 = it.z, c1 = it.w;
+        if (t < 0 || t >= B.nentries || s < 0 || s >= B.nscenes) continue;   // flagged in the scatter
         const Scene2& sc = B.scene[s];
-        const int q = k - B.scene_chunk_start[s] - B.chunk_start[t];
-        const int ts = ts_cur[t], te = ts_cur[t + 1];
         const int p0 = sc.p0, p1 = sc.p0 + sc.np;
-        const int c0 = ts + q * CHUNK, c1 = min(te, c0 + CHUNK);
-        if (q < 0 || c0 >= c1 || ts < p0 || te > p1) continue;
+        if (c0 >= c1 || c0 < p0 || c1 > p1) continue;
         const int lt = t - sc.t0;
         const int tx = sc.tx, ty = sc.ty, nx = sc.nx, ny = sc.ny;
         const int x0 = (lt % sc.ntx) * tx, y0 = (lt / sc.ntx) * ty;
@@ -707,7 +702,7 @@ struct vf_mpm2_batch {
     int ncells = 0, nentries = 0;
     cudaStream_t stream = nullptr;
     DeviceBuffer scene_d, tile_scene, part[2], key, perm, cell_count, cursor, tile_count, tile_start[2], grid[2];
-    DeviceBuffer chunk_start, scene_chunks, scene_chunk_start, item_tile;
+    DeviceBuffer chunk_start, scene_chunks, scene_chunk_start, item;
     DeviceBuffer ctl;      // step counter, two work counters, the done count, the barrier, the phase clock
     DeviceBuffer status;
     int64_t nodes = 0;
@@ -741,8 +736,8 @@ Batch2 view(vf_mpm2_batch* h) {
     b.chunk_start = h->chunk_start.as<int>();
     b.scene_chunks = h->scene_chunks.as<int>();
     b.scene_chunk_start = h->scene_chunk_start.as<int>();
-    b.item_tile = h->item_tile.as<int>();
-    b.item_cap = (int)(h->item_tile.bytes / 4);
+    b.item = h->item.as<int4>();
+    b.item_cap = (int)(h->item.bytes / sizeof(int4));
     b.grid[0] = h->grid[0].as<float4>();
     b.grid[1] = h->grid[1].as<float4>();
     unsigned* ctl = h->ctl.as<unsigned>();
@@ -933,7 +928,7 @@ int32_t vf_mpm2_batch_create(const vf_scene2* scenes, int32_t nscenes, uint32_t 
         (rc = h->grid[0].alloc((size_t)nodes * 16)) || (rc = h->grid[1].alloc((size_t)nodes * 16)) ||
         (rc = h->chunk_start.alloc((size_t)entries * 4)) || (rc = h->scene_chunks.alloc((size_t)nscenes * 4)) ||
         (rc = h->scene_chunk_start.alloc((size_t)(nscenes + 1) * 4)) ||
-        (rc = h->item_tile.alloc((size_t)(np / CHUNK + entries + 1) * 4)) ||
+        (rc = h->item.alloc((size_t)(np / CHUNK + entries + 1) * sizeof(int4))) ||
         (rc = h->ctl.alloc(128)) || (rc = h->status.alloc(16)))
         return fail(rc);
     if (cudaMemcpyAsync(h->scene_d.ptr, sc.data(), sc.size() * sizeof(Scene2), cudaMemcpyHostToDevice, h->stream) !=
@@ -1073,7 +1068,7 @@ void vf_mpm2_batch_destroy(vf_mpm2_batch* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
     for (DeviceBuffer* b : {&h->scene_d, &h->tile_scene, &h->part[0], &h->part[1], &h->key, &h->perm, &h->cell_count,
                             &h->cursor, &h->tile_count, &h->tile_start[0], &h->tile_start[1], &h->grid[0], &h->grid[1],
-                            &h->chunk_start, &h->scene_chunks, &h->scene_chunk_start, &h->item_tile, &h->ctl,
+                            &h->chunk_start, &h->scene_chunks, &h->scene_chunk_start, &h->item, &h->ctl,
                             &h->status})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
