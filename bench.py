@@ -584,12 +584,12 @@ def run_ours(args, dist: Dist):
 def roofline3(prof, steps, np3, touched):
     """The roofline of the step's dominant kernel from a profiled run (CUDA events around every launch).
 
-    Fused step (the default): k_g2p2g3 gathers each particle from grid k and scatters it into grid k+1, so the
-    P2G+G2P pair is one kernel. Its algorithmic bytes a launch: read x, y, z, m, j (20 B) and write the 16 advected
-    fields (64 B) a particle, read grid k's four floats and write grid k+1's four floats a touched node (32 B):
-    84 Np + 32 N_t. `pair_target_ms` is the time the separate passes' bytes (152 Np + 28 N_t) take at 70% of the
-    peak: the north-star bar for P2G+G2P, which the fused kernel's time is compared with.
-    Separate passes: k_p2g3_tile + k_g2p3_tile at 152 Np + 28 N_t."""
+    Separate passes (the default): k_p2g3_tile + k_g2p3_tile at 152 Np + 28 N_t.
+    Fused step (opt-in): k_g2p2g3 gathers each particle from grid k and scatters it into grid k+1, so the P2G+G2P
+    pair is one kernel. Its algorithmic bytes a launch: read x, y, z, m, j (20 B) and write the 16 advected fields
+    (64 B) a particle, read grid k's four floats and write grid k+1's four floats a touched node (32 B): 84 Np + 32 N_t.
+    `pair_target_ms` is the time the separate passes' bytes (152 Np + 28 N_t) take at 70% of the peak: the P2G+G2P
+    target at 8M particles, which either form's time is compared with."""
     peak, peak_kind = measured_peaks()
     sep_bytes = 152.0 * np3 + 28.0 * touched
     if "k_g2p2g3" in prof:
